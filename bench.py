@@ -1,0 +1,349 @@
+"""Benchmark: batched L^p-annealed projected-Adam steps (forward convolution +
+adjoint correlation + update) at n = 8400 cells, B = 256 candidates per GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|fp32]
+                    [--impl ours|reference]
+
+One *step* = every candidate of the batch advances one Adam step.  The timed
+region is ONE launch of the fused local-search kernel running K steps (the
+population stays resident in shared memory), bracketed by a barrier and
+device synchronisation, timed with CUDA events on the launching stream, max
+over ranks.  ``value`` = whole-job batched steps/s (N GPUs x K steps / max
+time).  ``e2e`` = the same metric through the public call with host buffers:
+per step an H2D copy of the population from pinned memory, one
+``run_local_search`` step and a D2H copy of the updated population.
+
+Synthetic data: lognormal(0,1) fp32 heights with 1/3 exact zeros, a support
+gap of width n/10 at [n/50, n/50+n/10) and an endpoint atom (seeded PCG64,
+seed 8400 + rank), normalised to sum 1.
+
+``--impl reference`` times the reference's own CPU implementation of the
+path, the fp64 L^p-Adam twin of tools/probe.cpp (localSearch, OpenMP over
+candidates as in probe.cpp:239) compiled from the reference sources into
+oracle/_ref, on all host cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_CELLS = 8400
+BATCH = 256
+FLOP_PER_CAND_STEP = 4.0 * N_CELLS * N_CELLS        # conv 2n^2 + correlation 2n^2 (src/main.cu:313,625)
+ANNEAL = dict(p_start=2.0, p_end=1024.0, lr_start=1e-3, lr_end=1e-3)
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"],
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained"), "src": "measured",
+                "sm_max_mhz": d.get("sm_max_mhz", 1965.0)}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+            "src": "fallback", "sm_max_mhz": 1965.0}
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region (SM clock, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# --------------------------------- reference arm ---------------------------
+def reference_arm(args) -> None:
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref not built (reference sources absent here)"}))
+        return
+    from sidon_b200 import synth
+    probe = oracle.ref_probe()
+    threads = probe.ref_probe_threads()
+    sample_c = max(2, 2 * threads)          # candidates per timed step (bounded sample)
+    iters = 4                               # Adam steps per candidate per call
+    pop = synth.population("lognormal", N_CELLS, sample_c, seed=8400, dtype=np.float64)
+
+    def one():
+        x = np.ascontiguousarray(pop.copy())
+        t0 = time.perf_counter()
+        probe.ref_probe_local_search_batch(x.ctypes.data, N_CELLS, sample_c, iters, 2.0, 1024.0,
+                                           1e-3, 1e-3, 0.9, 0.999, 0, None)
+        return time.perf_counter() - t0
+
+    for _ in range(max(1, min(args.warmup, 1))):
+        one()
+    times = [one() for _ in range(args.steps)]
+    cand_steps_s = sample_c * iters * len(times) / sum(times)
+    v = cand_steps_s / BATCH                # batched (256-candidate) steps per second
+    line = {
+        "impl": "reference", "metric": "lp_adam_batched_steps_per_s", "value": v,
+        "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"lp_adam n={N_CELLS} B={BATCH} (lognormal heights)",
+                   "global_batch": BATCH, "n": N_CELLS},
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "reference",
+                         "sample": f"tools/probe.cpp localSearch (fp64 CPU twin), {sample_c} "
+                                   f"candidates x {iters} steps per timed step, OpenMP over "
+                                   f"candidates; each call adds one final objective "
+                                   f"(~1/4 step); scaled to {BATCH}-candidate steps"},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def cpu_baseline(budget_s: float = 10.0) -> dict:
+    """The reference CPU twin on this host's cores (bounded sample)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    from sidon_b200 import synth
+    if not oracle.have_ref():
+        return {"value": None, "unit": "steps/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    probe = oracle.ref_probe()
+    threads = probe.ref_probe_threads()
+    c = max(2, threads)
+    iters = 4
+    pop = synth.population("lognormal", N_CELLS, c, seed=8400, dtype=np.float64)
+    done, t = 0, 0.0
+    while t < budget_s:
+        x = np.ascontiguousarray(pop.copy())
+        t0 = time.perf_counter()
+        probe.ref_probe_local_search_batch(x.ctypes.data, N_CELLS, c, iters, 2.0, 1024.0, 1e-3,
+                                           1e-3, 0.9, 0.999, 0, None)
+        t += time.perf_counter() - t0
+        done += c * iters
+    v = done / t / BATCH
+    return {"value": v, "unit": "steps/s", "cores": threads, "kind": "reference",
+            "sample": f"tools/probe.cpp localSearch fp64 twin, n={N_CELLS}, {c} candidates x "
+                      f"{iters} steps per call, {done} candidate-steps in {t:.1f}s on {threads} "
+                      f"threads, scaled to {BATCH}-candidate steps"}
+
+
+# ----------------------------------- our arm -------------------------------
+def our_arm(args) -> None:
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = _dist()
+    if ws > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import sidon_b200
+    sidon_b200.load(build=not (ROOT / "sidon-autocorrelation-bound_b200" / "libsidon_b200.so").exists())
+    from sidon_b200 import kernels, synth
+
+    prec = args.precision
+    host = synth.population("lognormal", N_CELLS, BATCH, seed=8400 + rank)
+    pop = torch.as_tensor(host, device=dev)
+    mom = torch.empty_like(pop)
+    vel = torch.empty_like(pop)
+    stream = torch.cuda.current_stream()
+
+    def run(x, iters):
+        kernels.run_local_search(x, iters, mom=mom, vel=vel, precision=prec, **ANNEAL)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up: W steps, untimed
+    run(pop, max(3, args.warmup))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    pop.copy_(torch.as_tensor(host, device=dev))
+    flush.fill_(1.0)                                   # evict L2 before the timed launch
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        start.record(stream)
+        run(pop, args.steps)
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = t.item()
+    launches = 1
+
+    # search-time F error vs fp64 on the final population
+    Fcert, _ = kernels.run_eval(pop, with_nactive=False)
+    _, saved, _ = kernels.lp_forward(pop, 2.0, precision="fp32")
+    S = saved[:, 1].double()
+    F32 = 2.0 * N_CELLS * saved[:, 0].double() / (S * S)
+    f_rel = (F32 - Fcert).abs().div(Fcert).max().item()
+
+    # end-to-end through the public call with host buffers
+    hpin = torch.as_tensor(host).pin_memory()
+    hout = torch.empty_like(hpin).pin_memory()
+    e2e_steps = max(3, min(args.steps, 20))
+    x = torch.empty_like(pop)
+    for _ in range(2):
+        x.copy_(hpin, non_blocking=True)
+        run(x, 1)
+        hout.copy_(x, non_blocking=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        x.copy_(hpin, non_blocking=True)
+        run(x, 1)
+        hout.copy_(x, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
+    e2e_val = ws * e2e_steps / (e_ms.item() / 1e3)
+
+    if rank == 0:
+        peaks = _peaks()
+        value = ws * args.steps / (ms_max / 1e3)
+        per_launch_flop = FLOP_PER_CAND_STEP * BATCH * args.steps
+        achieved_tf = per_launch_flop / (ms / 1e3) / 1e12
+        ck = clk.summary()
+        if prec == "fp32":
+            mhz = ck["sm_mhz"] or peaks["sm_max_mhz"]
+            peak = 148 * 128 * 2 * mhz * 1e6 / 1e12     # FFMA lanes x 2 flop x clock
+            roof = {"bound": "fp32_simt", "achieved": achieved_tf, "peak": peak,
+                    "unit": "TFLOP/s", "frac": achieved_tf / peak, "traffic": _traffic(prec),
+                    "peak_src": f"derived: 148 SMs x 128 FFMA/clk x 2 x {mhz:.0f} MHz (sampled)"}
+        else:
+            peak = peaks["bf16_tflops"]
+            roof = {"bound": "tensor", "achieved": achieved_tf, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved_tf / peak, "traffic": _traffic(prec),
+                    "peak_src": f"bf16_tflops ({peaks['src']}, burst)",
+                    "frac_of_3_product_ceiling": 3.0 * achieved_tf / peak if prec == "bf16x3"
+                    else achieved_tf / peak}
+        line = {
+            "metric": "lp_adam_batched_steps_per_s", "value": value, "unit": "steps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"fp32": "f32", "bf16x3": "bf16x3(f32 acc)",
+                                            "bf16x1": "bf16(f32 acc)"}[prec],
+            "data": "synthetic",
+            "config": {"workload": f"lp_adam n={N_CELLS} B={BATCH}/GPU lognormal heights, "
+                                   f"{prec} conv/corr, p {ANNEAL['p_start']}->{ANNEAL['p_end']}",
+                       "global_batch": BATCH * ws, "n": N_CELLS, "precision": prec,
+                       "parallelism": f"candidates sharded, {ws} x {BATCH}",
+                       "l2": "single launch of K steps, population resident in shared memory; "
+                             "L2 flushed (256 MB write) before the timed launch"},
+            "candidate_steps_per_s": value * BATCH,
+            "f_evals_per_s": value * BATCH,
+            "f_rel_err_vs_fp64": f_rel,
+            "roofline": roof,
+            "clocks": {"sm_mhz": ck["sm_mhz"], "sm_max_mhz": ck["sm_max_mhz"],
+                       "reasons": ck["reasons"]},
+            "e2e": {"value": e2e_val, "unit": "steps/s",
+                    "h2d_bytes_per_step": int(hpin.numel() * 4),
+                    "d2h_bytes_per_step": int(hout.numel() * 4)},
+            "gpu_launches": launches,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_budget)
+        print(json.dumps(line))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _traffic(prec: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get(prec)
+    return None
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default=os.environ.get("SIDON_BENCH_PRECISION", "fp32"),
+                    choices=["fp32", "bf16x3", "bf16x1"])
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,170 @@
+/* ---------------------------------------------------------------------------
+ * sidon_b200.h -- C ABI of the B200 engine for the discretised
+ * autoconvolution ratio
+ *
+ *     F(a) = 2 n max_k b_k / (sum_i a_i)^2 ,   b = a * a ,   a >= 0.
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream passed as
+ * void* (NULL = the legacy default stream), returns an int status (0 = ok,
+ * see sidon_status) and never exits the process.  Device pointers are
+ * caller-owned; nothing here allocates inside a hot call.  Populations are
+ * [P][n] row-major and are updated in place, as in the reference.
+ *
+ * Each declaration names the reference interface it replaces (paths are
+ * relative to the reference project root).
+ * ------------------------------------------------------------------------- */
+#ifndef SIDON_B200_H
+#define SIDON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SIDON_API __attribute__((visibility("default")))
+#else
+#define SIDON_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------- status codes ------------------------------ */
+enum sidon_status {
+  SIDON_OK = 0,
+  SIDON_ERR_ARG = 1,          /* null pointer, P <= 0, bad parameter           */
+  SIDON_ERR_N = 2,            /* n outside the supported range                 */
+  SIDON_ERR_SMEM = 3,         /* working set exceeds the per-CTA smem opt-in   */
+  SIDON_ERR_CUDA = 4,         /* CUDA runtime error (sidon_last_cuda_error)    */
+  SIDON_ERR_DTYPE = 5,        /* dtype / precision not supported by this call  */
+  SIDON_ERR_NONFINITE = 6,    /* input held NaN/Inf/negative heights           */
+  SIDON_ERR_TIMEOUT = 7,      /* a bounded device-side wait ran out            */
+  SIDON_ERR_DEVICE = 8        /* current device is not an sm_100 part          */
+};
+
+enum sidon_dtype { SIDON_F32 = 0, SIDON_F64 = 1 };
+
+/* arithmetic of the convolution/correlation inside the local search */
+enum sidon_precision {
+  SIDON_PREC_FP32_SIMT = 0,   /* fp32 FFMA chains on the CUDA cores            */
+  SIDON_PREC_BF16X1 = 1,      /* tcgen05 block-Toeplitz, hi*hi                 */
+  SIDON_PREC_BF16X3 = 2,      /* tcgen05 block-Toeplitz, hi*hi + hi*lo + lo*hi */
+  SIDON_PREC_FP64_SIMT = 3    /* fp64 DFMA chains (the polish instantiation)   */
+};
+
+/* operator ids for sidon_smem_bytes */
+enum sidon_op {
+  SIDON_OP_LOCAL_SEARCH = 0,  /* src/kernels.cuh:161-162 localSearchSmem<T>     */
+  SIDON_OP_EVAL = 1,          /* src/kernels.cuh:379-380 evalSmem<Acc>          */
+  SIDON_OP_FRANK_WOLFE = 2,   /* src/kernels.cuh:405-406 fwSmem<T>              */
+  SIDON_OP_LOCAL_SEARCH_TC = 3
+};
+
+/* Human-readable name of a status code. */
+SIDON_API const char* sidon_status_string(int status);
+/* The cudaError_t value behind the last SIDON_ERR_CUDA on this thread. */
+SIDON_API int sidon_last_cuda_error(void);
+/* ABI version of this library (bumped on any signature change). */
+SIDON_API int sidon_abi_version(void);
+
+/* Dynamic shared memory one CTA of `op` needs at size n and dtype, in bytes;
+ * 0 if the combination is unsupported.
+ * Replaces localSearchSmem / evalSmem / fwSmem (src/kernels.cuh:161-162,
+ * 379-380, 405-406). */
+SIDON_API size_t sidon_smem_bytes(int op, int n, int dtype);
+/* Largest n the op accepts on the current device (smem opt-in bound). */
+SIDON_API int sidon_max_n(int op, int dtype);
+
+/* fp64 F on the host: direct O(n * nnz) convolution skipping a_i == 0,
+ * M = max b, S = sum a (sequential), F = 2 n M / S^2.
+ * Replaces hostF (src/main.cu:95-105); bit-identical to it. */
+SIDON_API double sidon_hostF(const double* a, int n);
+
+/* Certifying evaluation of a population: F per candidate in fp64 (b formed
+ * as in hostF: each product rounded, then added in i order; S summed in i
+ * order -- so F equals hostF bit for bit) and, if out_nactive != NULL, the
+ * number of k with b_k >= M (1 - active_tol).  F = 1e30 when S <= 0.
+ * pop: device [P][n] of dtype; out_F: device [P]; out_nactive: device [P].
+ * Replaces kEval<T,double> + runEval (src/kernels.cuh:301-377,
+ * src/main.cu:161-166). */
+SIDON_API int sidon_eval(const void* pop, int dtype, int n, int P, double* out_F, int* out_nactive,
+               double active_tol, void* stream);
+
+/* Exact certification: every near-maximal b_k is recomputed EXACTLY (a
+ * fixed-point accumulator; fp32 products are exact in fp64, fp64 products
+ * are split with FMA) and rounded once; S is summed exactly and rounded
+ * once; F = 2 n M / (S S) in fp64.  Because a cell split maps M -> 2M and
+ * S -> 2S exactly, this F is bit-identical across sidon_refine.  Outputs
+ * (device, [P]; any may be NULL except out_F): F, M, S, argmax k.
+ * No single reference counterpart: it strengthens kEval
+ * (src/kernels.cuh:301-377) for the ladder's split invariance
+ * (src/kernels.cuh:535-536). */
+SIDON_API int sidon_certify(const void* pop, int dtype, int n, int P, double* out_F, double* out_M,
+                  double* out_S, int* out_kmax, void* stream);
+
+/* Fused L^p-annealed projected Adam / mirror descent: `iters` steps with
+ * `pop` resident in shared memory, p = p_start (p_end/p_start)^(it/(iters-1)),
+ * lr likewise; mode 0 = projected Adam, 1 = exponentiated gradient;
+ * skip[pid] != 0 leaves candidate pid untouched; mode_arr (may be NULL)
+ * overrides mode_default per candidate.  mom/vel: device [P][n] scratch of
+ * dtype, zeroed at entry as in the reference.  dtype SIDON_F32 with
+ * precision FP32_SIMT / BF16X1 / BF16X3, or SIDON_F64 with FP64_SIMT.
+ * Replaces kLocalSearch<T> + runLocalSearch (src/kernels.cuh:177-289,
+ * src/main.cu:152-159) and the fp64 polish launch (src/main.cu:837-839). */
+SIDON_API int sidon_local_search(void* pop, void* mom, void* vel, const int* skip, const int* mode_arr,
+                       int n, int P, int iters, double p_start, double p_end, double lr_start,
+                       double lr_end, double beta1, double beta2, int mode_default, int dtype,
+                       int precision, void* stream);
+
+/* Smoothed objective G_p(a) = 2n ||a*a||_p / (sum a)^2 for a batch (fp32
+ * heights, any scale).  Writes value[P] (device) and saved[P*4] (device,
+ * {M = max b, S = sum a, R = sum (b/M)^p, G_p}); b itself is not stored
+ * unless b_out != NULL ([P][2n-1] device, for the stored-b comparison).
+ * No reference counterpart as an entry point: it exposes the objective of
+ * the anneal (src/kernels.cuh:168-172). */
+SIDON_API int sidon_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
+                     float* b_out, int precision, void* stream);
+
+/* Gradient of G_p: grad_i = (4n R^(1/p)/S^2) (G_i/R - M/S) with
+ * G_i = sum_j (b_{i+j}/M)^(p-1) a_j.  b is recomputed tile by tile from a
+ * (b_in == NULL) or read from a stored [P][2n-1] array (b_in != NULL).
+ * saved: the forward's [P*4].  grad: device [P][n] fp32.
+ * Replaces the gradient that exists only inside kLocalSearch
+ * (src/kernels.cuh:221-244) and its CPU twin (tools/probe.cpp:77-92). */
+SIDON_API int sidon_lp_backward(const float* a, const float* saved, const float* b_in, int n, int P,
+                      double p, float* grad, int precision, void* stream);
+
+/* Frank-Wolfe / LP step solved by Chambolle-Pock: per round, M = max(a*a),
+ * pdhg_iters of  lambda <- [lambda + sigma (a*gbar - M)]_+ ,
+ * g <- [g + tau (1 - A^T lambda)]_+ , gbar = 2 g_new - g_old ; normalise g;
+ * nT-point line search over t in (0, t_max]; move a.  tau <= 0 or
+ * sigma <= 0 select the reference steps tau = 0.9/n, sigma = 0.9 n.
+ * Replaces kFrankWolfe<float> + runFrankWolfe (src/kernels.cuh:408-532,
+ * src/main.cu:170-178); returns SIDON_ERR_SMEM where the reference's
+ * runFrankWolfe returned false. */
+SIDON_API int sidon_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int pdhg_iters,
+                      int nT, float t_max, float tau, float sigma, void* stream);
+
+/* Cell split n -> 2n: dst[p][2i] = dst[p][2i+1] = src[p][i].
+ * Replaces kRefine<T> (src/kernels.cuh:538-547) and the host refine
+ * (src/main.cu:491-495). */
+SIDON_API int sidon_refine(const void* src, int n, int P, void* dst, int dtype, void* stream);
+
+/* Pairwise average 2n -> n.  Replaces kCoarsen<T> (src/kernels.cuh:550-557). */
+SIDON_API int sidon_coarsen(const void* src, int n2, int P, void* dst, int dtype, void* stream);
+
+/* Island selection + migration on the device: islands are n_islands
+ * groups of P/n_islands consecutive slots (at most 1024 per island); each is
+ * ranked by fit ascending (ties by slot index, NaN last) into order_out
+ * (device [P], caller-owned, required); then the
+ * j-th best of island i overwrites the j-th worst of island (i+1) mod NI for
+ * j < k_migrate (rows of pop and entries of fit).  Requires
+ * 2 k_migrate <= P/n_islands.  k_migrate = 0 ranks only.
+ * Replaces the host ranking and D2D migration (src/main.cu:676-692). */
+SIDON_API int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, int k_migrate,
+                         int* order_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIDON_B200_H */

@@ -1,0 +1,612 @@
+/* ---------------------------------------------------------------------------
+ * sidon_oracle.c -- CPU restatement of the reference hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker: tests/, the smoke
+ * check of __graft_entry__ and the cpu_baseline leg of bench.py may load it;
+ * nothing on the product path does.  Every function cites the reference
+ * file:line it restates (paths are relative to the reference project root).
+ *
+ * Objective:  F(a) = 2 n max_k b_k / (sum_i a_i)^2 ,  b = a*a ,  a >= 0.
+ *
+ * Arithmetic conventions (chosen so that the CUDA kernels can be compared
+ * bit for bit where that is meaningful):
+ *   - fp32 convolutions / correlations are fmaf chains over the summation
+ *     index in increasing order, starting from +0 (one rounding per term),
+ *     exactly as a per-output FFMA chain on the GPU;
+ *   - the fp64 certifying evaluation follows hostF (src/main.cu:95-105):
+ *     product rounded, then added, i ascending; S summed sequentially.
+ * ------------------------------------------------------------------------- */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define SO_EXPORT __attribute__((visibility("default")))
+
+/* ======================= F in fp64, hostF semantics ======================= */
+/* src/main.cu:95-105: b[i+j] += a_i a_j for a_i != 0 (i-major), M = max b,
+ * S = sum a (sequential), F = 2 n M / S^2.  b is returned when b_out != NULL. */
+SO_EXPORT double so_hostF_b(const double* a, int n, double* b_out) {
+  const int nb = 2 * n - 1;
+  double* b = (double*)calloc((size_t)nb, sizeof(double));
+  for (int i = 0; i < n; ++i) {
+    if (a[i] == 0.0) continue;
+    const double ai = a[i];
+    for (int j = 0; j < n; ++j) {
+      volatile double prod = ai * a[j];   /* keep mul and add separately rounded */
+      b[i + j] += prod;
+    }
+  }
+  double M = 0.0;
+  for (int k = 0; k < nb; ++k) M = b[k] > M ? b[k] : M;
+  double S = 0.0;
+  for (int i = 0; i < n; ++i) S += a[i];
+  if (b_out) memcpy(b_out, b, sizeof(double) * (size_t)nb);
+  free(b);
+  return 2.0 * (double)n * M / (S * S);
+}
+
+SO_EXPORT double so_hostF(const double* a, int n) { return so_hostF_b(a, n, NULL); }
+
+/* ================= certifying evaluation over a population =============== */
+/* src/kernels.cuh:301-377 (kEval): F per candidate plus the number of k with
+ * b_k >= M (1 - tol).  b is formed in hostF order (see header); F = 1e30 when
+ * S <= 0 (kernels.cuh:376). */
+SO_EXPORT void so_eval(const double* pop, int n, int P, double tol, double* F, int* nact) {
+  const int nb = 2 * n - 1;
+  double* b = (double*)malloc(sizeof(double) * (size_t)nb);
+  for (int p = 0; p < P; ++p) {
+    const double* a = pop + (size_t)p * n;
+    for (int k = 0; k < nb; ++k) b[k] = 0.0;
+    for (int i = 0; i < n; ++i) {
+      if (a[i] == 0.0) continue;
+      for (int j = 0; j < n; ++j) { volatile double prod = a[i] * a[j]; b[i + j] += prod; }
+    }
+    double M = 0.0, S = 0.0;
+    for (int k = 0; k < nb; ++k) M = b[k] > M ? b[k] : M;
+    for (int i = 0; i < n; ++i) S += a[i];
+    if (nact) {
+      const double thr = M * (1.0 - tol);
+      int c = 0;
+      for (int k = 0; k < nb; ++k) c += (b[k] >= thr);
+      nact[p] = c;
+    }
+    F[p] = (S > 0.0) ? (2.0 * (double)n * M / (S * S)) : 1e30;
+  }
+  free(b);
+}
+
+/* =================== long-double verifier (probe --verify) ================ */
+/* tools/probe.cpp:146-195: b_k as a direct sum over i ascending in long
+ * double, M, S, F, the round-off bound 3 n eps / (1 - n eps) with eps = 2^-63,
+ * and the count of b_k within 1e-9 of M.  Returns 1 if any a_i < 0. */
+SO_EXPORT int so_verify_ld(const double* a_in, int n, long double* F, long double* M_out,
+                           long double* S_out, int* kmax_out, int* nactive_out,
+                           long double* relbound) {
+  long double* a = (long double*)malloc(sizeof(long double) * (size_t)n);
+  int neg = 0;
+  for (int i = 0; i < n; ++i) { a[i] = (long double)a_in[i]; if (a[i] < 0) neg = 1; }
+  const int nb = 2 * n - 1;
+  long double* b = (long double*)malloc(sizeof(long double) * (size_t)nb);
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < nb; ++k) {
+    const int ilo = k - n + 1 > 0 ? k - n + 1 : 0, ihi = k < n - 1 ? k : n - 1;
+    long double s = 0.0L;
+    for (int i = ilo; i <= ihi; ++i) s += a[i] * a[k - i];
+    b[k] = s;
+  }
+  long double M = 0, S = 0; int kmax = 0;
+  for (int k = 0; k < nb; ++k) if (b[k] > M) { M = b[k]; kmax = k; }
+  for (int i = 0; i < n; ++i) S += a[i];
+  const long double eps = 1.084202172485504434e-19L;
+  const long double gam = (long double)n * eps / (1 - (long double)n * eps);
+  int nAct = 0;
+  for (int k = 0; k < nb; ++k) if (b[k] >= M * (1 - 1e-9L)) ++nAct;
+  *F = 2.0L * (long double)n * M / (S * S);
+  if (M_out) *M_out = M;
+  if (S_out) *S_out = S;
+  if (kmax_out) *kmax_out = kmax;
+  if (nactive_out) *nactive_out = nAct;
+  if (relbound) *relbound = 3 * gam;
+  free(a); free(b);
+  return neg;
+}
+
+/* ============================ fp32 primitives ============================= */
+/* src/kernels.cuh:97-135 (crossconv/autoconv): b_k = sum_i x_i y_{k-i},
+ * k = 0..2n-2, one fmaf chain per k over i ascending. */
+static void conv_f32(const float* x, const float* y, float* b, int n) {
+  for (int k = 0; k < 2 * n - 1; ++k) {
+    const int ilo = k - (n - 1) > 0 ? k - (n - 1) : 0, ihi = k < n - 1 ? k : n - 1;
+    float acc = 0.0f;
+    for (int i = ilo; i <= ihi; ++i) acc = fmaf(x[i], y[k - i], acc);
+    b[k] = acc;
+  }
+}
+/* src/kernels.cuh:142-158 (corrTile): G_i = sum_j c_{i+j} a_j, j ascending. */
+static void corr_f32(const float* a, const float* c, float* G, int n) {
+  for (int i = 0; i < n; ++i) {
+    float acc = 0.0f;
+    for (int j = 0; j < n; ++j) acc = fmaf(a[j], c[i + j], acc);
+    G[i] = acc;
+  }
+}
+SO_EXPORT void so_conv_f32(const float* x, const float* y, float* b, int n) { conv_f32(x, y, b, n); }
+SO_EXPORT void so_corr_f32(const float* a, const float* c, float* G, int n) { corr_f32(a, c, G, n); }
+
+/* fp64 twins (used by the fp64 local search) */
+static void conv_f64(const double* x, const double* y, double* b, int n) {
+  for (int k = 0; k < 2 * n - 1; ++k) {
+    const int ilo = k - (n - 1) > 0 ? k - (n - 1) : 0, ihi = k < n - 1 ? k : n - 1;
+    double acc = 0.0;
+    for (int i = ilo; i <= ihi; ++i) acc = fma(x[i], y[k - i], acc);
+    b[k] = acc;
+  }
+}
+static void corr_f64(const double* a, const double* c, double* G, int n) {
+  for (int i = 0; i < n; ++i) {
+    double acc = 0.0;
+    for (int j = 0; j < n; ++j) acc = fma(a[j], c[i + j], acc);
+    G[i] = acc;
+  }
+}
+
+/* ===================== L^p-annealed projected Adam ======================== */
+/* src/kernels.cuh:177-289 (kLocalSearch), one candidate, in the kernel's
+ * update order: conv, M, weights c_k = (1+d)^(p-1) with d = (b_k-M)/M and
+ * R = sum c_k (1+d), bias corrections, correlation G, g_i = G_i/R - M,
+ * Adam (mode 0) or mirror step (mode 1), projection, renormalisation.
+ * mom/vel are zeroed at entry (kernels.cuh:196). */
+#define SO_LS_BODY(T, CONV, CORR, EXP, LOG1P, SQRT, FMA)                                   \
+  const int nb = 2 * n - 1;                                                                \
+  T* b = (T*)malloc(sizeof(T) * (size_t)(2 * n));                                          \
+  T* G = (T*)malloc(sizeof(T) * (size_t)n);                                                \
+  T* m = (T*)calloc((size_t)n, sizeof(T));                                                 \
+  T* v = (T*)calloc((size_t)n, sizeof(T));                                                 \
+  const T lnPr = (T)log((double)pEnd / (double)pStart);                                    \
+  const T lnLr = (T)log((double)lrEnd / (double)lrStart);                                  \
+  T b1t = (T)1, b2t = (T)1;                                                                \
+  for (int it = 0; it < iters; ++it) {                                                     \
+    const T frac = iters > 1 ? (T)it / (T)(iters - 1) : (T)0;                              \
+    const T pexp = pStart * EXP(lnPr * frac);                                              \
+    const T lr = lrStart * EXP(lnLr * frac);                                               \
+    CONV(a, a, b, n);                                                                      \
+    T M = (T)0;                                                                            \
+    for (int k = 0; k < nb; ++k) M = b[k] > M ? b[k] : M;                                  \
+    if (!(M > (T)0)) break;                                                                \
+    T R = (T)0;                                                                            \
+    for (int k = 0; k < nb; ++k) {                                                         \
+      const T d = (b[k] - M) / M;                                                          \
+      const T c = d > (T)-1 ? EXP((pexp - (T)1) * LOG1P(d)) : (T)0;                        \
+      R += c * ((T)1 + d);                                                                 \
+      b[k] = c;                                                                            \
+    }                                                                                      \
+    b[nb] = (T)0;                                                                          \
+    b1t *= beta1; b2t *= beta2;                                                            \
+    const T bc1 = (T)1 / ((T)1 - b1t), bc2 = (T)1 / ((T)1 - b2t);                          \
+    CORR(a, b, G, n);                                                                      \
+    T S = (T)0;                                                                            \
+    for (int i = 0; i < n; ++i) {                                                          \
+      const T gi = G[i] / R - M;                                                           \
+      T x;                                                                                 \
+      if (mode == 0) {                                                                     \
+        const T mm = FMA(beta1, m[i], ((T)1 - beta1) * gi);                                \
+        const T vv = FMA(beta2, v[i], ((T)1 - beta2) * gi * gi);                           \
+        m[i] = mm; v[i] = vv;                                                              \
+        const T step = (lr / (T)n) * (mm * bc1) / (SQRT(vv * bc2) + (T)1e-30);             \
+        x = a[i] - step;                                                                   \
+        if (x < (T)0) x = (T)0;                                                            \
+      } else {                                                                             \
+        T e = -lr * (gi / M);                                                              \
+        if (e > (T)4) e = (T)4;                                                            \
+        if (e < (T)-4) e = (T)-4;                                                          \
+        x = a[i] * EXP(e);                                                                 \
+      }                                                                                    \
+      a[i] = x; S += x;                                                                    \
+    }                                                                                      \
+    if (!(S > (T)0)) { for (int i = 0; i < n; ++i) a[i] = (T)1 / (T)n; S = (T)1; }         \
+    const T inv = (T)1 / S;                                                                \
+    for (int i = 0; i < n; ++i) a[i] *= inv;                                               \
+  }                                                                                        \
+  free(b); free(G); free(m); free(v);
+
+static void ls_f32(float* a, int n, int iters, float pStart, float pEnd, float lrStart,
+                   float lrEnd, float beta1, float beta2, int mode) {
+  SO_LS_BODY(float, conv_f32, corr_f32, expf, log1pf, sqrtf, fmaf)
+}
+static void ls_f64(double* a, int n, int iters, double pStart, double pEnd, double lrStart,
+                   double lrEnd, double beta1, double beta2, int mode) {
+  SO_LS_BODY(double, conv_f64, corr_f64, exp, log1p, sqrt, fma)
+}
+
+/* Population driver with the kernel's skip[] / modeArr[] semantics
+ * (kernels.cuh:188-190): skipped candidates are left untouched. */
+SO_EXPORT void so_local_search_f32(float* pop, int n, int P, int iters, float pS, float pE,
+                                   float lrS, float lrE, float b1, float b2, const int* skip,
+                                   const int* mode_arr, int mode_default) {
+#pragma omp parallel for schedule(dynamic)
+  for (int p = 0; p < P; ++p) {
+    if (skip && skip[p]) continue;
+    ls_f32(pop + (size_t)p * n, n, iters, pS, pE, lrS, lrE, b1, b2,
+           mode_arr ? mode_arr[p] : mode_default);
+  }
+}
+SO_EXPORT void so_local_search_f64(double* pop, int n, int P, int iters, double pS, double pE,
+                                   double lrS, double lrE, double b1, double b2, const int* skip,
+                                   const int* mode_arr, int mode_default) {
+#pragma omp parallel for schedule(dynamic)
+  for (int p = 0; p < P; ++p) {
+    if (skip && skip[p]) continue;
+    ls_f64(pop + (size_t)p * n, n, iters, pS, pE, lrS, lrE, b1, b2,
+           mode_arr ? mode_arr[p] : mode_default);
+  }
+}
+
+/* One step's intermediates at fp32 (for single-step parity): b = a*a, M,
+ * c (in place of b), R, G.  Mirrors kernels.cuh:213-239. */
+SO_EXPORT void so_lp_step_terms_f32(const float* a, int n, float p, float* b_out, float* c_out,
+                                    float* G_out, float* MR_out) {
+  const int nb = 2 * n - 1;
+  float* b = (float*)malloc(sizeof(float) * (size_t)(2 * n));
+  conv_f32(a, a, b, n);
+  if (b_out) memcpy(b_out, b, sizeof(float) * (size_t)nb);
+  float M = 0.f;
+  for (int k = 0; k < nb; ++k) M = b[k] > M ? b[k] : M;
+  float R = 0.f;
+  for (int k = 0; k < nb; ++k) {
+    const float d = (b[k] - M) / M;
+    const float c = d > -1.f ? expf((p - 1.f) * log1pf(d)) : 0.f;
+    R += c * (1.f + d);
+    b[k] = c;
+  }
+  b[nb] = 0.f;
+  if (c_out) memcpy(c_out, b, sizeof(float) * (size_t)nb);
+  if (G_out) corr_f32(a, b, G_out, n);
+  MR_out[0] = M; MR_out[1] = R;
+  free(b);
+}
+
+/* ====================== smoothed objective and gradient =================== */
+/* G_p(a) = 2n ||a*a||_p / (sum a)^2 (the objective the reference's anneal
+ * minimises, kernels.cuh:168-172).  With M = max|b|, u = |b|/M,
+ * R = sum u^p:  G_p = 2n M R^(1/p) / S^2 and
+ *   dG_p/da_i = (4n R^(1/p) / S^2) (G_i / R - M / S),  G_i = sum_j u_{i+j}^(p-1) a_j,
+ * the gradient whose descent direction the reference uses when S = 1
+ * (kernels.cuh:169-172, tools/probe.cpp:87-92).  |b| keeps the value defined
+ * for finite-difference probes that step a coordinate below zero.  Long
+ * double throughout. */
+SO_EXPORT double so_lp_value_ld(const double* a_in, int n, double p) {
+  const int nb = 2 * n - 1;
+  long double* a = (long double*)malloc(sizeof(long double) * (size_t)n);
+  long double* b = (long double*)malloc(sizeof(long double) * (size_t)nb);
+  for (int i = 0; i < n; ++i) a[i] = a_in[i];
+  long double S = 0, M = 0;
+  for (int i = 0; i < n; ++i) S += a[i];
+  for (int k = 0; k < nb; ++k) {
+    const int ilo = k - n + 1 > 0 ? k - n + 1 : 0, ihi = k < n - 1 ? k : n - 1;
+    long double s = 0;
+    for (int i = ilo; i <= ihi; ++i) s += a[i] * a[k - i];
+    b[k] = fabsl(s);
+    if (b[k] > M) M = b[k];
+  }
+  long double R = 0;
+  for (int k = 0; k < nb; ++k) R += powl(b[k] / M, (long double)p);
+  const long double val = 2.0L * n * M * powl(R, 1.0L / (long double)p) / (S * S);
+  free(a); free(b);
+  return (double)val;
+}
+
+SO_EXPORT void so_lp_grad_ld(const double* a_in, int n, double p, double* grad, double* value) {
+  const int nb = 2 * n - 1;
+  long double* a = (long double*)malloc(sizeof(long double) * (size_t)n);
+  long double* c = (long double*)malloc(sizeof(long double) * (size_t)nb);
+  for (int i = 0; i < n; ++i) a[i] = a_in[i];
+  long double S = 0, M = 0;
+  for (int i = 0; i < n; ++i) S += a[i];
+  for (int k = 0; k < nb; ++k) {
+    const int ilo = k - n + 1 > 0 ? k - n + 1 : 0, ihi = k < n - 1 ? k : n - 1;
+    long double s = 0;
+    for (int i = ilo; i <= ihi; ++i) s += a[i] * a[k - i];
+    c[k] = s;
+    if (s > M) M = s;
+  }
+  long double R = 0;
+  for (int k = 0; k < nb; ++k) {
+    const long double u = c[k] / M;
+    R += powl(u, (long double)p);
+    c[k] = powl(u, (long double)p - 1.0L);
+  }
+  const long double Rp = powl(R, 1.0L / (long double)p);
+  const long double scale = 4.0L * n * Rp / (S * S);
+  for (int i = 0; i < n; ++i) {
+    long double g = 0;
+    for (int j = 0; j < n; ++j) g += c[i + j] * a[j];
+    grad[i] = (double)(scale * (g / R - M / S));
+  }
+  if (value) *value = (double)(2.0L * n * M * Rp / (S * S));
+  free(a); free(c);
+}
+
+/* ============== Frank-Wolfe step solved by Chambolle-Pock ================= */
+/* src/kernels.cuh:408-532 (kFrankWolfe), fp32, in the kernel's order.
+ * tau_scale / sig_scale: tau = tau_scale / n, sigma = sig_scale * n
+ * (the reference uses 0.9 and 0.9, kernels.cuh:440). */
+static void fw_f32(float* a, int n, int rounds, int pdhgIters, int nT, float tMax, float tau_c,
+                   float sig_c) {
+  const int nb = 2 * n - 1;
+  float* G = (float*)malloc(sizeof(float) * (size_t)n);
+  float* Gb = (float*)malloc(sizeof(float) * (size_t)n);
+  float* lam = (float*)calloc((size_t)(2 * n), sizeof(float));
+  float* tmp = (float*)malloc(sizeof(float) * (size_t)(2 * n));
+  float* cc = (float*)malloc(sizeof(float) * (size_t)n);
+  float s = 0.f;
+  for (int i = 0; i < n; ++i) s += a[i];
+  if (!(s > 0.f)) goto done;
+  {
+    const float inv = 1.f / s;
+    for (int i = 0; i < n; ++i) a[i] *= inv;
+  }
+  {
+    const float tau = tau_c / (float)n, sig = sig_c * (float)n;
+    for (int r = 0; r < rounds; ++r) {
+      conv_f32(a, a, tmp, n);
+      float M = 0.f;
+      for (int k = 0; k < nb; ++k) M = tmp[k] > M ? tmp[k] : M;
+      if (!(M > 0.f)) break;
+      for (int i = 0; i < n; ++i) { G[i] = a[i]; Gb[i] = a[i]; }
+      for (int k = 0; k < 2 * n; ++k) lam[k] = 0.f;
+      for (int it = 0; it < pdhgIters; ++it) {
+        conv_f32(a, Gb, tmp, n);
+        for (int k = 0; k < nb; ++k) {
+          const float l = lam[k] + sig * (tmp[k] - M);
+          lam[k] = l > 0.f ? l : 0.f;
+        }
+        corr_f32(a, lam, cc, n);
+        for (int i = 0; i < n; ++i) {
+          const float gn = G[i] + tau * (1.f - cc[i]);
+          Gb[i] = gn > 0.f ? gn : 0.f;
+        }
+        for (int i = 0; i < n; ++i) {
+          const float gn = Gb[i], go = G[i];
+          G[i] = gn;
+          Gb[i] = 2.f * gn - go;
+        }
+      }
+      float sg = 0.f;
+      for (int i = 0; i < n; ++i) sg += G[i];
+      if (!(sg > 0.f)) break;
+      {
+        const float inv = 1.f / sg;
+        for (int i = 0; i < n; ++i) G[i] *= inv;
+      }
+      float bestT = 0.f, bestM = M;
+      for (int st = 1; st <= nT; ++st) {
+        const float t = tMax * (float)st / (float)nT;
+        for (int i = 0; i < n; ++i) Gb[i] = (1.f - t) * a[i] + t * G[i];
+        conv_f32(Gb, Gb, tmp, n);
+        float mm = 0.f;
+        for (int k = 0; k < nb; ++k) mm = tmp[k] > mm ? tmp[k] : mm;
+        if (mm < bestM) { bestM = mm; bestT = t; }
+      }
+      if (!(bestT > 0.f)) break;
+      for (int i = 0; i < n; ++i) a[i] = (1.f - bestT) * a[i] + bestT * G[i];
+    }
+  }
+done:
+  free(G); free(Gb); free(lam); free(tmp); free(cc);
+}
+
+SO_EXPORT void so_frank_wolfe_f32(float* pop, int n, int P, int rounds, int pdhgIters, int nT,
+                                  float tMax, float tau_c, float sig_c, const int* skip) {
+#pragma omp parallel for schedule(dynamic)
+  for (int p = 0; p < P; ++p) {
+    if (skip && skip[p]) continue;
+    fw_f32(pop + (size_t)p * n, n, rounds, pdhgIters, nT, tMax, tau_c, sig_c);
+  }
+}
+
+/* ============================ cell-split ladder =========================== */
+/* src/kernels.cuh:538-547 (kRefine) and src/main.cu:494-495: a'_{2i} = a'_{2i+1} = a_i. */
+SO_EXPORT void so_refine_f64(const double* src, int n, int P, double* dst) {
+  for (int p = 0; p < P; ++p)
+    for (int i = 0; i < n; ++i) {
+      const double x = src[(size_t)p * n + i];
+      dst[(size_t)p * 2 * n + 2 * i] = x;
+      dst[(size_t)p * 2 * n + 2 * i + 1] = x;
+    }
+}
+/* src/kernels.cuh:550-557 (kCoarsen): d_i = 0.5 (s_{2i} + s_{2i+1}). */
+SO_EXPORT void so_coarsen_f64(const double* src, int n2, int P, double* dst) {
+  for (int p = 0; p < P; ++p)
+    for (int i = 0; i < n2 / 2; ++i)
+      dst[(size_t)p * (n2 / 2) + i] =
+          0.5 * (src[(size_t)p * n2 + 2 * i] + src[(size_t)p * n2 + 2 * i + 1]);
+}
+
+/* ========================= island ranking + migration ===================== */
+/* src/main.cu:676-692: each island (PI consecutive slots) is ranked by fp64
+ * fitness, ascending; ties are broken by slot index (the reference's
+ * std::sort leaves tie order unspecified).  Migration: the j-th best of
+ * island i overwrites the j-th worst of island (i+1) mod NI, j < k (k = 1 is
+ * the reference's "best of i -> worst of i+1").  order_out[i*PI + r] = slot of
+ * rank r in island i, computed before migration.  Requires 2k <= PI. */
+static const double* g_fit_cmp;
+static int cmp_slot(const void* x, const void* y) {
+  const int a = *(const int*)x, b = *(const int*)y;
+  const double fa = g_fit_cmp[a], fb = g_fit_cmp[b];
+  if (fa < fb) return -1;
+  if (fa > fb) return 1;
+  return (a > b) - (a < b);
+}
+SO_EXPORT int so_island_migrate_f32(float* pop, int n, double* fit, int P, int NI, int k,
+                                    int* order_out) {
+  if (NI <= 0 || P % NI) return 1;
+  const int PI = P / NI;
+  if (2 * k > PI) return 2;
+  int* ord = order_out ? order_out : (int*)malloc(sizeof(int) * (size_t)P);
+  for (int i = 0; i < NI; ++i) {
+    for (int r = 0; r < PI; ++r) ord[i * PI + r] = i * PI + r;
+    g_fit_cmp = fit;
+    qsort(ord + i * PI, (size_t)PI, sizeof(int), cmp_slot);
+  }
+  if (k > 0) {
+    for (int i = 0; i < NI; ++i) {
+      const int nx = (i + 1) % NI;
+      for (int j = 0; j < k; ++j) {
+        const int src = ord[i * PI + j], dst = ord[nx * PI + PI - 1 - j];
+        memcpy(pop + (size_t)dst * n, pop + (size_t)src * n, sizeof(float) * (size_t)n);
+      }
+    }
+    /* fitness follows the copied rows */
+    double* f2 = (double*)malloc(sizeof(double) * (size_t)P);
+    memcpy(f2, fit, sizeof(double) * (size_t)P);
+    for (int i = 0; i < NI; ++i) {
+      const int nx = (i + 1) % NI;
+      for (int j = 0; j < k; ++j) f2[ord[nx * PI + PI - 1 - j]] = fit[ord[i * PI + j]];
+    }
+    memcpy(fit, f2, sizeof(double) * (size_t)P);
+    free(f2);
+  }
+  if (!order_out) free(ord);
+  return 0;
+}
+
+/* ============================ exact certification ========================= */
+/* F from EXACT M = max_k b_k and EXACT S = sum a, each rounded once to fp64
+ * (round to nearest even), then F = 2 n M / (S S) in fp64.  Exact b_k comes
+ * from a fixed-point accumulator of 64-bit limbs covering 2^-1216..2^+1088
+ * (every product of two finite doubles above the subnormal range is exact
+ * in it).  Because refinement maps M -> 2M and S -> 2S exactly, this F is
+ * bit-identical before and after a cell split.  No reference counterpart:
+ * the reference's hostF (src/main.cu:95-105) is not split-invariant to the
+ * last bit. */
+#define XLIMBS 36
+#define XLO (-1216)
+typedef struct { uint64_t w[XLIMBS]; } xacc;
+
+static void xacc_add_u64(xacc* A, uint64_t mant, int e) {
+  /* adds mant * 2^e, mant < 2^64, e >= XLO */
+  const int sh = e - XLO;
+  int li = sh >> 6, bo = sh & 63;
+  unsigned __int128 v = (unsigned __int128)mant << bo;
+  uint64_t lo = (uint64_t)v, hi = (uint64_t)(v >> 64);
+  uint64_t old = A->w[li];
+  A->w[li] = old + lo;
+  uint64_t carry = (A->w[li] < old);
+  ++li;
+  while ((hi || carry) && li < XLIMBS) {
+    old = A->w[li];
+    uint64_t t = old + hi;
+    uint64_t c1 = (t < old);
+    uint64_t t2 = t + carry;
+    uint64_t c2 = (t2 < t);
+    A->w[li] = t2;
+    carry = c1 + c2;
+    hi = 0;
+    ++li;
+  }
+}
+static void xacc_add_double(xacc* A, double x) {
+  /* x >= 0 finite */
+  if (x == 0.0) return;
+  int e;
+  const double fr = frexp(x, &e);              /* x = fr * 2^e, fr in [0.5,1) */
+  const uint64_t mant = (uint64_t)ldexp(fr, 53);  /* exact 53-bit integer */
+  xacc_add_u64(A, mant, e - 53);               /* e - 53 >= -1127 > XLO for every double */
+}
+static int xacc_cmp(const xacc* A, const xacc* B) {
+  for (int i = XLIMBS - 1; i >= 0; --i) {
+    if (A->w[i] != B->w[i]) return A->w[i] > B->w[i] ? 1 : -1;
+  }
+  return 0;
+}
+static double xacc_to_double(const xacc* A) {
+  int top = XLIMBS - 1;
+  while (top >= 0 && A->w[top] == 0) --top;
+  if (top < 0) return 0.0;
+  const int lz = __builtin_clzll(A->w[top]);
+  const int msb = top * 64 + (63 - lz);        /* bit index of the leading one */
+  /* take 53 bits [msb-52, msb], round bit msb-53, sticky below */
+  uint64_t mant = 0;
+  for (int bit = msb; bit >= msb - 52; --bit) {
+    mant <<= 1;
+    if (bit >= 0) mant |= (A->w[bit >> 6] >> (bit & 63)) & 1ull;
+  }
+  int rb = 0, sticky = 0;
+  const int rbit = msb - 53;
+  if (rbit >= 0) {
+    const int li = rbit >> 6, bo = rbit & 63;
+    rb = (int)((A->w[li] >> bo) & 1ull);
+    if (bo > 0 && (A->w[li] & ((1ull << bo) - 1ull))) sticky = 1;
+    for (int j = li - 1; j >= 0 && !sticky; --j)
+      if (A->w[j]) sticky = 1;
+  }
+  if (rb && (sticky || (mant & 1ull))) ++mant;
+  return ldexp((double)mant, msb - 52 + XLO);
+}
+
+/* Exact b_k for one k of a double vector: products split by FMA into
+ * p + e with both exact doubles (p = fl(ab), e = fma(a,b,-p)); e may be
+ * negative, so positive and negative parts are accumulated apart. */
+static void exact_bk(const double* a, int n, int k, xacc* pos, xacc* neg) {
+  memset(pos, 0, sizeof(xacc));
+  memset(neg, 0, sizeof(xacc));
+  const int ilo = k - n + 1 > 0 ? k - n + 1 : 0, ihi = k < n - 1 ? k : n - 1;
+  for (int i = ilo; i <= ihi; ++i) {
+    const double x = a[i], y = a[k - i];
+    if (x == 0.0 || y == 0.0) continue;
+    const double p = x * y;
+    const double e = fma(x, y, -p);
+    xacc_add_double(pos, p);
+    if (e > 0) xacc_add_double(pos, e);
+    else if (e < 0) xacc_add_double(neg, -e);
+  }
+}
+static void xacc_sub(xacc* A, const xacc* B) {  /* A -= B, A >= B */
+  uint64_t borrow = 0;
+  for (int i = 0; i < XLIMBS; ++i) {
+    const uint64_t a = A->w[i], b = B->w[i];
+    const uint64_t d = a - b - borrow;
+    borrow = (a < b) || (a - b < borrow);
+    A->w[i] = d;
+  }
+}
+
+SO_EXPORT double so_certify_exact(const double* a, int n, int* kmax_out, double* M_out,
+                                  double* S_out) {
+  xacc best, cur, neg, S;
+  memset(&best, 0, sizeof best);
+  int kbest = 0;
+  for (int k = 0; k < 2 * n - 1; ++k) {
+    exact_bk(a, n, k, &cur, &neg);
+    xacc_sub(&cur, &neg);
+    if (xacc_cmp(&cur, &best) > 0) { best = cur; kbest = k; }
+  }
+  memset(&S, 0, sizeof S);
+  for (int i = 0; i < n; ++i) xacc_add_double(&S, a[i]);
+  const double M = xacc_to_double(&best), Sd = xacc_to_double(&S);
+  if (kmax_out) *kmax_out = kbest;
+  if (M_out) *M_out = M;
+  if (S_out) *S_out = Sd;
+  if (!(Sd > 0.0)) return 1e30;
+  return 2.0 * (double)n * M / (Sd * Sd);
+}
+
+/* exact b_k rounded once, for one k (used by tests of the GPU certifier) */
+SO_EXPORT double so_exact_bk(const double* a, int n, int k) {
+  xacc cur, neg;
+  exact_bk(a, n, k, &cur, &neg);
+  xacc_sub(&cur, &neg);
+  return xacc_to_double(&cur);
+}
+
+SO_EXPORT int so_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}

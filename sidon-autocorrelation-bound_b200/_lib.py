@@ -1,0 +1,90 @@
+"""ctypes binding of ``libsidon_b200.so`` (the C ABI in include/sidon_b200.h).
+
+There is no fallback: if the library is missing or cannot be loaded, every
+entry point raises.  ``load(build=True)`` compiles it first (nvcc, sm_100a).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+import threading
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libsidon_b200.so"
+
+# status codes (enum sidon_status)
+OK, ERR_ARG, ERR_N, ERR_SMEM, ERR_CUDA, ERR_DTYPE, ERR_NONFINITE, ERR_TIMEOUT, ERR_DEVICE = range(9)
+F32, F64 = 0, 1
+PREC_FP32_SIMT, PREC_BF16X1, PREC_BF16X3, PREC_FP64_SIMT = 0, 1, 2, 3
+OP_LOCAL_SEARCH, OP_EVAL, OP_FRANK_WOLFE, OP_LOCAL_SEARCH_TC = 0, 1, 2, 3
+
+_vp, _i, _d, _f, _sz = C.c_void_p, C.c_int, C.c_double, C.c_float, C.c_size_t
+
+# name -> (restype, argtypes); every symbol declared in include/sidon_b200.h
+SIGNATURES = {
+    "sidon_status_string": (C.c_char_p, [_i]),
+    "sidon_last_cuda_error": (_i, []),
+    "sidon_abi_version": (_i, []),
+    "sidon_smem_bytes": (_sz, [_i, _i, _i]),
+    "sidon_max_n": (_i, [_i, _i]),
+    "sidon_hostF": (_d, [_vp, _i]),
+    "sidon_eval": (_i, [_vp, _i, _i, _i, _vp, _vp, _d, _vp]),
+    "sidon_certify": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp]),
+    "sidon_local_search": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _d, _i,
+                                _i, _i, _vp]),
+    "sidon_lp_forward": (_i, [_vp, _i, _i, _d, _vp, _vp, _vp, _i, _vp]),
+    "sidon_lp_backward": (_i, [_vp, _vp, _vp, _i, _i, _d, _vp, _i, _vp]),
+    "sidon_frank_wolfe": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp]),
+    "sidon_refine": (_i, [_vp, _i, _i, _vp, _i, _vp]),
+    "sidon_coarsen": (_i, [_vp, _i, _i, _vp, _i, _vp]),
+    "sidon_island_migrate": (_i, [_vp, _i, _vp, _i, _i, _i, _vp, _vp]),
+}
+
+_lock = threading.Lock()
+_lib: C.CDLL | None = None
+
+
+class SidonError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, fn: str, status: int, cuda_error: int = 0):
+        self.status = status
+        self.cuda_error = cuda_error
+        msg = f"{fn}: {status_string(status)} (status {status})"
+        if status == ERR_CUDA:
+            msg += f", cudaError {cuda_error}"
+        super().__init__(msg)
+
+
+def load(build: bool = False) -> C.CDLL:
+    """Load (optionally building first) the CUDA library; raises if absent."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if build:
+            from . import build as _b
+            _b.build()
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH.name} is not built; run `python sidon-autocorrelation-bound_b200/build.py` "
+                "(no CPU fallback exists for the sidon_b200 kernels)")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def status_string(status: int) -> str:
+    return load().sidon_status_string(status).decode()
+
+
+def call(name: str, *args) -> None:
+    """Invoke an int-returning entry point and raise SidonError on failure."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != OK:
+        raise SidonError(name, rc, lib.sidon_last_cuda_error() if rc == ERR_CUDA else 0)

@@ -1,0 +1,256 @@
+// ---------------------------------------------------------------------------
+//  capi.cu -- the extern "C" boundary (include/sidon_b200.h): argument
+//  checks, status codes, shared-memory sizing, the host fp64 evaluator, and
+//  dispatch to the kernels.  Nothing here allocates device memory.
+// ---------------------------------------------------------------------------
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace sidon_host {
+
+// kernels (defined in the other translation units)
+size_t smem_local_search(int n, int dtype);
+size_t smem_eval(int n);
+size_t smem_fw(int n);
+size_t smem_certify(int n);
+size_t smem_local_search_tc(int n);
+int launch_local_search(void* pop, void* mom, void* vel, const int* skip, const int* mode_arr,
+                        int n, int P, int iters, double pS, double pE, double lrS, double lrE,
+                        double b1, double b2, int mode_default, int dtype, cudaStream_t st);
+int launch_local_search_tc(float* pop, float* mom, float* vel, const int* skip,
+                           const int* mode_arr, int n, int P, int iters, double pS, double pE,
+                           double lrS, double lrE, double b1, double b2, int mode_default,
+                           int precision, cudaStream_t st);
+int launch_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
+                      float* b_out, cudaStream_t st);
+int launch_lp_backward(const float* a, const float* saved, const float* b_in, int n, int P,
+                       double p, float* grad, cudaStream_t st);
+int launch_eval(const void* pop, int dtype, int n, int P, double* outF, int* outN, double tol,
+                cudaStream_t st);
+int launch_certify(const void* pop, int dtype, int n, int P, double* outF, double* outM,
+                   double* outS, int* outK, cudaStream_t st);
+int launch_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int pdhg, int nT,
+                       float tMax, float tau, float sig, cudaStream_t st);
+int launch_refine(const void* src, int n, int P, void* dst, int dtype, cudaStream_t st);
+int launch_coarsen(const void* src, int n2, int P, void* dst, int dtype, cudaStream_t st);
+int launch_island_migrate(float* pop, int n, double* fit, int P, int NI, int k, int* order,
+                          cudaStream_t st);
+
+static thread_local int g_last_cuda = 0;
+
+int set_cuda_error(cudaError_t e) {
+  g_last_cuda = (int)e;
+  return SIDON_ERR_CUDA;
+}
+int check_launch() {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_cuda_error(e);
+  return SIDON_OK;
+}
+int smem_optin() {
+  int dev = 0, v = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  return v;
+}
+int sm_count() {
+  int dev = 0, v = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 1;
+  return v > 0 ? v : 1;
+}
+int device_ok() {
+  int dev = 0, major = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  return major == 10 ? SIDON_OK : SIDON_ERR_DEVICE;
+}
+
+}  // namespace sidon_host
+
+using namespace sidon_host;
+
+namespace {
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+// common precondition checks; returns SIDON_OK or an error
+inline int pre(int n, int P) {
+  if (P < 0) return SIDON_ERR_ARG;
+  if (n < 1) return SIDON_ERR_N;
+  return device_ok();
+}
+}  // namespace
+
+extern "C" {
+
+const char* sidon_status_string(int status) {
+  switch (status) {
+    case SIDON_OK: return "ok";
+    case SIDON_ERR_ARG: return "invalid argument";
+    case SIDON_ERR_N: return "n outside the supported range";
+    case SIDON_ERR_SMEM: return "working set exceeds the shared-memory opt-in";
+    case SIDON_ERR_CUDA: return "CUDA runtime error";
+    case SIDON_ERR_DTYPE: return "dtype/precision not supported by this call";
+    case SIDON_ERR_NONFINITE: return "non-finite or negative heights";
+    case SIDON_ERR_TIMEOUT: return "device-side wait timed out";
+    case SIDON_ERR_DEVICE: return "current device is not sm_100";
+    default: return "unknown status";
+  }
+}
+
+int sidon_last_cuda_error(void) { return g_last_cuda; }
+int sidon_abi_version(void) { return 1; }
+
+size_t sidon_smem_bytes(int op, int n, int dtype) {
+  if (n < 1) return 0;
+  switch (op) {
+    case SIDON_OP_LOCAL_SEARCH: return smem_local_search(n, dtype);
+    case SIDON_OP_EVAL: return (dtype == SIDON_F32 || dtype == SIDON_F64) ? smem_eval(n) : 0;
+    case SIDON_OP_FRANK_WOLFE: return dtype == SIDON_F32 ? smem_fw(n) : 0;
+    case SIDON_OP_LOCAL_SEARCH_TC: return dtype == SIDON_F32 ? smem_local_search_tc(n) : 0;
+    default: return 0;
+  }
+}
+
+int sidon_max_n(int op, int dtype) {
+  const long long cap = smem_optin();
+  if (cap <= 0) return 0;
+  int lo = 0, hi = 1 << 22;
+  while (lo < hi) {                       // largest n with smem(n) <= cap (monotone in n)
+    const int mid = lo + (hi - lo + 1) / 2;
+    const size_t need = sidon_smem_bytes(op, mid, dtype);
+    if (need != 0 && (long long)need <= cap) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+double sidon_hostF(const double* a, int n) {
+  if (!a || n < 1) return NAN;
+  std::vector<double> b(2 * (size_t)n - 1, 0.0);
+  for (int i = 0; i < n; ++i) {
+    if (a[i] == 0.0) continue;
+    const double ai = a[i];
+    for (int j = 0; j < n; ++j) {
+      volatile double prod = ai * a[j];   // rounded product, then rounded sum
+      b[i + j] += prod;
+    }
+  }
+  double M = 0.0;
+  for (double x : b) M = x > M ? x : M;
+  double Ssum = 0.0;
+  for (int i = 0; i < n; ++i) Ssum += a[i];
+  return 2.0 * n * M / (Ssum * Ssum);
+}
+
+int sidon_eval(const void* pop, int dtype, int n, int P, double* out_F, int* out_nactive,
+               double active_tol, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!pop || !out_F) return SIDON_ERR_ARG;
+  if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
+  return launch_eval(pop, dtype, n, P, out_F, out_nactive, active_tol, S(stream));
+}
+
+int sidon_certify(const void* pop, int dtype, int n, int P, double* out_F, double* out_M,
+                  double* out_S, int* out_kmax, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!pop || !out_F) return SIDON_ERR_ARG;
+  if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
+  return launch_certify(pop, dtype, n, P, out_F, out_M, out_S, out_kmax, S(stream));
+}
+
+int sidon_local_search(void* pop, void* mom, void* vel, const int* skip, const int* mode_arr,
+                       int n, int P, int iters, double p_start, double p_end, double lr_start,
+                       double lr_end, double beta1, double beta2, int mode_default, int dtype,
+                       int precision, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0 || iters <= 0) return SIDON_OK;
+  if (!pop || !mom || !vel) return SIDON_ERR_ARG;
+  if (!(p_start > 0.0) || !(p_end > 0.0) || !(lr_start > 0.0) || !(lr_end > 0.0))
+    return SIDON_ERR_ARG;
+  if (dtype == SIDON_F32) {
+    if (precision == SIDON_PREC_FP32_SIMT)
+      return launch_local_search(pop, mom, vel, skip, mode_arr, n, P, iters, p_start, p_end,
+                                 lr_start, lr_end, beta1, beta2, mode_default, dtype, S(stream));
+    if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
+      return launch_local_search_tc((float*)pop, (float*)mom, (float*)vel, skip, mode_arr, n, P,
+                                    iters, p_start, p_end, lr_start, lr_end, beta1, beta2,
+                                    mode_default, precision, S(stream));
+    return SIDON_ERR_DTYPE;
+  }
+  if (dtype == SIDON_F64 && precision == SIDON_PREC_FP64_SIMT)
+    return launch_local_search(pop, mom, vel, skip, mode_arr, n, P, iters, p_start, p_end,
+                               lr_start, lr_end, beta1, beta2, mode_default, dtype, S(stream));
+  return SIDON_ERR_DTYPE;
+}
+
+int sidon_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
+                     float* b_out, int precision, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!a || !value || !saved || !(p >= 1.0)) return SIDON_ERR_ARG;
+  if (precision != SIDON_PREC_FP32_SIMT) return SIDON_ERR_DTYPE;
+  return launch_lp_forward(a, n, P, p, value, saved, b_out, S(stream));
+}
+
+int sidon_lp_backward(const float* a, const float* saved, const float* b_in, int n, int P,
+                      double p, float* grad, int precision, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!a || !saved || !grad || !(p >= 1.0)) return SIDON_ERR_ARG;
+  if (precision != SIDON_PREC_FP32_SIMT) return SIDON_ERR_DTYPE;
+  return launch_lp_backward(a, saved, b_in, n, P, p, grad, S(stream));
+}
+
+int sidon_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int pdhg_iters,
+                      int nT, float t_max, float tau, float sigma, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0 || rounds <= 0) return SIDON_OK;
+  if (!pop || pdhg_iters < 0 || nT < 1 || !(t_max > 0.f) || !(t_max <= 1.f)) return SIDON_ERR_ARG;
+  return launch_frank_wolfe(pop, skip, n, P, rounds, pdhg_iters, nT, t_max, tau, sigma, S(stream));
+}
+
+int sidon_refine(const void* src, int n, int P, void* dst, int dtype, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!src || !dst || src == dst) return SIDON_ERR_ARG;
+  if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
+  return launch_refine(src, n, P, dst, dtype, S(stream));
+}
+
+int sidon_coarsen(const void* src, int n2, int P, void* dst, int dtype, void* stream) {
+  int rc = pre(n2, P);
+  if (rc) return rc;
+  if (n2 % 2) return SIDON_ERR_N;
+  if (P == 0) return SIDON_OK;
+  if (!src || !dst || src == dst) return SIDON_ERR_ARG;
+  if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
+  return launch_coarsen(src, n2, P, dst, dtype, S(stream));
+}
+
+int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, int k_migrate,
+                         int* order_out, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!pop || !fit || !order_out || n_islands < 1 || k_migrate < 0) return SIDON_ERR_ARG;
+  if (P % n_islands) return SIDON_ERR_ARG;
+  const int PI = P / n_islands;
+  if (PI > 1024 || 2 * k_migrate > PI) return SIDON_ERR_ARG;
+  return launch_island_migrate(pop, n, fit, P, n_islands, k_migrate, order_out, S(stream));
+}
+
+}  // extern "C"

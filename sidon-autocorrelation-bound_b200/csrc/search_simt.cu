@@ -1,0 +1,436 @@
+// ---------------------------------------------------------------------------
+//  search_simt.cu -- CUDA-core kernels of the hot path:
+//    k_local_search   L^p-annealed projected Adam / mirror descent
+//                     (src/kernels.cuh:177-289), fp32 and fp64
+//    k_lp_forward     G_p(a) = 2n ||a*a||_p / S^2 and the saved {M, S, R}
+//    k_lp_backward    dG_p/da with b recomputed (or read back)
+//    k_eval           certifying fp64 F + active-peak count
+//                     (src/kernels.cuh:301-377, hostF arithmetic)
+//    k_frank_wolfe    Chambolle-Pock Frank-Wolfe step (src/kernels.cuh:408-532)
+//
+//  One CTA per candidate.  Shared memory (T = element type, MG = margin):
+//    sA [MG | n | MG]        heights (window + broadcast operand)
+//    sC [MG | 2n-1 | MG]     b, then the weights c (correlation window)
+//    sRed[32]                reduction scratch
+// ---------------------------------------------------------------------------
+#include "conv_simt.cuh"
+
+namespace sidon {
+
+template <typename T, int TK>
+__host__ __device__ constexpr size_t ls_smem_elems(int n) {
+  return (size_t)(n + 2 * margin<TK>()) + (size_t)(2 * n - 1 + 2 * margin<TK>()) + 32;
+}
+
+template <typename T>
+__device__ __forceinline__ void zero_fill(T* p, int count) {
+  for (int i = threadIdx.x; i < count; i += blockDim.x) p[i] = T(0);
+}
+
+// ------------------------------ local search ------------------------------
+template <typename T, int TK>
+__global__ void __launch_bounds__(1024, 1)
+k_local_search(T* pop, T* mom, T* vel, const int* __restrict__ skip,
+               const int* __restrict__ mode_arr, int n, int iters, T pStart, T pEnd, T lrStart,
+               T lrEnd, T beta1, T beta2, int mode_default) {
+  constexpr int MG = margin<TK>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* base = reinterpret_cast<T*>(smem_raw);
+  T* sA = base + MG;                        // [-MG, n + MG)
+  T* sC = base + (n + 2 * MG) + MG;         // [-MG, 2n - 1 + MG)
+  T* sRed = base + (n + 2 * MG) + (2 * n - 1 + 2 * MG);
+
+  const int pid = blockIdx.x;
+  if (skip && skip[pid]) return;
+  const int mode = mode_arr ? mode_arr[pid] : mode_default;
+  T* a = pop + (size_t)pid * n;
+  T* m = mom + (size_t)pid * n;
+  T* v = vel + (size_t)pid * n;
+  const int nb = 2 * n - 1;
+
+  zero_fill(base, (int)ls_smem_elems<T, TK>(n));
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) { sA[i] = a[i]; m[i] = T(0); v[i] = T(0); }
+  __syncthreads();
+
+  const T lnPr = T(log(double(pEnd) / double(pStart)));
+  const T lnLr = T(log(double(lrEnd) / double(lrStart)));
+  T b1t = T(1), b2t = T(1);
+
+  for (int it = 0; it < iters; ++it) {
+    const T frac = iters > 1 ? T(it) / T(iters - 1) : T(0);
+    const T pexp = pStart * dev_exp(lnPr * frac);
+    const T lr = lrStart * dev_exp(lnLr * frac);
+
+    // b = a * a, and the running max in the same pass
+    T mloc = T(0);
+    conv_warp_tiles<TK, true>(sA, sA, n, [&](int k, T val) {
+      sC[k] = val;
+      mloc = val > mloc ? val : mloc;
+    });
+    const T M = block_max(mloc, sRed);      // (barrier inside: sC complete)
+    if (!(M > T(0))) break;
+
+    // c_k = (1+d)^(p-1), R = sum c_k (1+d), d = (b_k - M)/M
+    T rloc = T(0);
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+      const T d = (sC[k] - M) / M;
+      const T cw = d > T(-1) ? pow_from_d(d, pexp - T(1)) : T(0);
+      rloc += cw * (T(1) + d);
+      sC[k] = cw;
+    }
+    const T R = block_sum(rloc, sRed);      // (barrier inside: c complete)
+
+    b1t *= beta1;
+    b2t *= beta2;
+    const T bc1 = T(1) / (T(1) - b1t), bc2 = T(1) / (T(1) - b2t);
+    const T lrn = lr / T(n);
+
+    // G = corr(c, a); update fused into the epilogue; the new heights are
+    // staged in the candidate's own row of pop (sA is still being read).
+    corr_warp_tiles<TK>(sA, sC, n, [&](int i, T G) {
+      const T gi = G / R - M;
+      T x;
+      if (mode == 0) {
+        const T mm = dev_fma(beta1, m[i], (T(1) - beta1) * gi);
+        const T vv = dev_fma(beta2, v[i], (T(1) - beta2) * gi * gi);
+        m[i] = mm;
+        v[i] = vv;
+        const T step = lrn * (mm * bc1) / (dev_sqrt(vv * bc2) + T(1e-30));
+        x = sA[i] - step;
+        if (x < T(0)) x = T(0);
+      } else {
+        T e = -lr * (gi / M);
+        if (e > T(4)) e = T(4);
+        if (e < T(-4)) e = T(-4);
+        x = sA[i] * dev_exp(e);
+      }
+      a[i] = x;
+    });
+    __syncthreads();
+
+    T sloc = T(0);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const T x = a[i];
+      sA[i] = x;
+      sloc += x;
+    }
+    T S = block_sum(sloc, sRed);
+    if (!(S > T(0))) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = T(1) / T(n);
+      S = T(1);
+    }
+    const T inv = T(1) / S;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] *= inv;
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = sA[i];
+}
+
+// ----------------------------- G_p forward --------------------------------
+// value = 2n M R^(1/p) / S^2 with M = max b, R = sum (b/M)^p, S = sum a.
+template <int TK>
+__global__ void __launch_bounds__(1024, 1)
+k_lp_forward(const float* __restrict__ pop, int n, float p, float* __restrict__ value,
+             float* __restrict__ saved, float* __restrict__ b_out) {
+  constexpr int MG = margin<TK>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* base = reinterpret_cast<float*>(smem_raw);
+  float* sA = base + MG;
+  float* sC = base + (n + 2 * MG) + MG;
+  float* sRed = base + (n + 2 * MG) + (2 * n - 1 + 2 * MG);
+  const int pid = blockIdx.x;
+  const float* a = pop + (size_t)pid * n;
+  const int nb = 2 * n - 1;
+  zero_fill(base, (int)ls_smem_elems<float, TK>(n));
+  __syncthreads();
+  float sl = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; sA[i] = x; sl += x; }
+  const float S = block_sum(sl, sRed);
+  float mloc = 0.f;
+  conv_warp_tiles<TK, true>(sA, sA, n, [&](int k, float val) {
+    sC[k] = val;
+    mloc = val > mloc ? val : mloc;
+  });
+  const float M = block_max(mloc, sRed);
+  float rloc = 0.f;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    const float d = (sC[k] - M) / M;
+    rloc += d > -1.f ? pow_from_d(d, p) : 0.f;
+    if (b_out) b_out[(size_t)pid * nb + k] = sC[k];
+  }
+  const float R = block_sum(rloc, sRed);
+  if (threadIdx.x == 0) {
+    const float val = 2.f * (float)n * M * powf(R, 1.f / p) / (S * S);
+    value[pid] = val;
+    saved[4 * pid + 0] = M;
+    saved[4 * pid + 1] = S;
+    saved[4 * pid + 2] = R;
+    saved[4 * pid + 3] = val;
+  }
+}
+
+// ----------------------------- G_p backward -------------------------------
+// grad_i = (4n R^(1/p)/S^2) (G_i/R - M/S),  G_i = sum_j (b_{i+j}/M)^(p-1) a_j
+template <int TK>
+__global__ void __launch_bounds__(1024, 1)
+k_lp_backward(const float* __restrict__ pop, const float* __restrict__ saved,
+              const float* __restrict__ b_in, int n, float p, float* __restrict__ grad) {
+  constexpr int MG = margin<TK>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* base = reinterpret_cast<float*>(smem_raw);
+  float* sA = base + MG;
+  float* sC = base + (n + 2 * MG) + MG;
+  const int pid = blockIdx.x;
+  const float* a = pop + (size_t)pid * n;
+  const int nb = 2 * n - 1;
+  const float M = saved[4 * pid + 0], S = saved[4 * pid + 1], R = saved[4 * pid + 2];
+  zero_fill(base, (int)ls_smem_elems<float, TK>(n));
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = a[i];
+  __syncthreads();
+  if (b_in) {
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) sC[k] = b_in[(size_t)pid * nb + k];
+  } else {
+    conv_warp_tiles<TK, true>(sA, sA, n, [&](int k, float val) { sC[k] = val; });
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    const float d = (sC[k] - M) / M;
+    sC[k] = d > -1.f ? pow_from_d(d, p - 1.f) : 0.f;
+  }
+  __syncthreads();
+  const float scale = 4.f * (float)n * powf(R, 1.f / p) / (S * S);
+  const float MS = M / S;
+  float* g = grad + (size_t)pid * n;
+  corr_warp_tiles<TK>(sA, sC, n, [&](int i, float G) { g[i] = scale * (G / R - MS); });
+}
+
+// ---------------------------- certifying eval -----------------------------
+// fp64, hostF arithmetic: b_k = sum_i fl(a_i a_{k-i}) added in i order;
+// S = sequential sum in i order; F = 2 n M / (S S) (src/main.cu:95-105).
+// nActive = #{k : b_k >= M (1 - tol)} by a second pass (src/kernels.cuh:347-375).
+template <typename Tin, int TK>
+__global__ void __launch_bounds__(1024, 1)
+k_eval(const Tin* __restrict__ pop, int n, double* __restrict__ outF, int* __restrict__ outN,
+       double tol) {
+  constexpr int MG = margin<TK>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* base = reinterpret_cast<double*>(smem_raw);
+  double* sA = base + MG;
+  double* sRed = base + (n + 2 * MG);
+  __shared__ double sS;
+  const int pid = blockIdx.x;
+  const Tin* a = pop + (size_t)pid * n;
+  zero_fill(base, n + 2 * MG);
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = (double)a[i];
+  __syncthreads();
+  double mloc = 0.0;
+  conv_warp_tiles<TK, false>(sA, sA, n, [&](int, double val) { mloc = val > mloc ? val : mloc; });
+  if (threadIdx.x == 0) {
+    double S = 0.0;
+    for (int i = 0; i < n; ++i) S = __dadd_rn(S, sA[i]);
+    sS = S;
+  }
+  const double M = block_max(mloc, sRed);
+  const double S = sS;
+  if (outN) {
+    const double thr = M * (1.0 - tol);
+    double cl = 0.0;
+    conv_warp_tiles<TK, false>(sA, sA, n, [&](int, double val) { cl += (val >= thr) ? 1.0 : 0.0; });
+    const double cnt = block_sum(cl, sRed);
+    if (threadIdx.x == 0) outN[pid] = (int)(cnt + 0.5);
+  }
+  if (threadIdx.x == 0) outF[pid] = (S > 0.0) ? (2.0 * (double)n * M / (S * S)) : 1e30;
+}
+
+// --------------------------- Frank-Wolfe / PDHG ---------------------------
+// sA [MG|n|MG] heights, sG [n] g, sGb [MG|n|MG] gbar / line-search point,
+// sL [MG|2n-1|MG] lambda, sRed[32].
+template <int TK>
+__host__ __device__ constexpr size_t fw_smem_elems(int n) {
+  return (size_t)(n + 2 * margin<TK>()) * 2 + (size_t)n + (size_t)(2 * n - 1 + 2 * margin<TK>()) +
+         32;
+}
+
+template <int TK>
+__global__ void __launch_bounds__(1024, 1)
+k_frank_wolfe(float* pop, const int* __restrict__ skip, int n, int rounds, int pdhgIters, int nT,
+              float tMax, float tau, float sig) {
+  constexpr int MG = margin<TK>();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* base = reinterpret_cast<float*>(smem_raw);
+  float* sA = base + MG;
+  float* sGb = base + (n + 2 * MG) + MG;
+  float* sG = base + 2 * (n + 2 * MG);
+  float* sL = sG + n + MG;
+  float* sRed = sG + n + (2 * n - 1 + 2 * MG);
+  const int pid = blockIdx.x;
+  if (skip && skip[pid]) return;
+  float* a = pop + (size_t)pid * n;
+  const int nb = 2 * n - 1;
+  zero_fill(base, (int)fw_smem_elems<TK>(n));
+  __syncthreads();
+  float sl = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; sA[i] = x; sl += x; }
+  const float s0 = block_sum(sl, sRed);
+  if (!(s0 > 0.f)) return;
+  {
+    const float inv = 1.f / s0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] *= inv;
+    __syncthreads();
+  }
+  if (!(tau > 0.f)) tau = 0.9f / (float)n;
+  if (!(sig > 0.f)) sig = 0.9f * (float)n;
+
+  for (int r = 0; r < rounds; ++r) {
+    float ml = 0.f;
+    conv_warp_tiles<TK, true>(sA, sA, n, [&](int, float val) { ml = val > ml ? val : ml; });
+    const float M = block_max(ml, sRed);
+    if (!(M > 0.f)) break;
+
+    for (int i = threadIdx.x; i < n; i += blockDim.x) { sG[i] = sA[i]; sGb[i] = sA[i]; }
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) sL[k] = 0.f;
+    __syncthreads();
+
+    for (int it = 0; it < pdhgIters; ++it) {
+      // lambda <- [lambda + sigma (a * gbar - M)]_+   (conv fused)
+      conv_warp_tiles<TK, true>(sA, sGb, n, [&](int k, float val) {
+        const float l = sL[k] + sig * (val - M);
+        sL[k] = l > 0.f ? l : 0.f;
+      });
+      __syncthreads();
+      // g_new <- [g + tau (1 - A^T lambda)]_+  parked in gbar
+      corr_warp_tiles<TK>(sA, sL, n, [&](int i, float cv) {
+        const float gn = sG[i] + tau * (1.f - cv);
+        sGb[i] = gn > 0.f ? gn : 0.f;
+      });
+      __syncthreads();
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float gn = sGb[i], go = sG[i];
+        sG[i] = gn;
+        sGb[i] = 2.f * gn - go;
+      }
+      __syncthreads();
+    }
+
+    float sg = 0.f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sg += sG[i];
+    sg = block_sum(sg, sRed);
+    if (!(sg > 0.f)) break;
+    {
+      const float inv = 1.f / sg;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) sG[i] *= inv;
+      __syncthreads();
+    }
+    // sum a = sum g = 1  =>  F(h) = 2n max(h*h) for every t
+    float bestT = 0.f, bestM = M;
+    for (int s = 1; s <= nT; ++s) {
+      const float t = tMax * (float)s / (float)nT;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) sGb[i] = (1.f - t) * sA[i] + t * sG[i];
+      __syncthreads();
+      float lc = 0.f;
+      conv_warp_tiles<TK, true>(sGb, sGb, n, [&](int, float val) { lc = val > lc ? val : lc; });
+      const float mm = block_max(lc, sRed);
+      if (mm < bestM) { bestM = mm; bestT = t; }
+    }
+    if (!(bestT > 0.f)) break;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = (1.f - bestT) * sA[i] + bestT * sG[i];
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = sA[i];
+}
+
+}  // namespace sidon
+
+// =========================== host launch wrappers ==========================
+namespace sidon_host {
+using namespace sidon;
+
+constexpr int kTK32 = 15;   // outputs per lane, fp32 kernels (odd: conflict-free windows)
+constexpr int kTK64 = 7;    // outputs per lane, fp64 kernels
+
+size_t smem_local_search(int n, int dtype) {
+  if (dtype == SIDON_F32) return sizeof(float) * ls_smem_elems<float, kTK32>(n);
+  if (dtype == SIDON_F64) return sizeof(double) * ls_smem_elems<double, kTK64>(n);
+  return 0;
+}
+size_t smem_eval(int n) { return sizeof(double) * ((size_t)n + 2 * margin<kTK64>() + 32); }
+size_t smem_fw(int n) { return sizeof(float) * fw_smem_elems<kTK32>(n); }
+
+static int prep(const void* fn, size_t smem) {
+  if ((long long)smem > (long long)smem_optin()) return SIDON_ERR_SMEM;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  return SIDON_OK;
+}
+
+int launch_local_search(void* pop, void* mom, void* vel, const int* skip, const int* mode_arr,
+                        int n, int P, int iters, double pS, double pE, double lrS, double lrE,
+                        double b1, double b2, int mode_default, int dtype, cudaStream_t st) {
+  if (dtype == SIDON_F32) {
+    const size_t sm = smem_local_search(n, dtype);
+    const void* fn = (const void*)k_local_search<float, kTK32>;
+    int rc = prep(fn, sm);
+    if (rc) return rc;
+    k_local_search<float, kTK32><<<P, 32 * warps_for<kTK32>(n), sm, st>>>(
+        (float*)pop, (float*)mom, (float*)vel, skip, mode_arr, n, iters, (float)pS, (float)pE,
+        (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default);
+  } else {
+    const size_t sm = smem_local_search(n, dtype);
+    const void* fn = (const void*)k_local_search<double, kTK64>;
+    int rc = prep(fn, sm);
+    if (rc) return rc;
+    k_local_search<double, kTK64><<<P, 32 * warps_for<kTK64>(n), sm, st>>>(
+        (double*)pop, (double*)mom, (double*)vel, skip, mode_arr, n, iters, pS, pE, lrS, lrE, b1,
+        b2, mode_default);
+  }
+  return check_launch();
+}
+
+int launch_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
+                      float* b_out, cudaStream_t st) {
+  const size_t sm = smem_local_search(n, SIDON_F32);
+  int rc = prep((const void*)k_lp_forward<kTK32>, sm);
+  if (rc) return rc;
+  k_lp_forward<kTK32><<<P, 32 * warps_for<kTK32>(n), sm, st>>>(a, n, (float)p, value, saved, b_out);
+  return check_launch();
+}
+
+int launch_lp_backward(const float* a, const float* saved, const float* b_in, int n, int P,
+                       double p, float* grad, cudaStream_t st) {
+  const size_t sm = smem_local_search(n, SIDON_F32);
+  int rc = prep((const void*)k_lp_backward<kTK32>, sm);
+  if (rc) return rc;
+  k_lp_backward<kTK32><<<P, 32 * warps_for<kTK32>(n), sm, st>>>(a, saved, b_in, n, (float)p, grad);
+  return check_launch();
+}
+
+int launch_eval(const void* pop, int dtype, int n, int P, double* outF, int* outN, double tol,
+                cudaStream_t st) {
+  const size_t sm = smem_eval(n);
+  const int threads = 32 * warps_for<kTK64>(n);
+  if (dtype == SIDON_F32) {
+    int rc = prep((const void*)k_eval<float, kTK64>, sm);
+    if (rc) return rc;
+    k_eval<float, kTK64><<<P, threads, sm, st>>>((const float*)pop, n, outF, outN, tol);
+  } else {
+    int rc = prep((const void*)k_eval<double, kTK64>, sm);
+    if (rc) return rc;
+    k_eval<double, kTK64><<<P, threads, sm, st>>>((const double*)pop, n, outF, outN, tol);
+  }
+  return check_launch();
+}
+
+int launch_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int pdhg, int nT,
+                       float tMax, float tau, float sig, cudaStream_t st) {
+  const size_t sm = smem_fw(n);
+  int rc = prep((const void*)k_frank_wolfe<kTK32>, sm);
+  if (rc) return rc;
+  k_frank_wolfe<kTK32><<<P, 32 * warps_for<kTK32>(n), sm, st>>>(pop, skip, n, rounds, pdhg, nT,
+                                                                 tMax, tau, sig);
+  return check_launch();
+}
+
+}  // namespace sidon_host

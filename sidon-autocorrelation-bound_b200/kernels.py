@@ -1,0 +1,220 @@
+"""Host-side mirror of the reference operator surface (src/kernels.cuh plus
+the launch helpers and hostF of src/main.cu) over the C ABI.
+
+Tensors are torch CUDA tensors (device memory and streams only); every call
+goes through libsidon_b200.so.  Names and argument meaning follow the
+reference: ``local_search_smem`` <-> ``localSearchSmem<T>``,
+``run_local_search`` <-> ``runLocalSearch``, ``run_eval`` <-> ``runEval``,
+``run_frank_wolfe`` <-> ``runFrankWolfe``, ``host_f`` <-> ``hostF``.  Where
+the reference aborts the process (``CUDA_OK``, src/kernels.cuh:20-28) these
+raise ``SidonError``; where ``runFrankWolfe`` returns false
+(src/main.cu:173) ``run_frank_wolfe`` returns False.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import SidonError
+
+PRECISIONS = {
+    "fp32": _lib.PREC_FP32_SIMT,
+    "bf16x1": _lib.PREC_BF16X1,
+    "bf16x3": _lib.PREC_BF16X3,
+    "fp64": _lib.PREC_FP64_SIMT,
+}
+
+
+def _dtype_code(t: torch.Tensor) -> int:
+    if t.dtype == torch.float32:
+        return _lib.F32
+    if t.dtype == torch.float64:
+        return _lib.F64
+    raise TypeError(f"heights must be float32 or float64, got {t.dtype}")
+
+
+def _dev(t: torch.Tensor, name: str, dtype=None) -> int:
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    return t.data_ptr()
+
+
+def _opt(t, name, dtype=None) -> int | None:
+    return None if t is None else _dev(t, name, dtype)
+
+
+def _stream(stream) -> int | None:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream or None
+
+
+def _pop_shape(pop: torch.Tensor) -> tuple[int, int]:
+    if pop.dim() != 2:
+        raise ValueError("population must be [P, n]")
+    return pop.shape[1], pop.shape[0]
+
+
+# ------------------------------ smem sizers --------------------------------
+def local_search_smem(n: int, dtype=torch.float32, precision: str | None = None) -> int:
+    """Bytes of dynamic shared memory per candidate (src/kernels.cuh:161-162)."""
+    if precision in ("bf16x1", "bf16x3"):
+        return _lib.load().sidon_smem_bytes(_lib.OP_LOCAL_SEARCH_TC, n, _lib.F32)
+    code = _lib.F32 if dtype == torch.float32 else _lib.F64
+    return _lib.load().sidon_smem_bytes(_lib.OP_LOCAL_SEARCH, n, code)
+
+
+def eval_smem(n: int) -> int:
+    """src/kernels.cuh:379-380 (evalSmem<double>)."""
+    return _lib.load().sidon_smem_bytes(_lib.OP_EVAL, n, _lib.F64)
+
+
+def fw_smem(n: int) -> int:
+    """src/kernels.cuh:405-406 (fwSmem<float>)."""
+    return _lib.load().sidon_smem_bytes(_lib.OP_FRANK_WOLFE, n, _lib.F32)
+
+
+def max_n(op: int, dtype_code: int = _lib.F32) -> int:
+    return _lib.load().sidon_max_n(op, dtype_code)
+
+
+# ------------------------------ host oracle --------------------------------
+def host_f(a) -> float:
+    """fp64 F on the host, bit-identical to hostF (src/main.cu:95-105)."""
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    return _lib.load().sidon_hostF(arr.ctypes.data, arr.size)
+
+
+# ------------------------------ operators ----------------------------------
+def run_local_search(pop: torch.Tensor, iters: int, p_start: float, p_end: float,
+                     lr_start: float, lr_end: float, mode_arr: torch.Tensor | None = None,
+                     skip: torch.Tensor | None = None, mom: torch.Tensor | None = None,
+                     vel: torch.Tensor | None = None, beta1: float = 0.9, beta2: float = 0.999,
+                     mode_default: int = 0, precision: str | None = None, stream=None) -> None:
+    """L^p-annealed projected Adam / mirror descent on every non-skipped
+    candidate, in place (kLocalSearch + runLocalSearch,
+    src/kernels.cuh:177-289, src/main.cu:152-159)."""
+    n, P = _pop_shape(pop)
+    code = _dtype_code(pop)
+    if precision is None:
+        precision = "fp32" if code == _lib.F32 else "fp64"
+    if mom is None:
+        mom = torch.empty_like(pop)
+    if vel is None:
+        vel = torch.empty_like(pop)
+    _lib.call("sidon_local_search", _dev(pop, "pop"), _dev(mom, "mom", pop.dtype),
+              _dev(vel, "vel", pop.dtype), _opt(skip, "skip", torch.int32),
+              _opt(mode_arr, "mode_arr", torch.int32), n, P, int(iters), float(p_start),
+              float(p_end), float(lr_start), float(lr_end), float(beta1), float(beta2),
+              int(mode_default), code, PRECISIONS[precision], _stream(stream))
+
+
+def run_eval(pop: torch.Tensor, active_tol: float = 1e-4, with_nactive: bool = True,
+             out_F: torch.Tensor | None = None, out_nactive: torch.Tensor | None = None,
+             stream=None):
+    """Certifying fp64 F per candidate (+ active-peak counts) (kEval + runEval,
+    src/kernels.cuh:301-377, src/main.cu:161-166).  Returns (F, nactive|None)."""
+    n, P = _pop_shape(pop)
+    code = _dtype_code(pop)
+    if out_F is None:
+        out_F = torch.empty(P, dtype=torch.float64, device=pop.device)
+    if with_nactive and out_nactive is None:
+        out_nactive = torch.empty(P, dtype=torch.int32, device=pop.device)
+    _lib.call("sidon_eval", _dev(pop, "pop"), code, n, P, _dev(out_F, "out_F", torch.float64),
+              _opt(out_nactive if with_nactive else None, "out_nactive", torch.int32),
+              float(active_tol), _stream(stream))
+    return out_F, (out_nactive if with_nactive else None)
+
+
+def certify(pop: torch.Tensor, stream=None):
+    """Exact certification (F, M, S, argmax k) per candidate; F is split-invariant."""
+    n, P = _pop_shape(pop)
+    code = _dtype_code(pop)
+    dev = pop.device
+    F = torch.empty(P, dtype=torch.float64, device=dev)
+    M = torch.empty(P, dtype=torch.float64, device=dev)
+    S = torch.empty(P, dtype=torch.float64, device=dev)
+    K = torch.empty(P, dtype=torch.int32, device=dev)
+    _lib.call("sidon_certify", _dev(pop, "pop"), code, n, P, F.data_ptr(), M.data_ptr(),
+              S.data_ptr(), K.data_ptr(), _stream(stream))
+    return F, M, S, K
+
+
+def run_frank_wolfe(pop: torch.Tensor, rounds: int, pdhg_iters: int, nT: int = 12,
+                    t_max: float = 0.30, skip: torch.Tensor | None = None, tau: float = 0.0,
+                    sigma: float = 0.0, stream=None) -> bool:
+    """Chambolle-Pock Frank-Wolfe step in place (kFrankWolfe + runFrankWolfe,
+    src/kernels.cuh:408-532, src/main.cu:170-178).  Returns False when the
+    candidate does not fit shared memory, like the reference."""
+    n, P = _pop_shape(pop)
+    try:
+        _lib.call("sidon_frank_wolfe", _dev(pop, "pop", torch.float32),
+                  _opt(skip, "skip", torch.int32), n, P, int(rounds), int(pdhg_iters), int(nT),
+                  float(t_max), float(tau), float(sigma), _stream(stream))
+    except SidonError as e:
+        if e.status == _lib.ERR_SMEM:
+            return False
+        raise
+    return True
+
+
+def refine(pop: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """n -> 2n cell split (kRefine, src/kernels.cuh:538-547)."""
+    n, P = _pop_shape(pop)
+    if out is None:
+        out = torch.empty((P, 2 * n), dtype=pop.dtype, device=pop.device)
+    _lib.call("sidon_refine", _dev(pop, "pop"), n, P, _dev(out, "out", pop.dtype),
+              _dtype_code(pop), _stream(stream))
+    return out
+
+
+def coarsen(pop: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """2n -> n pairwise average (kCoarsen, src/kernels.cuh:550-557)."""
+    n2, P = _pop_shape(pop)
+    if out is None:
+        out = torch.empty((P, n2 // 2), dtype=pop.dtype, device=pop.device)
+    _lib.call("sidon_coarsen", _dev(pop, "pop"), n2, P, _dev(out, "out", pop.dtype),
+              _dtype_code(pop), _stream(stream))
+    return out
+
+
+def lp_forward(a: torch.Tensor, p: float, store_b: bool = False, precision: str = "fp32",
+               stream=None):
+    """G_p(a) = 2n ||a*a||_p / (sum a)^2 per row.  Returns (value, saved, b|None)."""
+    n, P = _pop_shape(a)
+    dev = a.device
+    value = torch.empty(P, dtype=torch.float32, device=dev)
+    saved = torch.empty((P, 4), dtype=torch.float32, device=dev)
+    b = torch.empty((P, 2 * n - 1), dtype=torch.float32, device=dev) if store_b else None
+    _lib.call("sidon_lp_forward", _dev(a, "a", torch.float32), n, P, float(p), value.data_ptr(),
+              saved.data_ptr(), None if b is None else b.data_ptr(), PRECISIONS[precision],
+              _stream(stream))
+    return value, saved, b
+
+
+def lp_backward(a: torch.Tensor, saved: torch.Tensor, p: float, b: torch.Tensor | None = None,
+                precision: str = "fp32", stream=None) -> torch.Tensor:
+    """dG_p/da per row; b recomputed from a unless a stored b is given."""
+    n, P = _pop_shape(a)
+    grad = torch.empty_like(a)
+    _lib.call("sidon_lp_backward", _dev(a, "a", torch.float32), _dev(saved, "saved", torch.float32),
+              _opt(b, "b", torch.float32), n, P, float(p), grad.data_ptr(), PRECISIONS[precision],
+              _stream(stream))
+    return grad
+
+
+def island_migrate(pop: torch.Tensor, fit: torch.Tensor, n_islands: int, k: int = 1,
+                   order: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """Rank each island by fit and migrate best-of-i over worst-of-(i+1)
+    (src/main.cu:676-692), in place on pop and fit.  Returns the ranking."""
+    n, P = _pop_shape(pop)
+    if order is None:
+        order = torch.empty(P, dtype=torch.int32, device=pop.device)
+    _lib.call("sidon_island_migrate", _dev(pop, "pop", torch.float32), n,
+              _dev(fit, "fit", torch.float64), P, int(n_islands), int(k),
+              _dev(order, "order", torch.int32), _stream(stream))
+    return order

@@ -1,0 +1,107 @@
+"""The C-ABI library loads and exports every symbol include/sidon_b200.h
+declares; host-only entry points work without a GPU.  CPU only (no kernel
+launches)."""
+import ctypes
+import pathlib
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "sidon_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sidon_[A-Za-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for must in ("sidon_hostF", "sidon_eval", "sidon_local_search", "sidon_frank_wolfe",
+                 "sidon_refine", "sidon_island_migrate", "sidon_lp_forward", "sidon_lp_backward",
+                 "sidon_certify", "sidon_smem_bytes"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    import sidon_b200._lib as L
+    so = pathlib.Path(L.LIB_PATH)
+    out = subprocess.run(["nm", "-D", "--defined-only", str(so)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    for name in declared_functions():
+        assert name in exported, name
+        assert hasattr(lib, name)
+    # and the ctypes signature table covers exactly the declared set
+    assert set(L.SIGNATURES) == set(declared_functions())
+
+
+def test_abi_version_and_status_strings(lib):
+    assert lib.sidon_abi_version() == 1
+    import sidon_b200._lib as L
+    assert L.status_string(0) == "ok"
+    assert "shared-memory" in L.status_string(3)
+
+
+@pytest.mark.parametrize("n", [512, 4096, 8400])
+def test_host_entry_hostF_bitwise_reference(lib, certs, n):
+    w, meta = certs[n]
+    a = np.ascontiguousarray(w)
+    assert lib.sidon_hostF(a.ctypes.data, a.size) == meta["ref_hostF"]
+
+
+def test_host_entry_hostF_kat(lib, kat):
+    for case in kat["hand"] + kat["eval257"]:
+        a = np.ascontiguousarray(case["a"], dtype=np.float64)
+        assert lib.sidon_hostF(a.ctypes.data, a.size) == case["F"]
+
+
+def test_smem_sizers_are_monotone_and_cover_the_working_set(lib):
+    import sidon_b200._lib as L
+    prev = 0
+    for n in (64, 512, 4096, 8400, 16384):
+        s = lib.sidon_smem_bytes(L.OP_LOCAL_SEARCH, n, L.F32)
+        assert s >= 4 * 3 * n                 # a + b/c at least, like localSearchSmem<float>
+        assert s > prev
+        prev = s
+    assert lib.sidon_smem_bytes(L.OP_EVAL, 8400, L.F64) >= 8 * 8400
+    assert lib.sidon_smem_bytes(L.OP_FRANK_WOLFE, 8400, L.F32) >= 4 * 5 * 8400
+    assert lib.sidon_smem_bytes(L.OP_LOCAL_SEARCH, 0, L.F32) == 0
+    assert lib.sidon_smem_bytes(99, 100, L.F32) == 0
+
+
+def test_formats_roundtrip_with_reference_loadvec(tmp_path):
+    """Our saveVec text is read back by the reference's loadVec and vice versa."""
+    import oracle
+    if not oracle.have_ref():
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    from sidon_b200 import formats
+    rng = np.random.default_rng(0)
+    a = rng.uniform(0, 1, 33)
+    p1 = tmp_path / "ours.txt"
+    formats.save_vec(p1, a, 1.2345)
+    buf = np.zeros(64)
+    m = oracle.ref_main().ref_loadVec(str(p1).encode(), buf.ctypes.data, 64)
+    assert m == 33 and np.array_equal(buf[:33], a)
+    p2 = tmp_path / "ref.txt"
+    oracle.ref_main().ref_saveVec(str(p2).encode(), np.ascontiguousarray(a).ctypes.data, 33, 1.5)
+    assert np.array_equal(formats.load_vec(p2), a)
+
+
+def test_synth_is_deterministic_and_shaped():
+    from sidon_b200 import synth
+    a = synth.population("structured", 512, 3, seed=1)
+    b = synth.population("structured", 512, 3, seed=1)
+    assert a.dtype == np.float32 and a.shape == (3, 512)
+    assert np.array_equal(a, b)
+    assert np.all(a[:, 512 // 50: 512 // 8] == 0)                  # support gap
+    assert np.all(a >= 0) and np.allclose(a.sum(1), 1, atol=1e-5)
+    L = synth.population("lognormal", 8400, 2, seed=3)
+    g0 = 8400 // 50
+    assert np.all(L[:, g0: g0 + 840] == 0)
+    frac0 = np.mean(L == 0)
+    assert 0.3 < frac0 < 0.5
