@@ -64,6 +64,10 @@ enum sidon_op {
 SIDON_API const char* sidon_status_string(int status);
 /* The cudaError_t value behind the last SIDON_ERR_CUDA on this thread. */
 SIDON_API int sidon_last_cuda_error(void);
+/* Device-side status word of the tensor-core kernels: SIDON_ERR_TIMEOUT if a
+ * bounded wait inside a kernel ran out since the last reset, else SIDON_OK.
+ * Synchronous (copies one word from the current device); reset != 0 clears it. */
+SIDON_API int sidon_device_status(int reset);
 /* ABI version of this library (bumped on any signature change). */
 SIDON_API int sidon_abi_version(void);
 
@@ -120,6 +124,7 @@ SIDON_API int sidon_local_search(void* pop, void* mom, void* vel, const int* ski
  * heights, any scale).  Writes value[P] (device) and saved[P*4] (device,
  * {M = max b, S = sum a, R = sum (b/M)^p, G_p}); b itself is not stored
  * unless b_out != NULL ([P][2n-1] device, for the stored-b comparison).
+ * precision FP32_SIMT, or BF16X1 / BF16X3 (b on the tensor cores).
  * No reference counterpart as an entry point: it exposes the objective of
  * the anneal (src/kernels.cuh:168-172). */
 SIDON_API int sidon_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
@@ -128,6 +133,8 @@ SIDON_API int sidon_lp_forward(const float* a, int n, int P, double p, float* va
 /* Gradient of G_p: grad_i = (4n R^(1/p)/S^2) (G_i/R - M/S) with
  * G_i = sum_j (b_{i+j}/M)^(p-1) a_j.  b is recomputed tile by tile from a
  * (b_in == NULL) or read from a stored [P][2n-1] array (b_in != NULL).
+ * precision as for sidon_lp_forward (the correlation on the tensor cores
+ * for BF16X1 / BF16X3).
  * saved: the forward's [P*4].  grad: device [P][n] fp32.
  * Replaces the gradient that exists only inside kLocalSearch
  * (src/kernels.cuh:221-244) and its CPU twin (tools/probe.cpp:77-92). */

@@ -25,6 +25,7 @@ SIGNATURES = {
     "sidon_status_string": (C.c_char_p, [_i]),
     "sidon_last_cuda_error": (_i, []),
     "sidon_abi_version": (_i, []),
+    "sidon_device_status": (_i, [_i]),
     "sidon_smem_bytes": (_sz, [_i, _i, _i]),
     "sidon_max_n": (_i, [_i, _i]),
     "sidon_hostF": (_d, [_vp, _i]),

@@ -26,6 +26,11 @@ int launch_local_search_tc(float* pop, float* mom, float* vel, const int* skip,
                            int precision, cudaStream_t st);
 int launch_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
                       float* b_out, cudaStream_t st);
+int launch_lp_forward_tc(const float* a, int n, int P, double p, float* value, float* saved,
+                         float* b_out, int precision, cudaStream_t st);
+int launch_lp_backward_tc(const float* a, const float* saved, const float* b_in, int n, int P,
+                          double p, float* grad, int precision, cudaStream_t st);
+int device_status(int reset);
 int launch_lp_backward(const float* a, const float* saved, const float* b_in, int n, int P,
                        double p, float* grad, cudaStream_t st);
 int launch_eval(const void* pop, int dtype, int n, int P, double* outF, int* outN, double tol,
@@ -103,6 +108,12 @@ const char* sidon_status_string(int status) {
 }
 
 int sidon_last_cuda_error(void) { return g_last_cuda; }
+
+int sidon_device_status(int reset) {
+  int rc = device_ok();
+  if (rc) return rc;
+  return device_status(reset);
+}
 int sidon_abi_version(void) { return 1; }
 
 size_t sidon_smem_bytes(int op, int n, int dtype) {
@@ -199,8 +210,11 @@ int sidon_lp_forward(const float* a, int n, int P, double p, float* value, float
   if (rc) return rc;
   if (P == 0) return SIDON_OK;
   if (!a || !value || !saved || !(p >= 1.0)) return SIDON_ERR_ARG;
-  if (precision != SIDON_PREC_FP32_SIMT) return SIDON_ERR_DTYPE;
-  return launch_lp_forward(a, n, P, p, value, saved, b_out, S(stream));
+  if (precision == SIDON_PREC_FP32_SIMT)
+    return launch_lp_forward(a, n, P, p, value, saved, b_out, S(stream));
+  if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
+    return launch_lp_forward_tc(a, n, P, p, value, saved, b_out, precision, S(stream));
+  return SIDON_ERR_DTYPE;
 }
 
 int sidon_lp_backward(const float* a, const float* saved, const float* b_in, int n, int P,
@@ -209,8 +223,11 @@ int sidon_lp_backward(const float* a, const float* saved, const float* b_in, int
   if (rc) return rc;
   if (P == 0) return SIDON_OK;
   if (!a || !saved || !grad || !(p >= 1.0)) return SIDON_ERR_ARG;
-  if (precision != SIDON_PREC_FP32_SIMT) return SIDON_ERR_DTYPE;
-  return launch_lp_backward(a, saved, b_in, n, P, p, grad, S(stream));
+  if (precision == SIDON_PREC_FP32_SIMT)
+    return launch_lp_backward(a, saved, b_in, n, P, p, grad, S(stream));
+  if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
+    return launch_lp_backward_tc(a, saved, b_in, n, P, p, grad, precision, S(stream));
+  return SIDON_ERR_DTYPE;
 }
 
 int sidon_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int pdhg_iters,

@@ -56,9 +56,9 @@ int main() {
   { std::mt19937 rng(3); std::uniform_real_distribution<double> U(0, 1);
     for (int p = 0; p < 5; ++p) { std::printf("eval257 %d", p);
       for (int i = 0; i < 257; ++i) { double x = (p == 0) ? 1.0 : U(rng);
-        std::printf(" %.9g", (double)(float)x); } std::printf("\n"); } }
+        std::printf(" %.17g", (double)(float)x); } std::printf("\n"); } }
   { std::mt19937 rng(5); std::uniform_real_distribution<float> U(0.1f, 1.0f);
-    std::printf("ls128"); for (int i = 0; i < 128 * 4; ++i) std::printf(" %.9g", (double)U(rng));
+    std::printf("ls128"); for (int i = 0; i < 128 * 4; ++i) std::printf(" %.17g", (double)U(rng));
     std::printf("\n"); }
   return 0;
 }

@@ -63,12 +63,12 @@ def test_certify_certificates(cuda, certs, orc, n):
         assert F.item() == Fo and M.item() == Mo and S.item() == So
 
 
-@pytest.mark.parametrize("n", [512, 8400])
-def test_certify_bit_exact_across_cell_splits(cuda, certs, n):
+@pytest.mark.parametrize("n,splits", [(512, 3), (4096, 2), (8400, 1)])
+def test_certify_bit_exact_across_cell_splits(cuda, certs, n, splits):
     w, _ = certs[n]
     x = T(w[None, :], cuda)
     F0 = K().certify(x)[0].item()
-    for _ in range(2):
+    for _ in range(splits):
         x = K().refine(x)
         assert K().certify(x)[0].item() == F0
 

@@ -1,0 +1,130 @@
+"""Tensor-core (tcgen05 BF16x3 / BF16x1) path vs the oracle.  Needs a B200.
+
+Tolerances (relative to max b or max |grad|), from the split arithmetic:
+BF16x3 represents each height to ~2^-17 and drops lo*lo (~2^-18), with fp32
+accumulation -> b within 3e-5 of max b; BF16x1 keeps 8 bits -> 1e-2.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def K():
+    from sidon_b200 import kernels
+    return kernels
+
+
+def T(x, dev, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype, device=dev)
+
+
+def _status():
+    import sidon_b200
+    return sidon_b200.load().sidon_device_status(1)
+
+
+@pytest.mark.parametrize("n", [1, 100, 128, 129, 300, 1000, 4096, 8400])
+def test_tc_conv_bf16x3_vs_fp64(cuda, n):
+    rng = np.random.default_rng(n)
+    a = rng.lognormal(0, 1, (2, n)).astype(np.float32)
+    a[:, rng.uniform(size=n) < 1 / 3] = 0
+    a[:, 0] = 8 * a.mean() + 1.0          # endpoint atom (never an all-zero row)
+    _, saved, b = K().lp_forward(T(a, cuda), 8.0, store_b=True, precision="bf16x3")
+    b = b.cpu().numpy().astype(np.float64)
+    assert _status() == 0
+    for p in range(2):
+        ref = np.convolve(a[p].astype(np.float64), a[p].astype(np.float64))
+        err = np.max(np.abs(b[p] - ref)) / ref.max()
+        assert err <= 3e-5, (n, err)
+        assert abs(saved[p, 0].item() - ref.max()) <= 3e-5 * ref.max()
+
+
+def test_tc_conv_bf16x1_tolerance(cuda):
+    rng = np.random.default_rng(0)
+    a = rng.uniform(0, 1, (1, 700)).astype(np.float32)
+    _, _, b = K().lp_forward(T(a, cuda), 8.0, store_b=True, precision="bf16x1")
+    ref = np.convolve(a[0].astype(np.float64), a[0].astype(np.float64))
+    err = np.max(np.abs(b.cpu().numpy()[0] - ref)) / ref.max()
+    assert err <= 1e-2
+    assert _status() == 0
+
+
+@pytest.mark.parametrize("n,p", [(300, 8.0), (1000, 64.0), (4096, 64.0), (4096, 512.0)])
+def test_tc_gradient_vs_long_double(cuda, orc, n, p):
+    """BF16x3 adjoint vs the long-double oracle gradient; the weights
+    (b/M)^(p-1) amplify the split error by p-1, so the bound is
+    max(2e-3, 2e-5 p) of max|grad|."""
+    from sidon_b200 import synth
+    pop = synth.population("structured", n, 2, seed=n)
+    a = T(pop, cuda)
+    val, saved, _ = K().lp_forward(a, p, precision="bf16x3")
+    g = K().lp_backward(a, saved, p, precision="bf16x3").cpu().numpy()
+    assert _status() == 0
+    tol = max(2e-3, 2e-5 * p)
+    for r in range(2):
+        ref_g, ref_v = orc.lp_grad(pop[r].astype(np.float64), p)
+        assert abs(val[r].item() - ref_v) <= 1e-4 * ref_v
+        err = np.max(np.abs(g[r] - ref_g)) / np.abs(ref_g).max()
+        assert err <= tol, (n, p, err)
+
+
+def test_tc_backward_stored_b_matches_recompute(cuda):
+    from sidon_b200 import synth
+    a = T(synth.population("structured", 2048, 3, seed=5), cuda)
+    _, saved, b = K().lp_forward(a, 64.0, store_b=True, precision="bf16x3")
+    g1 = K().lp_backward(a, saved, 64.0, precision="bf16x3")
+    g2 = K().lp_backward(a, saved, 64.0, b=b, precision="bf16x3")
+    assert torch.equal(g1, g2)
+
+
+def test_tc_local_search_selftest(cuda, kat, orc):
+    """src/main.cu:258-288 with the tensor-core step: F decreases, heights
+    stay >= 0 and finite, and the run is bitwise reproducible."""
+    case = kat["ls128"]
+    start = np.asarray(case["a"], dtype=np.float32)
+    x1, x2 = T(start, cuda), T(start, cuda)
+    for x in (x1, x2):
+        K().run_local_search(x, 800, 4.0, 300.0, 0.06, 0.002, precision="bf16x3")
+    assert _status() == 0
+    assert torch.equal(x1, x2)
+    h = x1.cpu().numpy()
+    assert np.all(h >= 0) and np.all(np.isfinite(h))
+    F1, _ = K().run_eval(x1)
+    for p in range(4):
+        assert F1[p].item() < case["F"][p]
+
+
+def test_tc_local_search_tracks_fp32(cuda, orc):
+    """A short anneal at n=1000 with BF16x3 and with FP32 SIMT from the same
+    start: certified F agree to 1e-3 relative (different rounding, same
+    dynamics)."""
+    from sidon_b200 import synth
+    pop = synth.population("structured", 1000, 4, seed=77)
+    xt, xs = T(pop, cuda), T(pop, cuda)
+    K().run_local_search(xt, 30, 4.0, 64.0, 0.01, 0.004, precision="bf16x3")
+    K().run_local_search(xs, 30, 4.0, 64.0, 0.01, 0.004, precision="fp32")
+    assert _status() == 0
+    Ft, _ = K().run_eval(xt)
+    Fs, _ = K().run_eval(xs)
+    F0, _ = K().run_eval(T(pop, cuda))
+    for p in range(4):
+        assert Ft[p].item() < F0[p].item()
+        assert abs(Ft[p].item() - Fs[p].item()) <= 1e-3 * Fs[p].item()
+
+
+def test_tc_local_search_skip_modes_and_full_size(cuda):
+    from sidon_b200 import synth
+    pop = synth.population("lognormal", 8400, 3, seed=3)
+    x = T(pop, cuda)
+    skip = T(np.array([0, 1, 0], dtype=np.int32), cuda, torch.int32)
+    mode = T(np.array([0, 0, 1], dtype=np.int32), cuda, torch.int32)
+    K().run_local_search(x, 5, 2.0, 16.0, 1e-3, 1e-3, skip=skip, mode_arr=mode,
+                         precision="bf16x3")
+    assert _status() == 0
+    assert torch.equal(x[1], T(pop[1], cuda))
+    h = x.cpu().numpy()
+    assert np.all(h >= 0) and np.all(np.isfinite(h))
+    assert np.all(h[2] > 0) == np.all(pop[2] > 0)      # mirror steps keep zeros zero
+    assert abs(h[0].sum() - 1) < 1e-4 and abs(h[2].sum() - 1) < 1e-4
