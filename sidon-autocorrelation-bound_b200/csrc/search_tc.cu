@@ -15,7 +15,8 @@
 //    stages  STAGES x 8 KB   Hankel windows (hi | lo planes)
 //    bc      2 x rc x 256 B  row-shifted block-matrix copies (two hi slots,
 //                            or one hi + lo pair for the correlation)
-//    sa      fp32 heights, 128 zero cells before cell 0, >= 256 after n_pad
+//    sa      fp32 heights in the padded block layout (cell i at i + 4 floor(i/128)),
+//            zero margins of >= 128 cells on both sides
 //    crev    fp32 reversed weights c_rev[t] = c[2 m L - 2 - t], zero margin
 //    red     64 floats of reduction scratch, mbarriers, TMEM address, abort flag
 // ---------------------------------------------------------------------------
@@ -33,7 +34,7 @@ struct Layout {
   __host__ __device__ Layout(int n, bool with_crev) {
     m = (n + L - 1) / L;
     rc = round_up(ZP + m + 24, 8);   // whole 8-row core-matrix groups
-    sa_len = 128 + L * m + 384;
+    sa_len = 132 * (m + 6);
     crev_len = with_crev ? (2 * L * m + 512) : 0;
     size_t o = (size_t)STAGES * STAGE_BYTES;
     off_bc = o;
@@ -45,7 +46,7 @@ struct Layout {
     o += (size_t)crev_len * 4;
     o = (o + 15) & ~(size_t)15;
     off_red = o;
-    o += 64 * 4 + (STAGES + 4) * 8 + 16;
+    o += 64 * 4 + (2 * STAGES + 5) * 8 + 16;
     total = o + 1024;   // slack for aligning the dynamic base to 1 KB
   }
 };
@@ -63,31 +64,39 @@ __device__ __forceinline__ Shared setup(int n, bool with_crev, bool three, unsig
   Shared S;
   S.C.stages = base;
   S.C.bc = base + Lo.off_bc;
-  S.sa = reinterpret_cast<float*>(base + Lo.off_sa) + 128;
+  S.sa = reinterpret_cast<float*>(base + Lo.off_sa) + 132;
   S.crev = reinterpret_cast<float*>(base + Lo.off_crev);
   S.red = reinterpret_cast<float*>(base + Lo.off_red);
   uint64_t* bars = reinterpret_cast<uint64_t*>(S.red + 64);
-  S.C.bar_stage = bars;
-  S.C.bar_bc = bars + STAGES;
-  S.C.bar_done = bars + STAGES + 2;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + STAGES + 4);
+  S.C.full = bars;
+  S.C.empty = bars + STAGES;
+  S.C.bc_full = bars + 2 * STAGES;
+  S.C.bc_empty = bars + 2 * STAGES + 2;
+  S.C.bar_done = bars + 2 * STAGES + 4;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
   S.C.abort = reinterpret_cast<int*>(tslot + 1);
   S.C.m = Lo.m;
   S.C.rc = Lo.rc;
   S.C.n = n;
   S.C.three = three;
   S.C.done_use = 0;
-  S.C.bc_use[0] = S.C.bc_use[1] = 0;
+  S.C.st_next = 0;
+  S.C.bc_uses[0] = S.C.bc_uses[1] = 0;
 #pragma unroll
-  for (int s = 0; s < STAGES; ++s) S.C.stage_use[s] = 0;
+  for (int s = 0; s < STAGES; ++s) S.C.uses[s] = 0;
   // zero the fp32 buffers (margins must stay zero)
   float* z0 = reinterpret_cast<float*>(base + Lo.off_sa);
   for (int i = threadIdx.x; i < Lo.sa_len; i += blockDim.x) z0[i] = 0.f;
   for (int i = threadIdx.x; i < Lo.crev_len; i += blockDim.x) S.crev[i] = 0.f;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) mbar_init(&S.C.bar_stage[s], 1);
-    mbar_init(&S.C.bar_bc[0], 1);
-    mbar_init(&S.C.bar_bc[1], 1);
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&S.C.full[s], NBUILD_WARPS);
+      mbar_init(&S.C.empty[s], 1);
+    }
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&S.C.bc_full[s], NBUILD_WARPS);
+      mbar_init(&S.C.bc_empty[s], 1);
+    }
     mbar_init(S.C.bar_done, 1);
     mbar_fence_init();
     *S.C.abort = 0;
@@ -140,7 +149,7 @@ k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ sk
   const int W = acc_width(m);
   const Lane ln;
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) { S.sa[i] = a[i]; mg[i] = 0.f; vg[i] = 0.f; }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) { S.sa[pidx(i)] = a[i]; mg[i] = 0.f; vg[i] = 0.f; }
   __syncthreads();
 
   const float lnPr = (float)log((double)pEnd / (double)pStart);
@@ -216,29 +225,29 @@ k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ sk
           mg[i] = mm;
           vg[i] = vv;
           const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
-          x = S.sa[i] - step;
+          x = S.sa[pidx(i)] - step;
           if (x < 0.f) x = 0.f;
         } else {
           float e = -lr * (gi / M);
           if (e > 4.f) e = 4.f;
           if (e < -4.f) e = -4.f;
-          x = S.sa[i] * expf(e);
+          x = S.sa[pidx(i)] * expf(e);
         }
-        S.sa[i] = x;
+        S.sa[pidx(i)] = x;
         sloc += x;
       }
     }
     float Ssum = block_sum(sloc, S.red);
     if (!(Ssum > 0.f)) {
-      for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[i] = 1.f / (float)n;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] = 1.f / (float)n;
       Ssum = 1.f;
     }
     const float inv = 1.f / Ssum;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[i] *= inv;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] *= inv;
     __syncthreads();
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = S.sa[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = S.sa[pidx(i)];
   teardown(S);
 }
 
@@ -256,7 +265,7 @@ k_lp_forward_tc(const float* __restrict__ pop, int n, float p, float* __restrict
   const float* a = pop + (size_t)pid * n;
   __syncthreads();
   float sl = 0.f;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; S.sa[i] = x; sl += x; }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; S.sa[pidx(i)] = x; sl += x; }
   const float Ssum = block_sum(sl, S.red);
   zero_acc(C, COL_CONV, W);
   fence_before();
@@ -320,7 +329,7 @@ k_lp_backward_tc(const float* __restrict__ pop, const float* __restrict__ saved,
   const float* a = pop + (size_t)pid * n;
   const float M = saved[4 * pid + 0], Ssum = saved[4 * pid + 1], R = saved[4 * pid + 2];
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[i] = a[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] = a[i];
   __syncthreads();
   zero_acc(C, COL_CONV, W);
   zero_acc(C, COL_CORR, W);

@@ -181,17 +181,33 @@ __device__ __forceinline__ void split_bf16(float x, uint16_t& hi, uint16_t& lo) 
   lo = __bfloat16_as_ushort(l);
 }
 
-// Shared state of one CTA (every thread holds an identical copy).
+// Heights live in shared memory in a padded block layout: logical cell i at
+// physical index i + 4 floor(i / 128) (block stride 132 floats = 33 x 16 B),
+// so that loading the same 16 B of eight consecutive blocks hits eight
+// distinct bank groups.
+__device__ __forceinline__ int pidx(int i) { return i + 4 * (i >> 7); }
+
+// Warp roles during the tile phases: warp MMA_WARP (lane 0) issues every
+// MMA; the other warps build windows and block-matrix copies.
+constexpr int MMA_WARP = NTHREADS / 32 - 1;
+constexpr int NBUILD_WARPS = NTHREADS / 32 - 1;
+constexpr int NBUILD = NBUILD_WARPS * 32;
+
+// Shared state of one CTA.  Every thread holds a copy; the pipeline counters
+// of a role are kept identical by every thread of that role.
 struct Ctx {
   unsigned char* stages;   // STAGES x (hi plane | lo plane), 1 KB aligned
   unsigned char* bc;       // block-matrix copies: 2 planes of rc x 256 B
-  uint64_t* bar_stage;     // STAGES mbarriers (arrival: tcgen05.commit)
-  uint64_t* bar_bc;        // 2 mbarriers, one per copy slot
+  uint64_t* full;          // STAGES "window ready" barriers (NBUILD_WARPS arrivals)
+  uint64_t* empty;         // STAGES "window consumed" barriers (tcgen05.commit)
+  uint64_t* bc_full;       // 2 "copy ready" barriers (NBUILD_WARPS arrivals)
+  uint64_t* bc_empty;      // 2 "copy consumed" barriers (tcgen05.commit)
   uint64_t* bar_done;      // "all MMAs of a phase done"
   uint32_t tmem;           // TMEM base address (512 columns)
-  int stage_use[STAGES];   // completions expected per stage so far
-  int bc_use[2];
+  int uses[STAGES];        // times each stage has been filled (builders) / consumed (MMA)
+  int bc_uses[2];
   int done_use;
+  int st_next;             // next stage in the ring
   int* abort;              // shared abort flag
   int m, rc, n;
   bool three;              // BF16x3 (else BF16x1)
@@ -215,61 +231,74 @@ __device__ __forceinline__ bool wait_phase(Ctx& C, uint64_t* bar, uint32_t parit
   return true;
 }
 
-// Row-shifted block-matrix copy into slot `slot` (planes hi, and lo if
-// want_lo): BC[x][s] = a[(x - rho - ZP) L + L - 1 - s] for block rows in [0, m).
-// sa: fp32 heights with zero margins.
-__device__ __forceinline__ void build_bc(Ctx& C, const float* sa, int rho, int slot, bool want_lo) {
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo_elem, float hi_elem) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo_elem, hi_elem);   // .x = first argument
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ float bf_lo_f(uint32_t p) { return __uint_as_float(p << 16); }
+__device__ __forceinline__ float bf_hi_f(uint32_t p) { return __uint_as_float(p & 0xFFFF0000u); }
+
+// hi / lo planes of 8 values (v[0] lands at the lowest address); the lo plane
+// holds lsc * (v - hi) rounded (lsc = 2 doubles it exactly).
+__device__ __forceinline__ void split8(const float (&v)[8], float lsc, uint4& hi, uint4& lo) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    h[q] = pack_bf16x2(v[2 * q], v[2 * q + 1]);
+    l[q] = pack_bf16x2(lsc * (v[2 * q] - bf_lo_f(h[q])), lsc * (v[2 * q + 1] - bf_hi_f(h[q])));
+  }
+  hi = make_uint4(h[0], h[1], h[2], h[3]);
+  lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// Row-shifted block-matrix copy into slot `slot` (hi plane, and lo plane in
+// the next slot's space when want_lo): BC[x][s] = a[(x - rho - ZP) L + L-1-s]
+// for block rows in [0, m).  Chunk c = ((x>>3)*16 + h)*8 + (x&7) sits at byte
+// 16 c, so consecutive builder threads store consecutive 16 B; the 8
+// heights of a chunk are two aligned float4 of one block (padded layout).
+__device__ __forceinline__ void build_bc(Ctx& C, const float* sa, int rho, int slot, bool want_lo,
+                                         int bt) {
   const int rc = C.rc;
   unsigned char* hi = C.bc + (size_t)slot * rc * 256;
-  unsigned char* lo = hi + (size_t)rc * 256;      // slot 0's lo plane is slot 1's space
-  const int tasks = rc * 16;
-  for (int t = threadIdx.x; t < tasks; t += blockDim.x) {
-    const int x = t >> 4, h = t & 15;
+  unsigned char* lo = hi + (size_t)rc * 256;
+  const int chunks = rc * 16;
+  for (int c = bt; c < chunks; c += NBUILD) {
+    const int x = ((c >> 7) << 3) | (c & 7), h = (c >> 3) & 15;
     const int J = x - rho - ZP;
-    const bool in = (J >= 0 && J < C.m);
-    uint32_t ph[4], pl[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      uint16_t h0 = 0, l0 = 0, h1 = 0, l1 = 0;
-      if (in) {
-        const int i0 = J * L + L - 1 - (8 * h + 2 * q);   // element s0; s0 + 1 is i0 - 1
-        split_bf16(sa[i0], h0, l0);
-        split_bf16(sa[i0 - 1], h1, l1);
-      }
-      ph[q] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-      pl[q] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+    uint4 vh = make_uint4(0, 0, 0, 0), vl = vh;
+    if (J >= 0 && J < C.m) {
+      // s = 8h .. 8h+7  <->  cells J L + L-1-8h down to J L + L-8-8h
+      const float* src = sa + pidx(J * L) + (L - 8 - 8 * h);
+      const float4 u0 = *reinterpret_cast<const float4*>(src);
+      const float4 u1 = *reinterpret_cast<const float4*>(src + 4);
+      const float v[8] = {u1.w, u1.z, u1.y, u1.x, u0.w, u0.z, u0.y, u0.x};
+      split8(v, 1.f, vh, vl);
     }
-    const int off = (x >> 3) * 2048 + h * 128 + (x & 7) * 16;
-    *reinterpret_cast<uint4*>(hi + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
-    if (want_lo) *reinterpret_cast<uint4*>(lo + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+    *reinterpret_cast<uint4*>(hi + 16 * c) = vh;
+    if (want_lo) *reinterpret_cast<uint4*>(lo + 16 * c) = vl;
   }
 }
 
-// Window of tile w into stage st: CM[q'][i][j] = x[8 (16 w + q') + off + i + j],
-// planes hi and lo (lo doubled when lo2: the convolution's symmetric term).
-__device__ __forceinline__ void build_window(Ctx& C, int st, const float* x, int off, int w,
-                                             bool lo2) {
+// Window of tile w into stage st: CM[q'][i][j] = x[8 (16 w + q') + off + i + j]
+// (x indexed through map()), planes hi and lsc*lo.
+template <typename MapFn>
+__device__ __forceinline__ void build_window(Ctx& C, int st, const float* x, MapFn&& map, int off,
+                                             int w, float lsc, int bt) {
   unsigned char* hi = C.stages + st * STAGE_BYTES;
   unsigned char* lo = hi + PLANE;
-  const float lsc = lo2 ? 2.f : 1.f;
-  for (int t = threadIdx.x; t < WIN_CM * 8; t += blockDim.x) {
-    const int qp = t >> 3, i = t & 7;
-    const float* src = x + 8 * (16 * w + qp) + off + i;
-    uint32_t ph[4], pl[4];
+  for (int t = bt; t < WIN_CM * 8; t += NBUILD) {
+    const int base = 8 * (16 * w + (t >> 3)) + off + (t & 7);
+    float v[8];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      uint16_t h0, l0, h1, l1;
-      split_bf16(src[2 * q], h0, l0);
-      split_bf16(src[2 * q + 1], h1, l1);
-      ph[q] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-      if (lo2) {
-        l0 = __bfloat16_as_ushort(__hmul(__ushort_as_bfloat16(l0), __float2bfloat16(lsc)));
-        l1 = __bfloat16_as_ushort(__hmul(__ushort_as_bfloat16(l1), __float2bfloat16(lsc)));
-      }
-      pl[q] = (uint32_t)l0 | ((uint32_t)l1 << 16);
-    }
-    *reinterpret_cast<uint4*>(hi + qp * 128 + i * 16) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
-    *reinterpret_cast<uint4*>(lo + qp * 128 + i * 16) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+    for (int j = 0; j < 8; ++j) v[j] = x[map(base + j)];
+    uint4 vh, vl;
+    split8(v, lsc, vh, vl);
+    *reinterpret_cast<uint4*>(hi + 16 * t) = vh;
+    *reinterpret_cast<uint4*>(lo + 16 * t) = vl;
   }
 }
 
@@ -313,50 +342,68 @@ __device__ __forceinline__ void issue_tile(Ctx& C, int st, int slot, const Tile&
   }
 }
 
-// Run tiles w = 0..ntiles-1 in residue classes w mod 8.  geom(w) gives the
-// tile; the window source is x with offset off.  Ends with every MMA of the
-// sequence complete (bar_done) and the accumulator readable.
-template <typename GeomFn>
-__device__ bool run_tiles(Ctx& C, int ntiles, const float* sa, const float* x, int off, bool corr,
-                          GeomFn&& geom, unsigned int* status) {
+// Run tiles w = 0..ntiles-1 in residue classes w mod 8 through the
+// warp-specialised pipeline.  geom(w) gives the tile; the window source is
+// x[map(.)] with offset off.  Ends with every MMA of the sequence complete
+// (bar_done) and the accumulator readable by all warps.
+template <typename GeomFn, typename MapFn>
+__device__ bool run_tiles(Ctx& C, int ntiles, const float* sa, const float* x, MapFn&& map,
+                          int off, bool corr, GeomFn&& geom, unsigned int* status) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool want_lo = corr && C.three;
-  int st_next = 0;
-  for (int rho = 0; rho < 8 && rho < ntiles; ++rho) {
-    // the correlation's copy needs both planes, which fill both slots
-    const int slot = corr ? 0 : (rho & 1);
-    if (corr) {
-      // previous class must have finished reading the (only) copy
-      if (C.bc_use[0] > 0 &&
-          !wait_phase(C, &C.bar_bc[0], (uint32_t)((C.bc_use[0] - 1) & 1), status))
-        break;
-    } else if (C.bc_use[slot] > 0 &&
-               !wait_phase(C, &C.bar_bc[slot], (uint32_t)((C.bc_use[slot] - 1) & 1), status)) {
-      break;
-    }
-    build_bc(C, sa, rho, slot, want_lo);
-    for (int w = rho; w < ntiles; w += 8) {
-      const Tile T = geom(w);
-      const int st = st_next;
-      st_next = (st_next + 1 == STAGES) ? 0 : st_next + 1;
-      const int use = C.stage_use[st];
-      if (use > 0 && !wait_phase(C, &C.bar_stage[st], (uint32_t)((use - 1) & 1), status)) break;
-      build_window(C, st, x, off, w, !corr);
-      fence_async_smem();
-      __syncthreads();
-      if (*((volatile int*)C.abort)) break;
-      if (threadIdx.x == 0) {
-        fence_after();
-        issue_tile(C, st, slot, T, corr);
-        mma_commit(&C.bar_stage[st]);
+  const float lsc = corr ? 1.f : 2.f;
+  int st = C.st_next;
+  if (warp == MMA_WARP) {
+    if (lane == 0) {
+      fence_after();
+      for (int rho = 0; rho < 8 && rho < ntiles; ++rho) {
+        const int slot = corr ? 0 : (rho & 1);
+        if (!wait_phase(C, &C.bc_full[slot], (uint32_t)(C.bc_uses[slot] & 1), status)) break;
+        C.bc_uses[slot] += 1;
+        bool ok = true;
+        for (int w = rho; w < ntiles; w += 8) {
+          if (!wait_phase(C, &C.full[st], (uint32_t)(C.uses[st] & 1), status)) { ok = false; break; }
+          C.uses[st] += 1;
+          fence_after();
+          issue_tile(C, st, slot, geom(w), corr);
+          mma_commit(&C.empty[st]);
+          st = (st + 1 == STAGES) ? 0 : st + 1;
+        }
+        mma_commit(&C.bc_empty[slot]);
+        if (!ok) break;
       }
-      C.stage_use[st] = use + 1;
+      mma_commit(C.bar_done);
     }
-    if (*((volatile int*)C.abort)) break;
-    if (threadIdx.x == 0) mma_commit(&C.bar_bc[slot]);
-    C.bc_use[slot] += 1;
+    __syncwarp();
+  } else {
+    const int bt = threadIdx.x - (warp > MMA_WARP ? 32 : 0);   // 0 .. NBUILD-1
+    for (int rho = 0; rho < 8 && rho < ntiles; ++rho) {
+      const int slot = corr ? 0 : (rho & 1);
+      const int u = C.bc_uses[slot];
+      if (u > 0 && !wait_phase(C, &C.bc_empty[slot], (uint32_t)((u - 1) & 1), status)) break;
+      C.bc_uses[slot] = u + 1;
+      build_bc(C, sa, rho, slot, want_lo, bt);
+      fence_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&C.bc_full[slot]);
+      bool ok = true;
+      for (int w = rho; w < ntiles; w += 8) {
+        const int us = C.uses[st];
+        if (us > 0 && !wait_phase(C, &C.empty[st], (uint32_t)((us - 1) & 1), status)) {
+          ok = false;
+          break;
+        }
+        C.uses[st] = us + 1;
+        build_window(C, st, x, map, off, w, lsc, bt);
+        fence_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&C.full[st]);
+        st = (st + 1 == STAGES) ? 0 : st + 1;
+      }
+      if (!ok) break;
+    }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) mma_commit(C.bar_done);
+  C.st_next = st;
   const bool ok = wait_phase(C, C.bar_done, (uint32_t)(C.done_use & 1), status);
   C.done_use += 1;
   fence_after();
@@ -373,7 +420,7 @@ __device__ __forceinline__ int acc_width(int m) { return round_up(2 * m + 16, 32
 // b = a * a into accumulator columns of COL_CONV (column K, lane r = b_{K L + r})
 __device__ __forceinline__ bool conv_tc(Ctx& C, const float* sa, unsigned int* status) {
   const int m = C.m;
-  return run_tiles(C, m + 1, sa, sa, -(L - 1), false,
+  return run_tiles(C, m + 1, sa, sa, [](int i) { return pidx(i); }, -(L - 1), false,
                    [&](int d) {
                      Tile T;
                      const int off = (d / DG) * DG;
@@ -391,7 +438,7 @@ __device__ __forceinline__ bool conv_tc(Ctx& C, const float* sa, unsigned int* s
 __device__ __forceinline__ bool corr_tc(Ctx& C, const float* sa, const float* crev,
                                         unsigned int* status) {
   const int m = C.m;
-  return run_tiles(C, 2 * m - 1, sa, crev, 0, true,
+  return run_tiles(C, 2 * m - 1, sa, crev, [](int i) { return i; }, 0, true,
                    [&](int e) {
                      Tile T;
                      const int lo = max(0, m - 1 - e), hi = min(m, 2 * m - 1 - e);
