@@ -7,17 +7,18 @@
 //    k_lp_backward_tc   dG_p/da with b recomputed on the tensor cores
 //
 //  One CTA (8 warps) per candidate, one CTA per SM (the shared-memory
-//  working set is ~17 n bytes), 512 TMEM columns: accumulator of the
-//  convolution at column 0, of the correlation at column 256.  The
-//  elementwise work (max, weights, Adam) runs on the 8 warps reading TMEM.
+//  working set is ~24 n bytes), 512 TMEM columns: the convolution
+//  accumulator at column 0, the correlation accumulator after it.  The
+//  elementwise work (max, weights, Adam) runs on all 8 warps; the weights
+//  beyond 2n-1 stay zero for the whole launch (the correlation copies read
+//  whole blocks).
 //
-//  Shared memory (offsets 1 KB aligned):
-//    stages  STAGES x 8 KB   Hankel windows (hi | lo planes)
-//    bc      2 x rc x 256 B  row-shifted block-matrix copies (two hi slots,
-//                            or one hi + lo pair for the correlation)
-//    sa      fp32 heights in the padded block layout (cell i at i + 4 floor(i/128)),
-//            zero margins of >= 128 cells on both sides
-//    crev    fp32 reversed weights c_rev[t] = c[2 m L - 2 - t], zero margin
+//  Shared memory (see Layout):
+//    stages  STAGES x 6 KB   Hankel windows (hi | lo planes)
+//    bc      B-matrix copies: two conv slots (hi) or one corr hi|lo pair
+//    sa      fp32 heights, padded block layout (cell i at i + 4 floor(i/64)),
+//            zero margins on both sides
+//    cb      fp32 padded scratch: b, then the weights c, then G
 //    red     64 floats of reduction scratch, mbarriers, TMEM address, abort flag
 // ---------------------------------------------------------------------------
 #include "conv_simt.cuh"
@@ -28,44 +29,47 @@ namespace tc {
 
 __device__ unsigned int g_status_word = 0u;   // SIDON_ERR_TIMEOUT after a timed-out wait
 
+// dynamic shared memory plan (byte offsets from a 1 KB aligned base)
 struct Layout {
-  int m, rc, sa_len, crev_len;
-  size_t off_bc, off_sa, off_crev, off_red, total;
-  __host__ __device__ Layout(int n, bool with_crev) {
-    m = (n + L - 1) / L;
-    rc = round_up(ZP + m + 24, 8);   // whole 8-row core-matrix groups
-    sa_len = 132 * (m + 6);
-    crev_len = with_crev ? (2 * L * m + 512) : 0;
+  int m, rc, rcc, sa_len, cb_len;
+  size_t off_bc, off_sa, off_cb, off_red, total;
+  __host__ __device__ Layout(int n) {
+    m = (n + BL - 1) / BL;
+    rc = conv_copy_rows(m);
+    rcc = corr_copy_rows(m);
+    sa_len = 68 * (m + 8);                 // padded heights, 136 cells of margin in front
+    cb_len = 68 * (2 * m + 2);             // padded weights / gather scratch
     size_t o = (size_t)STAGES * STAGE_BYTES;
     off_bc = o;
-    o += (size_t)2 * rc * 256;
+    const int rows = rcc > rc ? rcc : rc;
+    o += (size_t)2 * rows * 128;           // two conv slots or one corr hi|lo pair
     off_sa = o;
     o += (size_t)sa_len * 4;
-    o = (o + 1023) & ~(size_t)1023;
-    off_crev = o;
-    o += (size_t)crev_len * 4;
+    o = (o + 15) & ~(size_t)15;
+    off_cb = o;
+    o += (size_t)cb_len * 4;
     o = (o + 15) & ~(size_t)15;
     off_red = o;
     o += 64 * 4 + (2 * STAGES + 5) * 8 + 16;
-    total = o + 1024;   // slack for aligning the dynamic base to 1 KB
+    total = o + 1024;                      // slack for aligning the dynamic base to 1 KB
   }
 };
 
 struct Shared {
   Ctx C;
-  float* sa;     // cell 0
-  float* crev;   // element 0
+  float* sa;     // padded heights, logical cell 0
+  float* cb;     // padded weights / gather scratch, logical index 0
   float* red;
 };
 
-__device__ __forceinline__ Shared setup(int n, bool with_crev, bool three, unsigned char* raw) {
-  const Layout Lo(n, with_crev);
+__device__ __forceinline__ Shared setup(int n, bool three, unsigned char* raw) {
+  const Layout Lo(n);
   unsigned char* base = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
   Shared S;
   S.C.stages = base;
   S.C.bc = base + Lo.off_bc;
-  S.sa = reinterpret_cast<float*>(base + Lo.off_sa) + 132;
-  S.crev = reinterpret_cast<float*>(base + Lo.off_crev);
+  S.sa = reinterpret_cast<float*>(base + Lo.off_sa) + 136;
+  S.cb = reinterpret_cast<float*>(base + Lo.off_cb);
   S.red = reinterpret_cast<float*>(base + Lo.off_red);
   uint64_t* bars = reinterpret_cast<uint64_t*>(S.red + 64);
   S.C.full = bars;
@@ -77,17 +81,18 @@ __device__ __forceinline__ Shared setup(int n, bool with_crev, bool three, unsig
   S.C.abort = reinterpret_cast<int*>(tslot + 1);
   S.C.m = Lo.m;
   S.C.rc = Lo.rc;
+  S.C.rcc = Lo.rcc;
   S.C.n = n;
+  S.C.dmax = last_tile(n);
   S.C.three = three;
   S.C.done_use = 0;
   S.C.st_next = 0;
   S.C.bc_uses[0] = S.C.bc_uses[1] = 0;
 #pragma unroll
   for (int s = 0; s < STAGES; ++s) S.C.uses[s] = 0;
-  // zero the fp32 buffers (margins must stay zero)
   float* z0 = reinterpret_cast<float*>(base + Lo.off_sa);
   for (int i = threadIdx.x; i < Lo.sa_len; i += blockDim.x) z0[i] = 0.f;
-  for (int i = threadIdx.x; i < Lo.crev_len; i += blockDim.x) S.crev[i] = 0.f;
+  for (int i = threadIdx.x; i < Lo.cb_len; i += blockDim.x) S.cb[i] = 0.f;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&S.C.full[s], NBUILD_WARPS);
@@ -118,16 +123,13 @@ __device__ __forceinline__ void teardown(Shared& S) {
   }
 }
 
-// lane quadrant / column-half of the calling warp
-struct Lane {
-  int quad, half, r;
-  __device__ Lane() {
-    const int w = threadIdx.x >> 5;
-    quad = w & 3;
-    half = w >> 2;
-    r = 32 * quad + (threadIdx.x & 31);
-  }
-};
+// zero both accumulators and hand the tensor memory to the MMA warp
+__device__ __forceinline__ void prime(Ctx& C, bool corr_too) {
+  zero_acc(C, COL_CONV, conv_width(C.m));
+  if (corr_too) zero_acc(C, col_corr(C.m), corr_width(C.m));
+  fence_before();
+  __syncthreads();
+}
 
 // ------------------------------ local search ------------------------------
 __global__ void __launch_bounds__(NTHREADS, 1)
@@ -143,10 +145,9 @@ k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ sk
   float* mg = mom + (size_t)pid * n;
   float* vg = vel + (size_t)pid * n;
 
-  Shared S = setup(n, true, three != 0, smem_raw);
+  Shared S = setup(n, three != 0, smem_raw);
   Ctx& C = S.C;
-  const int m = C.m, nb = 2 * n - 1;
-  const int W = acc_width(m);
+  const int nb = 2 * n - 1;
   const Lane ln;
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) { S.sa[pidx(i)] = a[i]; mg[i] = 0.f; vg[i] = 0.f; }
@@ -155,49 +156,29 @@ k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ sk
   const float lnPr = (float)log((double)pEnd / (double)pStart);
   const float lnLr = (float)log((double)lrEnd / (double)lrStart);
   float b1t = 1.f, b2t = 1.f;
-  const int nch = (2 * m + 31) / 32;
 
   for (int it = 0; it < iters; ++it) {
     const float frac = iters > 1 ? (float)it / (float)(iters - 1) : 0.f;
     const float pexp = pStart * expf(lnPr * frac);
     const float lr = lrStart * expf(lnLr * frac);
 
-    zero_acc(C, COL_CONV, W);
-    zero_acc(C, COL_CORR, W);
-    fence_before();
-    __syncthreads();
+    prime(C, true);
     if (!conv_tc(C, S.sa, status)) break;
+    gather_conv(C, ln, S.cb);                     // b in cb
 
-    // M = max b
     float mloc = 0.f;
-    for (int c = ln.half; c < nch; c += 2) {
-      float v[32];
-      tmem_ld32(C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)(COL_CONV + 32 * c), v);
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int k = (32 * c + t) * L + ln.r;
-        if (k < nb) mloc = fmaxf(mloc, v[t]);
-      }
-    }
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) mloc = fmaxf(mloc, S.cb[pidx(k)]);
     const float M = block_max(mloc, S.red);
     if (!(M > 0.f)) break;
-    // c_k = (1+d)^(p-1), R = sum c_k (1+d); stored reversed for the correlation
+    // c_k = (1+d)^(p-1) in place, R = sum c_k (1+d), d = (b_k - M)/M
     float rloc = 0.f;
-    for (int c = ln.half; c < nch; c += 2) {
-      float v[32];
-      tmem_ld32(C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)(COL_CONV + 32 * c), v);
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int k = (32 * c + t) * L + ln.r;
-        if (k < nb) {
-          const float d = (v[t] - M) / M;
-          const float cw = d > -1.f ? pow_from_d(d, pexp - 1.f) : 0.f;
-          rloc += cw * (1.f + d);
-          S.crev[2 * L * m - 2 - k] = cw;
-        }
-      }
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+      const float d = (S.cb[pidx(k)] - M) / M;
+      const float cw = d > -1.f ? pow_from_d(d, pexp - 1.f) : 0.f;
+      rloc += cw * (1.f + d);
+      S.cb[pidx(k)] = cw;
     }
-    const float R = block_sum(rloc, S.red);   // barrier: crev complete
+    const float R = block_sum(rloc, S.red);      // barrier: weights complete
     b1t *= beta1;
     b2t *= beta2;
     const float bc1 = 1.f / (1.f - b1t), bc2 = 1.f / (1.f - b2t);
@@ -205,37 +186,29 @@ k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ sk
 
     fence_before();
     __syncthreads();
-    if (!corr_tc(C, S.sa, S.crev, status)) break;
+    if (!corr_tc(C, S.sa, S.cb, status)) break;
+    gather_corr(C, ln, S.cb);                     // G in cb (weights no longer needed)
 
     float sloc = 0.f;
-    for (int c = ln.half; c < nch; c += 2) {
-      float v[32];
-      tmem_ld32(C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)(COL_CORR + 32 * c), v);
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int col = 32 * c + t;
-        if (col < m - 1 || col >= 2 * m - 1) continue;
-        const int i = (2 * m - 2 - col) * L + L - 1 - ln.r;
-        if (i >= n) continue;
-        const float gi = v[t] / R - M;
-        float x;
-        if (mode == 0) {
-          const float mm = __fmaf_rn(beta1, mg[i], (1.f - beta1) * gi);
-          const float vv = __fmaf_rn(beta2, vg[i], (1.f - beta2) * gi * gi);
-          mg[i] = mm;
-          vg[i] = vv;
-          const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
-          x = S.sa[pidx(i)] - step;
-          if (x < 0.f) x = 0.f;
-        } else {
-          float e = -lr * (gi / M);
-          if (e > 4.f) e = 4.f;
-          if (e < -4.f) e = -4.f;
-          x = S.sa[pidx(i)] * expf(e);
-        }
-        S.sa[pidx(i)] = x;
-        sloc += x;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float gi = S.cb[pidx(i)] / R - M;
+      float x;
+      if (mode == 0) {
+        const float mm = __fmaf_rn(beta1, mg[i], (1.f - beta1) * gi);
+        const float vv = __fmaf_rn(beta2, vg[i], (1.f - beta2) * gi * gi);
+        mg[i] = mm;
+        vg[i] = vv;
+        const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
+        x = S.sa[pidx(i)] - step;
+        if (x < 0.f) x = 0.f;
+      } else {
+        float e = -lr * (gi / M);
+        if (e > 4.f) e = 4.f;
+        if (e < -4.f) e = -4.f;
+        x = S.sa[pidx(i)] * expf(e);
       }
+      S.sa[pidx(i)] = x;
+      sloc += x;
     }
     float Ssum = block_sum(sloc, S.red);
     if (!(Ssum > 0.f)) {
@@ -258,50 +231,32 @@ k_lp_forward_tc(const float* __restrict__ pop, int n, float p, float* __restrict
                 unsigned int* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const int pid = blockIdx.x;
-  Shared S = setup(n, false, three != 0, smem_raw);
+  Shared S = setup(n, three != 0, smem_raw);
   Ctx& C = S.C;
-  const int m = C.m, nb = 2 * n - 1, W = acc_width(m), nch = (2 * m + 31) / 32;
+  const int nb = 2 * n - 1;
   const Lane ln;
   const float* a = pop + (size_t)pid * n;
   __syncthreads();
   float sl = 0.f;
   for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; S.sa[pidx(i)] = x; sl += x; }
   const float Ssum = block_sum(sl, S.red);
-  zero_acc(C, COL_CONV, W);
-  fence_before();
-  __syncthreads();
+  prime(C, false);
   const bool ok = conv_tc(C, S.sa, status);
+  if (ok) gather_conv(C, ln, S.cb);
   float mloc = 0.f;
-  if (ok) {
-    for (int c = ln.half; c < nch; c += 2) {
-      float v[32];
-      tmem_ld32(C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)(COL_CONV + 32 * c), v);
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int k = (32 * c + t) * L + ln.r;
-        if (k < nb) {
-          mloc = fmaxf(mloc, v[t]);
-          if (b_out) b_out[(size_t)pid * nb + k] = v[t];
-        }
-      }
+  if (ok)
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+      const float v = S.cb[pidx(k)];
+      mloc = fmaxf(mloc, v);
+      if (b_out) b_out[(size_t)pid * nb + k] = v;
     }
-  }
   const float M = block_max(mloc, S.red);
   float rloc = 0.f;
-  if (ok) {
-    for (int c = ln.half; c < nch; c += 2) {
-      float v[32];
-      tmem_ld32(C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)(COL_CONV + 32 * c), v);
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int k = (32 * c + t) * L + ln.r;
-        if (k < nb) {
-          const float d = (v[t] - M) / M;
-          rloc += d > -1.f ? pow_from_d(d, p) : 0.f;
-        }
-      }
+  if (ok)
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+      const float d = (S.cb[pidx(k)] - M) / M;
+      rloc += d > -1.f ? pow_from_d(d, p) : 0.f;
     }
-  }
   const float R = block_sum(rloc, S.red);
   if (threadIdx.x == 0) {
     const float val = ok ? 2.f * (float)n * M * powf(R, 1.f / p) / (Ssum * Ssum)
@@ -322,61 +277,37 @@ k_lp_backward_tc(const float* __restrict__ pop, const float* __restrict__ saved,
                  int three, unsigned int* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const int pid = blockIdx.x;
-  Shared S = setup(n, true, three != 0, smem_raw);
+  Shared S = setup(n, three != 0, smem_raw);
   Ctx& C = S.C;
-  const int m = C.m, nb = 2 * n - 1, W = acc_width(m), nch = (2 * m + 31) / 32;
+  const int nb = 2 * n - 1;
   const Lane ln;
   const float* a = pop + (size_t)pid * n;
   const float M = saved[4 * pid + 0], Ssum = saved[4 * pid + 1], R = saved[4 * pid + 2];
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] = a[i];
   __syncthreads();
-  zero_acc(C, COL_CONV, W);
-  zero_acc(C, COL_CORR, W);
-  fence_before();
-  __syncthreads();
+  prime(C, true);
   bool ok = true;
   if (b_in) {
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-      const float d = (b_in[(size_t)pid * nb + k] - M) / M;
-      S.crev[2 * L * m - 2 - k] = d > -1.f ? pow_from_d(d, p - 1.f) : 0.f;
-    }
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) S.cb[pidx(k)] = b_in[(size_t)pid * nb + k];
+    __syncthreads();
   } else {
     ok = conv_tc(C, S.sa, status);
-    if (ok) {
-      for (int c = ln.half; c < nch; c += 2) {
-        float v[32];
-        tmem_ld32(C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)(COL_CONV + 32 * c), v);
-#pragma unroll
-        for (int t = 0; t < 32; ++t) {
-          const int k = (32 * c + t) * L + ln.r;
-          if (k < nb) {
-            const float d = (v[t] - M) / M;
-            S.crev[2 * L * m - 2 - k] = d > -1.f ? pow_from_d(d, p - 1.f) : 0.f;
-          }
-        }
-      }
-    }
+    if (ok) gather_conv(C, ln, S.cb);
+  }
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    const float d = (S.cb[pidx(k)] - M) / M;
+    S.cb[pidx(k)] = d > -1.f ? pow_from_d(d, p - 1.f) : 0.f;
   }
   fence_before();
   __syncthreads();
-  if (ok) ok = corr_tc(C, S.sa, S.crev, status);
+  if (ok) ok = corr_tc(C, S.sa, S.cb, status);
+  if (ok) gather_corr(C, ln, S.cb);
   const float scale = 4.f * (float)n * powf(R, 1.f / p) / (Ssum * Ssum);
   const float MS = M / Ssum;
   float* g = grad + (size_t)pid * n;
-  if (ok) {
-    for (int c = ln.half; c < nch; c += 2) {
-      float v[32];
-      tmem_ld32(C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)(COL_CORR + 32 * c), v);
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int col = 32 * c + t;
-        if (col < m - 1 || col >= 2 * m - 1) continue;
-        const int i = (2 * m - 2 - col) * L + L - 1 - ln.r;
-        if (i < n) g[i] = scale * (v[t] / R - MS);
-      }
-    }
-  }
+  if (ok)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] = scale * (S.cb[pidx(i)] / R - MS);
   teardown(S);
 }
 
@@ -405,12 +336,13 @@ int device_status(int reset) {
   return (int)v;
 }
 
-size_t smem_local_search_tc(int n) { return tc::Layout(n, true).total; }
-static size_t smem_lp_forward_tc(int n) { return tc::Layout(n, false).total; }
+size_t smem_local_search_tc(int n) { return tc::Layout(n).total; }
+static size_t smem_lp_forward_tc(int n) { return tc::Layout(n).total; }
 
+// the two accumulators must fit the 512 TMEM columns
 static int tc_n_ok(int n) {
-  const int m = (n + tc::L - 1) / tc::L;
-  return (n >= 1 && 2 * round_up(2 * m + 16, 32) <= 512) ? SIDON_OK : SIDON_ERR_N;
+  const int m = (n + tc::BL - 1) / tc::BL;
+  return (n >= 1 && tc::conv_width(m) + tc::corr_width(m) <= 512) ? SIDON_OK : SIDON_ERR_N;
 }
 
 static int prep_tc(const void* fn, size_t sm) {

@@ -2,53 +2,53 @@
 //  tc_engine.cuh -- block-Toeplitz convolution / correlation on the 5th-gen
 //  tensor cores (tcgen05, accumulators in TMEM), BF16 operands split hi + lo.
 //
-//  Blocks of L = 128 cells, m = ceil(n/L) blocks.
+//  Geometry.  Input blocks of BL = 64 cells, m = ceil(n/64) blocks.  A tile
+//  w is the 128 x 64 Hankel window of the heights
+//        A_w[R][s] = a[64 w - 63 + R + s]      (lanes R = 0..127, K index s),
+//  and the tiles are w = 0, 2, 4, ... (every second diagonal: 128 lanes span
+//  two 64-cell output blocks, so each product a_i a_j lands in exactly one
+//  accumulator cell).  The UMMA shape is M = 128, K = 16, N = (number of
+//  blocks) ~ m, which keeps every instruction above the tensor core's fixed
+//  per-instruction cost (measured: ~92 cycles per M128 K16 instruction,
+//  N/2 cycles of math).
 //
-//  Block matrix (the B operand, K-major, rows J, K index s):
-//      Bt[J][s] = a[J L + L - 1 - s]      (blocks of a, reversed inside a block)
-//  in the canonical no-swizzle core-matrix layout: 8x8 bf16 core matrices of
-//  128 B, LBO = 128 B between K-adjacent cores, SBO = 2048 B between 8-row
-//  groups.
+//  Convolution  b = a * a.  B operand: the reversed blocks
+//        Bt[J][s] = a[64 J + 63 - s],  J = 0..m-1.
+//  Tile d accumulates A_d Bt^T into TMEM columns J + d, so cell (R, col)
+//  collects products with index sum 64 col + R:
+//        b_k = D[k mod 64][k / 64] + D[k mod 64 + 64][k / 64 - 1].
 //
-//  Convolution  b_{K L + r} = sum_d sum_s A_d[r][s] Bt[K - d][s]  with the
-//  Hankel tile A_d[r][s] = a[(d-1) L + 1 + r + s], d = 0..m: tile d times
-//  the block rows J lands in accumulator column K = J + d (TMEM lane r holds
-//  b_{K L + r}).
+//  Correlation  G_i = sum_j c_{i+j} a_j = sum_k c_k a_{k-i}.  B operand: the
+//  weight blocks  Cb[K][s] = c[64 K + s], K = 0..2m-1.  Tile t (same windows
+//  of a) accumulates A_t Cb[col + t]^T into column col, and cell (R, col)
+//  collects the output i = 64 col + 63 - R:
+//        G_i = D2[R0][col0] + D2[R0 + 64][col0 + 1],  R0 = (63 - i) mod 64.
 //
-//  Correlation  G_i = sum_j c_{i+j} a_j  with i = I L + L - 1 - r' and
-//  c_rev[t] = c[2 m L - 2 - t]: the Hankel tile H_e[r'][s] = c_rev[e L + r' + s]
-//  (e = 0..2m-2) times block row J lands in column e + J; column
-//  col in [m-1, 2m-1) holds block I = 2m - 2 - col.  Only the rows that reach
-//  a valid column are multiplied.
+//  Shifts.  A tile's B rows are shifted by its diagonal.  Shifts in multiples
+//  of 8 rows are descriptor offsets (8-row core-matrix groups); accumulator
+//  column offsets are kept multiples of DG (TMEM alignment); the residue
+//  (tile mod 8, one of 0, 2, 4, 6) is absorbed by a row-shifted copy of the
+//  B matrix, built once per residue class:
+//        conv:  BC_rho[x] = Bt[x - rho - ZP]  (ZP zero rows in front),
+//        corr:  CC_rho[x] = Cb[x + rho].
 //
-//  Accumulator column offsets are kept multiples of DG (TMEM alignment).
-//  A tile w whose target column is w + J is issued at column off (a multiple
-//  of DG), so its B rows start at block t = off - w <= 0.  The residue
-//  (-t) mod 8 = w mod 8 is absorbed by a row-shifted copy of the block matrix,
-//      BC_rho[x] = Bt[x - rho - Z]   (Z zero rows in front),
-//  whose descriptor starts at row t + rho + Z (a multiple of 8).  Tiles run in
-//  residue classes rho = 0..7, so each copy is built once per class.
-//
-//  A Hankel tile is never materialised as an L x L matrix.  A K-major core
-//  matrix (row group R, K group S) of a Hankel tile holds
-//  x[start + 8(R+S) + i + j], so the tile is the sequence of 8x8 "shifted
-//  windows" CM[q][i][j] = x[base + 8q + i + j] addressed with
-//  LBO = SBO = 128 B: one tile needs 31 consecutive windows (4 KB per plane)
-//  built from 255 consecutive values.
+//  A Hankel window is never materialised as a 128 x 64 matrix.  A K-major
+//  core matrix (row group G, K group S) of it holds a[start + 8(G+S) + i + j],
+//  so the window is the sequence of 23 8x8 "shifted windows"
+//  CM[q][i][j] = a[start + 8q + i + j] addressed with LBO = SBO = 128 B.
 //
 //  Arithmetic: x = x_hi + x_lo with x_hi = bf16(x), x_lo = bf16(x - x_hi).
 //  The convolution is symmetric (sum_{i+j=k} h_i l_j = sum_{i+j=k} l_i h_j),
 //  so BF16x3 needs two products: b = A_hi B_hi + A_lo2 B_hi with the window
 //  plane A_lo2 = bf16(2 x_lo) (exact doubling); the correlation uses
-//  A_hi B_hi + A_hi B_lo + A_lo B_hi.  BF16x1 keeps A_hi B_hi.  fp32
+//  A_hi B_hi + A_lo B_hi + A_hi B_lo.  BF16x1 keeps A_hi B_hi.  fp32
 //  accumulation in TMEM.
 //
-//  Synchronisation: a ring of STAGES window buffers; every tile's MMAs are
-//  followed by tcgen05.commit on the stage's mbarrier, which the builders
-//  wait on (bounded) before refilling that stage; the block-matrix copies
-//  have their own mbarriers.  One elected thread issues all MMAs.  Every
-//  wait gives up after ~2^31 clock cycles, records SIDON_ERR_TIMEOUT in the
-//  library's device status word and unwinds.
+//  Pipeline: one MMA warp (one elected lane issues every MMA) and builder
+//  warps; a ring of STAGES window buffers and two copy slots, each guarded by
+//  a full barrier (builder arrivals) and an empty barrier (tcgen05.commit).
+//  Every wait gives up after ~2^31 clock cycles, records SIDON_ERR_TIMEOUT in
+//  the library's device status word and unwinds.
 // ---------------------------------------------------------------------------
 #pragma once
 #include <cuda_bf16.h>
@@ -58,11 +58,13 @@
 namespace sidon {
 namespace tc {
 
-constexpr int L = 128;               // block size (= UMMA M)
+constexpr int L = 128;               // UMMA M (lanes)
+constexpr int BL = 64;               // input block = K of a tile
+constexpr int KSTEPS = BL / 16;      // K16 instructions per tile and product
 constexpr int STAGES = 3;            // window ring depth
 constexpr int DG = 16;               // accumulator column granule of an MMA destination
 constexpr int ZP = DG;               // zero rows in front of a block-matrix copy
-constexpr int WIN_CM = 32;           // core matrices per window (31 used)
+constexpr int WIN_CM = 24;           // core matrices per window (23 used)
 constexpr int PLANE = WIN_CM * 128;  // bytes per hi or lo window plane
 constexpr int STAGE_BYTES = 2 * PLANE;
 constexpr int NTHREADS = 256;        // 8 warps: lanes quadrant = warp % 4
@@ -86,6 +88,8 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
 __device__ __forceinline__ uint32_t idesc_bf16(int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(L >> 4) << 24);
 }
+// B plane of 64-wide rows: core matrix (row group g, K group h) at g*1024 + h*128
+constexpr uint32_t B_SBO = 1024;
 
 __device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
                                          uint32_t idesc, uint32_t accumulate) {
@@ -181,14 +185,14 @@ __device__ __forceinline__ void split_bf16(float x, uint16_t& hi, uint16_t& lo) 
   lo = __bfloat16_as_ushort(l);
 }
 
-// Heights live in shared memory in a padded block layout: logical cell i at
-// physical index i + 4 floor(i / 128) (block stride 132 floats = 33 x 16 B),
-// so that loading the same 16 B of eight consecutive blocks hits eight
-// distinct bank groups.
-__device__ __forceinline__ int pidx(int i) { return i + 4 * (i >> 7); }
+// Heights and weights live in shared memory in a padded block layout: logical
+// index i at physical i + 4 floor(i / 64) (block stride 68 floats = 17 x 16 B),
+// so that the same 16 B of eight consecutive blocks fall in eight distinct
+// bank groups when a copy gathers a column of blocks.
+__device__ __forceinline__ int pidx(int i) { return i + 4 * (i >> 6); }
 
 // Warp roles during the tile phases: warp MMA_WARP (lane 0) issues every
-// MMA; the other warps build windows and block-matrix copies.
+// MMA; the other warps build windows and B-matrix copies.
 constexpr int MMA_WARP = NTHREADS / 32 - 1;
 constexpr int NBUILD_WARPS = NTHREADS / 32 - 1;
 constexpr int NBUILD = NBUILD_WARPS * 32;
@@ -197,7 +201,7 @@ constexpr int NBUILD = NBUILD_WARPS * 32;
 // of a role are kept identical by every thread of that role.
 struct Ctx {
   unsigned char* stages;   // STAGES x (hi plane | lo plane), 1 KB aligned
-  unsigned char* bc;       // block-matrix copies: 2 planes of rc x 256 B
+  unsigned char* bc;       // B-matrix copies (two conv slots or one corr hi|lo pair)
   uint64_t* full;          // STAGES "window ready" barriers (NBUILD_WARPS arrivals)
   uint64_t* empty;         // STAGES "window consumed" barriers (tcgen05.commit)
   uint64_t* bc_full;       // 2 "copy ready" barriers (NBUILD_WARPS arrivals)
@@ -209,11 +213,16 @@ struct Ctx {
   int done_use;
   int st_next;             // next stage in the ring
   int* abort;              // shared abort flag
-  int m, rc, n;
+  int m, rc, rcc, n, dmax; // blocks, conv / corr copy rows, cells, last tile
   bool three;              // BF16x3 (else BF16x1)
 };
 
-__device__ __forceinline__ int bc_rows(int m) { return round_up(ZP + m + 24, 8); }
+__host__ __device__ __forceinline__ int conv_copy_rows(int m) { return round_up(ZP + m + 40, 8); }
+__host__ __device__ __forceinline__ int corr_copy_rows(int m) { return round_up(2 * m + 24, 8); }
+__host__ __device__ __forceinline__ int last_tile(int n) { return (((n + 62) / 64) + 1) / 2 * 2; }
+__host__ __device__ __forceinline__ int conv_width(int m) { return round_up(2 * m + 17, 32); }
+__host__ __device__ __forceinline__ int corr_n(int m) { return round_up(m + 1, 16); }
+__host__ __device__ __forceinline__ int corr_width(int m) { return round_up(corr_n(m), 32); }
 
 // bounded wait on an mbarrier phase; sets the abort flag on timeout
 __device__ __forceinline__ bool wait_phase(Ctx& C, uint64_t* bar, uint32_t parity,
@@ -235,8 +244,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-__device__ __forceinline__ uint32_t pack_bf16x2(float lo_elem, float hi_elem) {
-  const __nv_bfloat162 v = __floats2bfloat162_rn(lo_elem, hi_elem);   // .x = first argument
+__device__ __forceinline__ uint32_t pack_bf16x2(float first, float second) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(first, second);   // .x = first (low half)
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 __device__ __forceinline__ float bf_lo_f(uint32_t p) { return __uint_as_float(p << 16); }
@@ -255,27 +264,51 @@ __device__ __forceinline__ void split8(const float (&v)[8], float lsc, uint4& hi
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// Row-shifted block-matrix copy into slot `slot` (hi plane, and lo plane in
-// the next slot's space when want_lo): BC[x][s] = a[(x - rho - ZP) L + L-1-s]
-// for block rows in [0, m).  Chunk c = ((x>>3)*16 + h)*8 + (x&7) sits at byte
-// 16 c, so consecutive builder threads store consecutive 16 B; the 8
-// heights of a chunk are two aligned float4 of one block (padded layout).
-__device__ __forceinline__ void build_bc(Ctx& C, const float* sa, int rho, int slot, bool want_lo,
-                                         int bt) {
-  const int rc = C.rc;
-  unsigned char* hi = C.bc + (size_t)slot * rc * 256;
-  unsigned char* lo = hi + (size_t)rc * 256;
-  const int chunks = rc * 16;
+// chunk c of a 64-wide B plane: row x, K group h; byte offset 16 c
+__device__ __forceinline__ void chunk_xh(int c, int& x, int& h) {
+  x = ((c >> 6) << 3) | (c & 7);
+  h = (c >> 3) & 7;
+}
+
+// Convolution copy in slot `slot` (hi plane only):
+// BC[x][s] = a[64 (x - rho - ZP) + 63 - s] for block rows in [0, m).
+__device__ __forceinline__ void build_conv_copy(Ctx& C, const float* sa, int rho, int slot, int bt) {
+  unsigned char* hi = C.bc + (size_t)slot * C.rc * 128;
+  const int chunks = C.rc * 8;
   for (int c = bt; c < chunks; c += NBUILD) {
-    const int x = ((c >> 7) << 3) | (c & 7), h = (c >> 3) & 15;
+    int x, h;
+    chunk_xh(c, x, h);
     const int J = x - rho - ZP;
-    uint4 vh = make_uint4(0, 0, 0, 0), vl = vh;
+    uint4 vh = make_uint4(0, 0, 0, 0), vl;
     if (J >= 0 && J < C.m) {
-      // s = 8h .. 8h+7  <->  cells J L + L-1-8h down to J L + L-8-8h
-      const float* src = sa + pidx(J * L) + (L - 8 - 8 * h);
+      // s = 8h .. 8h+7  <->  cells 64J + 63 - 8h down to 64J + 56 - 8h
+      const float* src = sa + pidx(64 * J + 56 - 8 * h);
       const float4 u0 = *reinterpret_cast<const float4*>(src);
       const float4 u1 = *reinterpret_cast<const float4*>(src + 4);
       const float v[8] = {u1.w, u1.z, u1.y, u1.x, u0.w, u0.z, u0.y, u0.x};
+      split8(v, 1.f, vh, vl);
+    }
+    *reinterpret_cast<uint4*>(hi + 16 * c) = vh;
+  }
+}
+
+// Correlation copy (hi plane, lo plane right after it):
+// CC[x][s] = c[64 (x + rho) + s] for weight blocks in [0, 2m).
+__device__ __forceinline__ void build_corr_copy(Ctx& C, const float* cb, int rho, bool want_lo,
+                                                int bt) {
+  unsigned char* hi = C.bc;
+  unsigned char* lo = hi + (size_t)C.rcc * 128;
+  const int chunks = C.rcc * 8;
+  for (int c = bt; c < chunks; c += NBUILD) {
+    int x, h;
+    chunk_xh(c, x, h);
+    const int K = x + rho;
+    uint4 vh = make_uint4(0, 0, 0, 0), vl = vh;
+    if (K < 2 * C.m) {
+      const float* src = cb + pidx(64 * K + 8 * h);
+      const float4 u0 = *reinterpret_cast<const float4*>(src);
+      const float4 u1 = *reinterpret_cast<const float4*>(src + 4);
+      const float v[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
       split8(v, 1.f, vh, vl);
     }
     *reinterpret_cast<uint4*>(hi + 16 * c) = vh;
@@ -283,18 +316,17 @@ __device__ __forceinline__ void build_bc(Ctx& C, const float* sa, int rho, int s
   }
 }
 
-// Window of tile w into stage st: CM[q'][i][j] = x[8 (16 w + q') + off + i + j]
-// (x indexed through map()), planes hi and lsc*lo.
-template <typename MapFn>
-__device__ __forceinline__ void build_window(Ctx& C, int st, const float* x, MapFn&& map, int off,
-                                             int w, float lsc, int bt) {
+// Window of tile w into stage st: CM[q][i][j] = a[64 w - 63 + 8 q + i + j],
+// planes hi and lsc * lo.
+__device__ __forceinline__ void build_window(Ctx& C, int st, const float* sa, int w, float lsc,
+                                             int bt) {
   unsigned char* hi = C.stages + st * STAGE_BYTES;
   unsigned char* lo = hi + PLANE;
   for (int t = bt; t < WIN_CM * 8; t += NBUILD) {
-    const int base = 8 * (16 * w + (t >> 3)) + off + (t & 7);
+    const int base = 64 * w - 63 + 8 * (t >> 3) + (t & 7);
     float v[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = x[map(base + j)];
+    for (int j = 0; j < 8; ++j) v[j] = sa[pidx(base + j)];
     uint4 vh, vl;
     split8(v, lsc, vh, vl);
     *reinterpret_cast<uint4*>(hi + 16 * t) = vh;
@@ -317,55 +349,75 @@ struct Tile {
   int dcol, x0, N;
 };
 
+// accumulator column bases
+constexpr int COL_CONV = 0;
+__device__ __forceinline__ int col_corr(int m) { return conv_width(m); }
+
 // Issue the MMAs of one tile (one thread).  corr selects the 3-product
 // correlation arithmetic, otherwise the 2-product symmetric convolution.
-__device__ __forceinline__ void issue_tile(Ctx& C, int st, int slot, const Tile& T, bool corr) {
+__device__ __forceinline__ void issue_tile(Ctx& C, int st, uint32_t b_hi, uint32_t b_lo,
+                                           const Tile& T, bool corr) {
   const uint32_t a_hi = smem_u32(C.stages + st * STAGE_BYTES);
   const uint32_t a_lo = a_hi + PLANE;
-  const uint32_t b_hi = smem_u32(C.bc + (size_t)slot * C.rc * 256) + (uint32_t)(T.x0 >> 3) * 2048u;
-  const uint32_t b_lo = b_hi + (uint32_t)C.rc * 256u;
+  const uint32_t bh0 = b_hi + (uint32_t)(T.x0 >> 3) * B_SBO;
+  const uint32_t bl0 = b_lo + (uint32_t)(T.x0 >> 3) * B_SBO;
   const uint32_t id = idesc_bf16(T.N);
   const uint32_t d = C.tmem + (uint32_t)T.dcol;
 #pragma unroll
-  for (int kc = 0; kc < L / 16; ++kc) {
+  for (int kc = 0; kc < KSTEPS; ++kc) {
     const uint64_t ah = sdesc(a_hi + kc * 256, 128, 128);
-    const uint64_t bh = sdesc(b_hi + kc * 256, 128, 2048);
+    const uint64_t bh = sdesc(bh0 + kc * 256, 128, B_SBO);
     mma_bf16(d, ah, bh, id, 1u);
     if (C.three) {
       const uint64_t al = sdesc(a_lo + kc * 256, 128, 128);
       mma_bf16(d, al, bh, id, 1u);
       if (corr) {
-        const uint64_t bl = sdesc(b_lo + kc * 256, 128, 2048);
+        const uint64_t bl = sdesc(bl0 + kc * 256, 128, B_SBO);
         mma_bf16(d, ah, bl, id, 1u);
       }
     }
   }
 }
 
-// Run tiles w = 0..ntiles-1 in residue classes w mod 8 through the
-// warp-specialised pipeline.  geom(w) gives the tile; the window source is
-// x[map(.)] with offset off.  Ends with every MMA of the sequence complete
+// Run the tiles w = 0, 2, ..., dmax in residue classes w mod 8 through the
+// warp-specialised pipeline.  Ends with every MMA of the sequence complete
 // (bar_done) and the accumulator readable by all warps.
-template <typename GeomFn, typename MapFn>
-__device__ bool run_tiles(Ctx& C, int ntiles, const float* sa, const float* x, MapFn&& map,
-                          int off, bool corr, GeomFn&& geom, unsigned int* status) {
+//   corr = false: convolution, copies from the heights sa (two slots);
+//   corr = true:  correlation, copies from the padded weights cb (one slot).
+__device__ bool run_tiles(Ctx& C, const float* sa, const float* cb, bool corr,
+                          unsigned int* status) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool want_lo = corr && C.three;
   const float lsc = corr ? 1.f : 2.f;
+  const int m = C.m;
   int st = C.st_next;
   if (warp == MMA_WARP) {
     if (lane == 0) {
       fence_after();
-      for (int rho = 0; rho < 8 && rho < ntiles; ++rho) {
-        const int slot = corr ? 0 : (rho & 1);
+      const int cb_cols = corr_n(m);
+      for (int rho = 0; rho < 8 && rho <= C.dmax; rho += 2) {
+        const int slot = corr ? 0 : ((rho >> 1) & 1);
         if (!wait_phase(C, &C.bc_full[slot], (uint32_t)(C.bc_uses[slot] & 1), status)) break;
         C.bc_uses[slot] += 1;
+        const uint32_t bbase = smem_u32(C.bc) + (corr ? 0u : (uint32_t)slot * C.rc * 128u);
+        const uint32_t blo = bbase + (uint32_t)C.rcc * 128u;
         bool ok = true;
-        for (int w = rho; w < ntiles; w += 8) {
+        for (int w = rho; w <= C.dmax; w += 8) {
+          Tile T;
+          if (corr) {
+            T.dcol = col_corr(m);
+            T.x0 = w - rho;
+            T.N = cb_cols;
+          } else {
+            const int off = (w / DG) * DG, t = off - w;
+            T.dcol = COL_CONV + off;
+            T.x0 = t + rho + ZP;
+            T.N = round_up(m - t, 16);
+          }
           if (!wait_phase(C, &C.full[st], (uint32_t)(C.uses[st] & 1), status)) { ok = false; break; }
           C.uses[st] += 1;
           fence_after();
-          issue_tile(C, st, slot, geom(w), corr);
+          issue_tile(C, st, bbase, blo, T, corr);
           mma_commit(&C.empty[st]);
           st = (st + 1 == STAGES) ? 0 : st + 1;
         }
@@ -377,24 +429,25 @@ __device__ bool run_tiles(Ctx& C, int ntiles, const float* sa, const float* x, M
     __syncwarp();
   } else {
     const int bt = threadIdx.x - (warp > MMA_WARP ? 32 : 0);   // 0 .. NBUILD-1
-    for (int rho = 0; rho < 8 && rho < ntiles; ++rho) {
-      const int slot = corr ? 0 : (rho & 1);
+    for (int rho = 0; rho < 8 && rho <= C.dmax; rho += 2) {
+      const int slot = corr ? 0 : ((rho >> 1) & 1);
       const int u = C.bc_uses[slot];
       if (u > 0 && !wait_phase(C, &C.bc_empty[slot], (uint32_t)((u - 1) & 1), status)) break;
       C.bc_uses[slot] = u + 1;
-      build_bc(C, sa, rho, slot, want_lo, bt);
+      if (corr) build_corr_copy(C, cb, rho, want_lo, bt);
+      else build_conv_copy(C, sa, rho, slot, bt);
       fence_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&C.bc_full[slot]);
       bool ok = true;
-      for (int w = rho; w < ntiles; w += 8) {
+      for (int w = rho; w <= C.dmax; w += 8) {
         const int us = C.uses[st];
         if (us > 0 && !wait_phase(C, &C.empty[st], (uint32_t)((us - 1) & 1), status)) {
           ok = false;
           break;
         }
         C.uses[st] = us + 1;
-        build_window(C, st, x, map, off, w, lsc, bt);
+        build_window(C, st, sa, w, lsc, bt);
         fence_async_smem();
         __syncwarp();
         if (lane == 0) mbar_arrive(&C.full[st]);
@@ -411,45 +464,80 @@ __device__ bool run_tiles(Ctx& C, int ntiles, const float* sa, const float* x, M
   return ok && !*((volatile int*)C.abort);
 }
 
-// accumulator column bases
-constexpr int COL_CONV = 0;
-constexpr int COL_CORR = 256;
+// lane quadrant / column-half of the calling warp (8 warps: 4 quadrants x 2)
+struct Lane {
+  int quad, half, r;
+  __device__ Lane() {
+    const int w = threadIdx.x >> 5;
+    quad = w & 3;
+    half = w >> 2;
+    r = 32 * quad + (threadIdx.x & 31);
+  }
+};
 
-__device__ __forceinline__ int acc_width(int m) { return round_up(2 * m + 16, 32); }
-
-// b = a * a into accumulator columns of COL_CONV (column K, lane r = b_{K L + r})
-__device__ __forceinline__ bool conv_tc(Ctx& C, const float* sa, unsigned int* status) {
-  const int m = C.m;
-  return run_tiles(C, m + 1, sa, sa, [](int i) { return pidx(i); }, -(L - 1), false,
-                   [&](int d) {
-                     Tile T;
-                     const int off = (d / DG) * DG;
-                     const int t = off - d;                       // (-DG, 0]
-                     T.dcol = COL_CONV + off;
-                     T.x0 = t + (d & 7) + ZP;
-                     T.N = round_up(m - t, 16);
-                     return T;
-                   },
-                   status);
+// b = a * a into X (padded layout, k < 2n-1): the two cells of each k are
+// combined through X.  Ends synchronised.
+__device__ __forceinline__ void gather_conv(Ctx& C, const Lane& ln, float* X) {
+  const int nb = 2 * C.n - 1, nch = (2 * C.m + 1 + 31) / 32;
+  const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16);
+  if (ln.quad >= 2) {
+    if (ln.half == 0) X[pidx(ln.r - 64)] = 0.f;          // k < 64 has one cell only
+    for (int c = ln.half; c < nch; c += 2) {
+      float v[32];
+      tmem_ld32(lanebase + (uint32_t)(COL_CONV + 32 * c), v);
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const int k = 64 * (32 * c + t) + ln.r;             // cell (r, col) -> k = 64 col + r
+        if (k < nb) X[pidx(k)] = v[t];
+      }
+    }
+  }
+  __syncthreads();
+  if (ln.quad < 2) {
+    for (int c = ln.half; c < nch; c += 2) {
+      float v[32];
+      tmem_ld32(lanebase + (uint32_t)(COL_CONV + 32 * c), v);
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const int k = 64 * (32 * c + t) + ln.r;
+        if (k < nb) X[pidx(k)] += v[t];
+      }
+    }
+  }
+  __syncthreads();
 }
 
-// G = corr(c, a) into the accumulator columns of COL_CORR; crev is the
-// reversed weight sequence (zero margins), sa the heights.
-__device__ __forceinline__ bool corr_tc(Ctx& C, const float* sa, const float* crev,
+// G_i into Y (padded layout, i < n) from the correlation accumulator.
+__device__ __forceinline__ void gather_corr(Ctx& C, const Lane& ln, float* Y) {
+  const int n = C.n, nch = (corr_n(C.m) + 31) / 32;
+  const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)col_corr(C.m);
+  for (int pass = 0; pass < 2; ++pass) {
+    if ((pass == 0) == (ln.quad >= 2)) {
+      for (int c = ln.half; c < nch; c += 2) {
+        float v[32];
+        tmem_ld32(lanebase + (uint32_t)(32 * c), v);
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+          const int i = 64 * (32 * c + t) + 63 - ln.r;   // cell (r, col) -> i = 64 col + 63 - r
+          if (i >= 0 && i < n) {
+            if (pass == 0) Y[pidx(i)] = v[t];
+            else Y[pidx(i)] += v[t];
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// b = a * a (accumulator at COL_CONV)
+__device__ __forceinline__ bool conv_tc(Ctx& C, const float* sa, unsigned int* status) {
+  return run_tiles(C, sa, nullptr, false, status);
+}
+// G = corr(c, a) (accumulator at col_corr); cb: padded weights (zero beyond 2n-1)
+__device__ __forceinline__ bool corr_tc(Ctx& C, const float* sa, const float* cb,
                                         unsigned int* status) {
-  const int m = C.m;
-  return run_tiles(C, 2 * m - 1, sa, crev, [](int i) { return i; }, 0, true,
-                   [&](int e) {
-                     Tile T;
-                     const int lo = max(0, m - 1 - e), hi = min(m, 2 * m - 1 - e);
-                     const int off = ((e + lo) / DG) * DG;
-                     const int t = off - e;                       // (lo - DG, lo]
-                     T.dcol = COL_CORR + off;
-                     T.x0 = t + (e & 7) + ZP;
-                     T.N = round_up(hi - t, 16);
-                     return T;
-                   },
-                   status);
+  return run_tiles(C, sa, cb, true, status);
 }
 
 }  // namespace tc
