@@ -39,7 +39,9 @@ enum sidon_status {
   SIDON_ERR_DTYPE = 5,        /* dtype / precision not supported by this call  */
   SIDON_ERR_NONFINITE = 6,    /* input held NaN/Inf/negative heights           */
   SIDON_ERR_TIMEOUT = 7,      /* a bounded device-side wait ran out            */
-  SIDON_ERR_DEVICE = 8        /* current device is not an sm_100 part          */
+  SIDON_ERR_DEVICE = 8,       /* current device is not an sm_100 part          */
+  SIDON_ERR_CAPACITY = 9      /* P * n beyond the fixed scratch of the
+                                 allocation-free local search                   */
 };
 
 enum sidon_dtype { SIDON_F32 = 0, SIDON_F64 = 1 };
@@ -119,6 +121,28 @@ SIDON_API int sidon_local_search(void* pop, void* mom, void* vel, const int* ski
                        int n, int P, int iters, double p_start, double p_end, double lr_start,
                        double lr_end, double beta1, double beta2, int mode_default, int dtype,
                        int precision, void* stream);
+
+/* The fused local search of sidon_local_search for callers that cannot
+ * allocate device memory -- e.g. a plugin inside an application whose
+ * allocator owns every device byte, or a hot path that must never call
+ * cudaMalloc/cudaFree because they can synchronise the device.  Such a caller
+ * passes only its population (fp32, [P][n], in place, plus the optional skip
+ * and mode_arr); the Adam moments live in a fixed 8 MiB device array inside
+ * the library, held by every GPU that loads it until the process exits.
+ * Limit: P * n <= 1048576 cells per call, else SIDON_ERR_CAPACITY.  precision:
+ * FP32_SIMT, BF16X1 or BF16X3.  Nothing is allocated: the first call on a
+ * device (with that device current) looks up the array's device address with
+ * cudaGetSymbolAddress and caches it, so make that first call before any
+ * stream capture.  All calls share the one array: the kernels zero a
+ * candidate's moments before using them, and calls that overlap on the GPU
+ * (concurrent streams) race on it.
+ * No counterpart in the reference (its driver always allocates the moment
+ * buffers, src/main.cu:118-137). */
+SIDON_API int sidon_local_search_noalloc(float* pop, const int* skip, const int* mode_arr, int n,
+                                         int P, int iters, double p_start, double p_end,
+                                         double lr_start, double lr_end, double beta1,
+                                         double beta2, int mode_default, int precision,
+                                         void* stream);
 
 /* Smoothed objective G_p(a) = 2n ||a*a||_p / (sum a)^2 for a batch (fp32
  * heights, any scale).  Writes value[P] (device) and saved[P*4] (device,

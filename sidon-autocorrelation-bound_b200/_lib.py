@@ -14,6 +14,7 @@ LIB_PATH = HERE / "libsidon_b200.so"
 
 # status codes (enum sidon_status)
 OK, ERR_ARG, ERR_N, ERR_SMEM, ERR_CUDA, ERR_DTYPE, ERR_NONFINITE, ERR_TIMEOUT, ERR_DEVICE = range(9)
+ERR_CAPACITY = 9
 F32, F64 = 0, 1
 PREC_FP32_SIMT, PREC_BF16X1, PREC_BF16X3, PREC_FP64_SIMT = 0, 1, 2, 3
 OP_LOCAL_SEARCH, OP_EVAL, OP_FRANK_WOLFE, OP_LOCAL_SEARCH_TC = 0, 1, 2, 3
@@ -33,6 +34,8 @@ SIGNATURES = {
     "sidon_certify": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "sidon_local_search": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _d, _i,
                                 _i, _i, _vp]),
+    "sidon_local_search_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _d, _i, _i,
+                                        _vp]),
     "sidon_lp_forward": (_i, [_vp, _i, _i, _d, _vp, _vp, _vp, _i, _vp]),
     "sidon_lp_backward": (_i, [_vp, _vp, _vp, _i, _i, _d, _vp, _i, _vp]),
     "sidon_frank_wolfe": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp]),

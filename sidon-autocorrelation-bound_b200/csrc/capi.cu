@@ -103,6 +103,7 @@ const char* sidon_status_string(int status) {
     case SIDON_ERR_NONFINITE: return "non-finite or negative heights";
     case SIDON_ERR_TIMEOUT: return "device-side wait timed out";
     case SIDON_ERR_DEVICE: return "current device is not sm_100";
+    case SIDON_ERR_CAPACITY: return "P * n exceeds the fixed scratch of the allocation-free call";
     default: return "unknown status";
   }
 }

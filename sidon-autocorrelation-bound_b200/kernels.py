@@ -113,6 +113,27 @@ def run_local_search(pop: torch.Tensor, iters: int, p_start: float, p_end: float
               int(mode_default), code, PRECISIONS[precision], _stream(stream))
 
 
+# P * n limit of run_local_search_noalloc (the library's fixed moment array)
+NOALLOC_MAX_CELLS = 1 << 20
+
+
+def run_local_search_noalloc(pop: torch.Tensor, iters: int, p_start: float, p_end: float,
+                             lr_start: float, lr_end: float, mode_arr: torch.Tensor | None = None,
+                             skip: torch.Tensor | None = None, beta1: float = 0.9,
+                             beta2: float = 0.999, mode_default: int = 0, precision: str = "fp32",
+                             stream=None) -> None:
+    """run_local_search for callers that cannot allocate device memory: only
+    the population is passed; the Adam moments live in a fixed device array
+    inside the library (P * n <= NOALLOC_MAX_CELLS).  Calls share that array,
+    so calls overlapping on the GPU race on it.  fp32 heights only."""
+    n, P = _pop_shape(pop)
+    _lib.call("sidon_local_search_noalloc", _dev(pop, "pop", torch.float32),
+              _opt(skip, "skip", torch.int32), _opt(mode_arr, "mode_arr", torch.int32), n, P,
+              int(iters), float(p_start), float(p_end), float(lr_start), float(lr_end),
+              float(beta1), float(beta2), int(mode_default), PRECISIONS[precision],
+              _stream(stream))
+
+
 def run_eval(pop: torch.Tensor, active_tol: float = 1e-4, with_nactive: bool = True,
              out_F: torch.Tensor | None = None, out_nactive: torch.Tensor | None = None,
              stream=None):
