@@ -237,9 +237,9 @@ def our_arm(args) -> None:
     ms_max = t.item()
     launches = 1
 
-    # search-time F error vs fp64 on the final population
+    # search-time F (the step's own arithmetic) error vs fp64 on the final population
     Fcert, _ = kernels.run_eval(pop, with_nactive=False)
-    _, saved, _ = kernels.lp_forward(pop, 2.0, precision="fp32")
+    _, saved, _ = kernels.lp_forward(pop, 2.0, precision=prec)
     S = saved[:, 1].double()
     F32 = 2.0 * N_CELLS * saved[:, 0].double() / (S * S)
     f_rel = (F32 - Fcert).abs().div(Fcert).max().item()

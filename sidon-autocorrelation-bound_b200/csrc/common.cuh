@@ -70,12 +70,50 @@ __device__ __forceinline__ T block_sum(T v, T* scratch) {
 // src/kernels.cuh:36-44).  The accurate libdevice exp/log1p are used.
 __device__ __forceinline__ float pow_from_d(float d, float q) { return expf(q * log1pf(d)); }
 __device__ __forceinline__ double pow_from_d(double d, double q) { return exp(q * log1p(d)); }
+// Search-time weights of the tensor-core kernels: the reference's own form,
+// __expf(q * log1pf(d)) (src/kernels.cuh:43); log1pf keeps d near 0 exact.
+__device__ __forceinline__ float pow_from_d_fast(float d, float q) { return __expf(q * log1pf(d)); }
 __device__ __forceinline__ float dev_exp(float x) { return expf(x); }
 __device__ __forceinline__ double dev_exp(double x) { return exp(x); }
 __device__ __forceinline__ float dev_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double dev_sqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float dev_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double dev_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// Refined maximum of b = a * a for the reported objective: every k whose
+// approximate b_k (from a fp32 or tensor-core convolution) lies within
+// `rel` of the approximate maximum is recomputed with fp64 accumulation of
+// the exact fp32 products; the largest recomputed value is returned to all
+// threads.  aval(i) reads height i (0 <= i < n); bval(k) the approximate b_k.
+// list: >= cap ints of shared scratch; cnt: one shared int; red: >= 32
+// doubles.  If more than cap candidates qualify, the approximate maximum is
+// kept for the rest (they are scanned in order, the first cap recomputed).
+template <typename AFn, typename BFn>
+__device__ double refine_max(int n, AFn&& aval, BFn&& bval, float approx, float rel, int* list,
+                             int cap, int* cnt, double* red) {
+  const int nb = 2 * n - 1;
+  const float thr = approx * (1.f - rel);
+  if (threadIdx.x == 0) *cnt = 0;
+  __syncthreads();
+  for (int k = threadIdx.x; k < nb; k += blockDim.x)
+    if (bval(k) >= thr) {
+      const int s = atomicAdd(cnt, 1);
+      if (s < cap) list[s] = k;
+    }
+  __syncthreads();
+  const int total = *cnt, c = total < cap ? total : cap;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, NW = blockDim.x >> 5;
+  double best = total > cap ? (double)approx : 0.0;
+  for (int q = wid; q < c; q += NW) {
+    const int k = list[q];
+    const int lo = k - (n - 1) > 0 ? k - (n - 1) : 0, hi = k < n - 1 ? k : n - 1;
+    double acc = 0.0;
+    for (int i = lo + lane; i <= hi; i += 32) acc = __fma_rn((double)aval(i), (double)aval(k - i), acc);
+    acc = warp_sum(acc);
+    best = acc > best ? acc : best;
+  }
+  return block_max(best, red);
+}
 
 // round-up helper
 __host__ __device__ constexpr inline int round_up(int x, int m) { return (x + m - 1) / m * m; }

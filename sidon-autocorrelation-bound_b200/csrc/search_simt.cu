@@ -128,13 +128,20 @@ k_local_search(T* pop, T* mom, T* vel, const int* __restrict__ skip,
 }
 
 // ----------------------------- G_p forward --------------------------------
-// value = 2n M R^(1/p) / S^2 with M = max b, R = sum (b/M)^p, S = sum a.
+// value = 2n M R^(1/p) / S^2 with M = max b, R = sum (b/M)^p, S = sum a.  M is
+// refined in fp64 over the near-maximal k and S summed in fp64, so the
+// reported objective carries fp64-level error; R uses the fp32 b.
+constexpr int kRefineCap = 1024;
+
 template <int TK>
 __global__ void __launch_bounds__(1024, 1)
 k_lp_forward(const float* __restrict__ pop, int n, float p, float* __restrict__ value,
              float* __restrict__ saved, float* __restrict__ b_out) {
   constexpr int MG = margin<TK>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_list[kRefineCap];
+  __shared__ int s_cnt;
+  __shared__ double s_red[32];
   float* base = reinterpret_cast<float*>(smem_raw);
   float* sA = base + MG;
   float* sC = base + (n + 2 * MG) + MG;
@@ -144,15 +151,19 @@ k_lp_forward(const float* __restrict__ pop, int n, float p, float* __restrict__ 
   const int nb = 2 * n - 1;
   zero_fill(base, (int)ls_smem_elems<float, TK>(n));
   __syncthreads();
-  float sl = 0.f;
+  double sl = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; sA[i] = x; sl += x; }
-  const float S = block_sum(sl, sRed);
+  const double S = block_sum(sl, s_red);
   float mloc = 0.f;
   conv_warp_tiles<TK, true>(sA, sA, n, [&](int k, float val) {
     sC[k] = val;
     mloc = val > mloc ? val : mloc;
   });
-  const float M = block_max(mloc, sRed);
+  const float Mapprox = block_max(mloc, sRed);
+  const double Md = refine_max(
+      n, [&](int i) { return sA[i]; }, [&](int k) { return sC[k]; }, Mapprox, 5e-4f, s_list,
+      kRefineCap, &s_cnt, s_red);
+  const float M = (float)Md;
   float rloc = 0.f;
   for (int k = threadIdx.x; k < nb; k += blockDim.x) {
     const float d = (sC[k] - M) / M;
@@ -161,12 +172,12 @@ k_lp_forward(const float* __restrict__ pop, int n, float p, float* __restrict__ 
   }
   const float R = block_sum(rloc, sRed);
   if (threadIdx.x == 0) {
-    const float val = 2.f * (float)n * M * powf(R, 1.f / p) / (S * S);
-    value[pid] = val;
+    const double val = 2.0 * (double)n * Md * pow((double)R, 1.0 / (double)p) / (S * S);
+    value[pid] = (float)val;
     saved[4 * pid + 0] = M;
-    saved[4 * pid + 1] = S;
+    saved[4 * pid + 1] = (float)S;
     saved[4 * pid + 2] = R;
-    saved[4 * pid + 3] = val;
+    saved[4 * pid + 3] = (float)val;
   }
 }
 

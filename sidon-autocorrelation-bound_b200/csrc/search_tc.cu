@@ -172,9 +172,10 @@ k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ sk
     if (!(M > 0.f)) break;
     // c_k = (1+d)^(p-1) in place, R = sum c_k (1+d), d = (b_k - M)/M
     float rloc = 0.f;
+    const float invM = 1.f / M, q = pexp - 1.f;
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-      const float d = (S.cb[pidx(k)] - M) / M;
-      const float cw = d > -1.f ? pow_from_d(d, pexp - 1.f) : 0.f;
+      const float d = (S.cb[pidx(k)] - M) * invM;
+      const float cw = d > -1.f ? pow_from_d_fast(d, q) : 0.f;
       rloc += cw * (1.f + d);
       S.cb[pidx(k)] = cw;
     }
@@ -189,26 +190,44 @@ k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ sk
     if (!corr_tc(C, S.sa, S.cb, status)) break;
     gather_corr(C, ln, S.cb);                     // G in cb (weights no longer needed)
 
+    // Adam / mirror step; four cells per thread per pass so the moment loads
+    // of HBM/L2 overlap
     float sloc = 0.f;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const float gi = S.cb[pidx(i)] / R - M;
-      float x;
-      if (mode == 0) {
-        const float mm = __fmaf_rn(beta1, mg[i], (1.f - beta1) * gi);
-        const float vv = __fmaf_rn(beta2, vg[i], (1.f - beta2) * gi * gi);
-        mg[i] = mm;
-        vg[i] = vv;
-        const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
-        x = S.sa[pidx(i)] - step;
-        if (x < 0.f) x = 0.f;
-      } else {
-        float e = -lr * (gi / M);
-        if (e > 4.f) e = 4.f;
-        if (e < -4.f) e = -4.f;
-        x = S.sa[pidx(i)] * expf(e);
+    const float invR = 1.f / R;
+    for (int i0 = threadIdx.x; i0 < n; i0 += 4 * blockDim.x) {
+      float g4[4], m4[4], v4[4], x4[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if (i < n) {
+          g4[u] = S.cb[pidx(i)] * invR - M;
+          x4[u] = S.sa[pidx(i)];
+          if (mode == 0) { m4[u] = mg[i]; v4[u] = vg[i]; }
+        }
       }
-      S.sa[pidx(i)] = x;
-      sloc += x;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if (i >= n) continue;
+        const float gi = g4[u];
+        float x;
+        if (mode == 0) {
+          const float mm = __fmaf_rn(beta1, m4[u], (1.f - beta1) * gi);
+          const float vv = __fmaf_rn(beta2, v4[u], (1.f - beta2) * gi * gi);
+          mg[i] = mm;
+          vg[i] = vv;
+          const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
+          x = x4[u] - step;
+          if (x < 0.f) x = 0.f;
+        } else {
+          float e = -lr * (gi * invM);
+          if (e > 4.f) e = 4.f;
+          if (e < -4.f) e = -4.f;
+          x = x4[u] * __expf(e);
+        }
+        S.sa[pidx(i)] = x;
+        sloc += x;
+      }
     }
     float Ssum = block_sum(sloc, S.red);
     if (!(Ssum > 0.f)) {
@@ -225,11 +244,18 @@ k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ sk
 }
 
 // ------------------------------ G_p forward -------------------------------
+// As k_lp_forward: M refined in fp64 over the near-maximal k (the split
+// error of b is < 3e-5 of max b), S in fp64, R from the tensor-core b.
+constexpr int kRefineCap = 1024;
+
 __global__ void __launch_bounds__(NTHREADS, 1)
 k_lp_forward_tc(const float* __restrict__ pop, int n, float p, float* __restrict__ value,
                 float* __restrict__ saved, float* __restrict__ b_out, int three,
                 unsigned int* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ int s_list[kRefineCap];
+  __shared__ int s_cnt;
+  __shared__ double s_red[32];
   const int pid = blockIdx.x;
   Shared S = setup(n, three != 0, smem_raw);
   Ctx& C = S.C;
@@ -237,9 +263,9 @@ k_lp_forward_tc(const float* __restrict__ pop, int n, float p, float* __restrict
   const Lane ln;
   const float* a = pop + (size_t)pid * n;
   __syncthreads();
-  float sl = 0.f;
+  double sl = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; S.sa[pidx(i)] = x; sl += x; }
-  const float Ssum = block_sum(sl, S.red);
+  const double Ssum = block_sum(sl, s_red);
   prime(C, false);
   const bool ok = conv_tc(C, S.sa, status);
   if (ok) gather_conv(C, ln, S.cb);
@@ -250,22 +276,26 @@ k_lp_forward_tc(const float* __restrict__ pop, int n, float p, float* __restrict
       mloc = fmaxf(mloc, v);
       if (b_out) b_out[(size_t)pid * nb + k] = v;
     }
-  const float M = block_max(mloc, S.red);
+  const float Mapprox = block_max(mloc, S.red);
+  const double Md = refine_max(
+      n, [&](int i) { return S.sa[pidx(i)]; }, [&](int k) { return S.cb[pidx(k)]; }, Mapprox,
+      2e-4f, s_list, kRefineCap, &s_cnt, s_red);
+  const float M = (float)Md;
   float rloc = 0.f;
   if (ok)
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
       const float d = (S.cb[pidx(k)] - M) / M;
-      rloc += d > -1.f ? pow_from_d(d, p) : 0.f;
+      rloc += d > -1.f ? pow_from_d_fast(d, p) : 0.f;
     }
   const float R = block_sum(rloc, S.red);
   if (threadIdx.x == 0) {
-    const float val = ok ? 2.f * (float)n * M * powf(R, 1.f / p) / (Ssum * Ssum)
-                         : __int_as_float(0x7fc00000);
-    value[pid] = val;
+    const double val = 2.0 * (double)n * Md * pow((double)R, 1.0 / (double)p) / (Ssum * Ssum);
+    const float v = ok ? (float)val : __int_as_float(0x7fc00000);
+    value[pid] = v;
     saved[4 * pid + 0] = M;
-    saved[4 * pid + 1] = Ssum;
+    saved[4 * pid + 1] = (float)Ssum;
     saved[4 * pid + 2] = R;
-    saved[4 * pid + 3] = val;
+    saved[4 * pid + 3] = v;
   }
   teardown(S);
 }
@@ -297,7 +327,7 @@ k_lp_backward_tc(const float* __restrict__ pop, const float* __restrict__ saved,
   }
   for (int k = threadIdx.x; k < nb; k += blockDim.x) {
     const float d = (S.cb[pidx(k)] - M) / M;
-    S.cb[pidx(k)] = d > -1.f ? pow_from_d(d, p - 1.f) : 0.f;
+    S.cb[pidx(k)] = d > -1.f ? pow_from_d_fast(d, p - 1.f) : 0.f;
   }
   fence_before();
   __syncthreads();
