@@ -195,6 +195,96 @@ SIDON_API int sidon_coarsen(const void* src, int n2, int P, void* dst, int dtype
 SIDON_API int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, int k_migrate,
                          int* order_out, void* stream);
 
+/* ---------------------------- ragged batches ------------------------------
+ * A ragged batch holds P candidates of different sizes back to back:
+ * candidate p is pop[offsets[p] .. offsets[p+1]) (offsets: device int64
+ * [P+1], non-decreasing; n_p = offsets[p+1] - offsets[p]).  n_max bounds
+ * every n_p and sizes the launch; a candidate with n_p outside [1, n_max] is
+ * left untouched.  order (device int [P], may be NULL = 0..P-1) is the order
+ * in which the launch takes the candidates up; sidon_ragged_order writes the
+ * longest-first order that balances the tail.  mom/vel (and every per-row
+ * output) follow the layout of pop.  Each candidate's result is bit-identical
+ * to the uniform entry point's at its own n.  No reference counterpart: the
+ * reference runs one n per launch (src/main.cu:118-137). */
+
+/* order_out[r] = candidate of rank r by size descending, ties by index. */
+SIDON_API int sidon_ragged_order(const long long* offsets, int P, int* order_out, void* stream);
+
+/* sidon_local_search over a ragged fp32 batch; precision FP32_SIMT, BF16X1
+ * or BF16X3 (the tensor-core kernel runs persistently, one CTA per SM). */
+SIDON_API int sidon_local_search_ragged(float* pop, float* mom, float* vel,
+                                        const long long* offsets, const int* order, int n_max,
+                                        const int* skip, const int* mode_arr, int P, int iters,
+                                        double p_start, double p_end, double lr_start,
+                                        double lr_end, double beta1, double beta2,
+                                        int mode_default, int precision, void* stream);
+
+/* sidon_eval over a ragged batch (fp32 or fp64 heights). */
+SIDON_API int sidon_eval_ragged(const void* pop, int dtype, const long long* offsets,
+                                const int* order, int n_max, int P, double* out_F,
+                                int* out_nactive, double active_tol, void* stream);
+
+/* sidon_frank_wolfe over a ragged fp32 batch. */
+SIDON_API int sidon_frank_wolfe_ragged(float* pop, const long long* offsets, const int* order,
+                                       int n_max, const int* skip, int P, int rounds,
+                                       int pdhg_iters, int nT, float t_max, float tau,
+                                       float sigma, void* stream);
+
+/* sidon_island_migrate over a ragged fp32 batch: a migrant of another size
+ * is resampled by nearest neighbour, dst[t] = src[min(m-1, t m / n)], and
+ * normalised to sum 1 in fp64 (the injection of src/main.cu:555-562); its
+ * fit becomes NaN until the next evaluation.  Same-size migrants are copied
+ * with their fit. */
+SIDON_API int sidon_island_migrate_ragged(float* pop, const long long* offsets, double* fit,
+                                          int P, int n_islands, int k_migrate, int* order_out,
+                                          void* stream);
+
+/* ------------------------------ anneal driver -----------------------------
+ * The stream-ordered generation loop of the island search: `steps` Adam
+ * steps with p and lr geometric over the whole anneal, cut into segments at
+ * every multiple of fw_every and migrate_every; after a segment ending at a
+ * multiple of fw_every a Frank-Wolfe step (fw_rounds rounds of pdhg_iters
+ * Chambolle-Pock iterations), after one ending at a multiple of
+ * migrate_every (before the last step) an fp64 evaluation into fit and a
+ * top-k_migrate migration between the n_islands islands; at the end an fp64
+ * evaluation into fit.  Adam moments restart with each segment, as they do
+ * with each local-search launch of the reference driver.  Nothing is
+ * allocated and nothing synchronises, so the whole loop can be captured in a
+ * CUDA graph (sidon_anneal_capture).  Replaces the generation loop of
+ * src/main.cu:586-785 for its local-search, Frank-Wolfe and migration
+ * steps. */
+typedef struct sidon_anneal_config {
+  int steps;                 /* Adam steps in total */
+  double p_start, p_end;     /* L^p exponent, geometric over the steps */
+  double lr_start, lr_end;   /* step size, geometric over the steps */
+  double beta1, beta2;
+  int precision;             /* local-search precision (FP32_SIMT, BF16X1, BF16X3) */
+  int fw_every;              /* Frank-Wolfe after every fw_every steps (0 = never) */
+  int fw_rounds, pdhg_iters, fw_nT;
+  float fw_t_max, fw_tau, fw_sigma;  /* tau, sigma <= 0: the reference steps */
+  int n_islands;             /* islands of P / n_islands consecutive candidates */
+  int migrate_every;         /* migration after every migrate_every steps (0 = never) */
+  int k_migrate;
+} sidon_anneal_config;
+
+/* pop: fp32, ragged (offsets != NULL) or uniform [P][n_max] (offsets ==
+ * NULL); mom/vel: scratch of pop's layout; fit: device double [P] (fp64 F
+ * at the end); rank: device int [P] (island ranking scratch, required when
+ * migrating); order: as for the ragged calls. */
+SIDON_API int sidon_anneal(float* pop, float* mom, float* vel, const long long* offsets,
+                           const int* order, int n_max, int P, double* fit, int* rank,
+                           const sidon_anneal_config* cfg, void* stream);
+
+/* Records sidon_anneal with these arguments as a CUDA graph (nothing runs)
+ * and returns it in *graph; sidon_graph_launch replays it on a stream (the
+ * buffers must stay valid), sidon_graph_destroy releases it. */
+typedef struct sidon_graph_s* sidon_graph;
+SIDON_API int sidon_anneal_capture(float* pop, float* mom, float* vel, const long long* offsets,
+                                   const int* order, int n_max, int P, double* fit, int* rank,
+                                   const sidon_anneal_config* cfg, sidon_graph* graph);
+SIDON_API int sidon_graph_launch(sidon_graph graph, void* stream);
+SIDON_API int sidon_graph_destroy(sidon_graph graph);
+
 #ifdef __cplusplus
 }
 #endif

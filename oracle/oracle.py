@@ -46,6 +46,8 @@ _SIG = {
     "so_refine_f64": (None, [_vp, _i, _i, _vp]),
     "so_coarsen_f64": (None, [_vp, _i, _i, _vp]),
     "so_island_migrate_f32": (_i, [_vp, _i, _vp, _i, _i, _i, _vp]),
+    "so_resample_f32": (None, [_vp, _i, _vp, _i]),
+    "so_island_migrate_ragged_f32": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp]),
     "so_certify_exact": (_d, [_vp, _i, _vp, _vp, _vp]),
     "so_exact_bk": (_d, [_vp, _i, _i]),
     "so_num_threads": (_i, []),
@@ -245,6 +247,28 @@ def island_migrate(pop, fit, NI, k):
     if rc:
         raise ValueError(f"island_migrate: bad arguments ({rc})")
     return pop, fit, order
+
+
+def resample(src, n):
+    """Nearest-neighbour resample to n cells + fp64 renormalisation
+    (src/main.cu:555-562)."""
+    src = _c(src, np.float32)
+    dst = np.empty(n, np.float32)
+    lib().so_resample_f32(src.ctypes.data, src.size, dst.ctypes.data, n)
+    return dst
+
+
+def island_migrate_ragged(flat, offsets, fit, NI, k):
+    flat = _c(flat, np.float32).copy()
+    off = _c(offsets, np.int64)
+    fit = _c(fit, np.float64).copy()
+    P = off.size - 1
+    order = np.empty(P, np.int32)
+    rc = lib().so_island_migrate_ragged_f32(flat.ctypes.data, off.ctypes.data, fit.ctypes.data,
+                                            P, NI, k, order.ctypes.data)
+    if rc:
+        raise ValueError(f"island_migrate_ragged: bad arguments ({rc})")
+    return flat, fit, order
 
 
 def certify_exact(a):

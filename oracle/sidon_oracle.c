@@ -474,6 +474,60 @@ SO_EXPORT int so_island_migrate_f32(float* pop, int n, double* fit, int P, int N
   return 0;
 }
 
+/* src/main.cu:555-562 (injectDouble) for an fp32 source: nearest-neighbour
+ * resample x_t = src[min(m-1, floor(t m / n))], S = sum of x_t in t order
+ * (fp64), dst_t = fl32(x_t / S) when S > 0 (else the resampled values). */
+SO_EXPORT void so_resample_f32(const float* src, int m, float* dst, int n) {
+  double S = 0.0;
+  for (int t = 0; t < n; ++t) {
+    long long q = (long long)t * m / n;
+    if (q > m - 1) q = m - 1;
+    dst[t] = src[q];
+    S += (double)src[q];
+  }
+  if (S > 0.0)
+    for (int t = 0; t < n; ++t) dst[t] = (float)((double)dst[t] / S);
+}
+
+/* Ragged island migration: ranking as so_island_migrate_f32; a migrant of
+ * the destination's size is copied with its fitness, one of another size is
+ * resampled by so_resample_f32 and its fitness set to NaN.  Candidate p is
+ * pop[off[p] .. off[p+1]). */
+SO_EXPORT int so_island_migrate_ragged_f32(float* pop, const long long* off, double* fit, int P,
+                                           int NI, int k, int* order_out) {
+  if (NI <= 0 || P % NI) return 1;
+  const int PI = P / NI;
+  if (2 * k > PI) return 2;
+  int* ord = order_out ? order_out : (int*)malloc(sizeof(int) * (size_t)P);
+  for (int i = 0; i < NI; ++i) {
+    for (int r = 0; r < PI; ++r) ord[i * PI + r] = i * PI + r;
+    g_fit_cmp = fit;
+    qsort(ord + i * PI, (size_t)PI, sizeof(int), cmp_slot);
+  }
+  if (k > 0) {
+    double* f2 = (double*)malloc(sizeof(double) * (size_t)P);
+    memcpy(f2, fit, sizeof(double) * (size_t)P);
+    for (int i = 0; i < NI; ++i) {
+      const int nx = (i + 1) % NI;
+      for (int j = 0; j < k; ++j) {
+        const int src = ord[i * PI + j], dst = ord[nx * PI + PI - 1 - j];
+        const int m = (int)(off[src + 1] - off[src]), n = (int)(off[dst + 1] - off[dst]);
+        if (m == n) {
+          memcpy(pop + off[dst], pop + off[src], sizeof(float) * (size_t)n);
+          f2[dst] = fit[src];
+        } else {
+          so_resample_f32(pop + off[src], m, pop + off[dst], n);
+          f2[dst] = NAN;
+        }
+      }
+    }
+    memcpy(fit, f2, sizeof(double) * (size_t)P);
+    free(f2);
+  }
+  if (!order_out) free(ord);
+  return 0;
+}
+
 /* ============================ exact certification ========================= */
 /* F from EXACT M = max_k b_k and EXACT S = sum a, each rounded once to fp64
  * (round to nearest even), then F = 2 n M / (S S) in fp64.  Exact b_k comes

@@ -42,7 +42,35 @@ SIGNATURES = {
     "sidon_refine": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "sidon_coarsen": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "sidon_island_migrate": (_i, [_vp, _i, _vp, _i, _i, _i, _vp, _vp]),
+    "sidon_ragged_order": (_i, [_vp, _i, _vp, _vp]),
+    "sidon_local_search_ragged": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _i, _i, _d, _d, _d,
+                                       _d, _d, _d, _i, _i, _vp]),
+    "sidon_eval_ragged": (_i, [_vp, _i, _vp, _vp, _i, _i, _vp, _vp, _d, _vp]),
+    "sidon_frank_wolfe_ragged": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _i, _f, _f, _f, _vp]),
+    "sidon_island_migrate_ragged": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _vp]),
+    "sidon_anneal": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
+    "sidon_anneal_capture": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
+    "sidon_graph_launch": (_i, [_vp, _vp]),
+    "sidon_graph_destroy": (_i, [_vp]),
 }
+
+
+class AnnealConfig(C.Structure):
+    """struct sidon_anneal_config."""
+
+    _fields_ = [
+        ("steps", _i),
+        ("p_start", _d), ("p_end", _d),
+        ("lr_start", _d), ("lr_end", _d),
+        ("beta1", _d), ("beta2", _d),
+        ("precision", _i),
+        ("fw_every", _i),
+        ("fw_rounds", _i), ("pdhg_iters", _i), ("fw_nT", _i),
+        ("fw_t_max", _f), ("fw_tau", _f), ("fw_sigma", _f),
+        ("n_islands", _i),
+        ("migrate_every", _i),
+        ("k_migrate", _i),
+    ]
 
 _lock = threading.Lock()
 _lib: C.CDLL | None = None

@@ -5,6 +5,7 @@
 // ---------------------------------------------------------------------------
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -17,13 +18,16 @@ size_t smem_eval(int n);
 size_t smem_fw(int n);
 size_t smem_certify(int n);
 size_t smem_local_search_tc(int n);
-int launch_local_search(void* pop, void* mom, void* vel, const int* skip, const int* mode_arr,
-                        int n, int P, int iters, double pS, double pE, double lrS, double lrE,
-                        double b1, double b2, int mode_default, int dtype, cudaStream_t st);
-int launch_local_search_tc(float* pop, float* mom, float* vel, const int* skip,
-                           const int* mode_arr, int n, int P, int iters, double pS, double pE,
-                           double lrS, double lrE, double b1, double b2, int mode_default,
-                           int precision, cudaStream_t st);
+int launch_local_search(void* pop, void* mom, void* vel, const long long* offsets,
+                        const int* order, int P, int n_fixed, int n_max, const int* skip,
+                        const int* mode_arr, int iters, double pS, double pE, double lrS,
+                        double lrE, double b1, double b2, int mode_default, int dtype,
+                        cudaStream_t st);
+int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* offsets,
+                           const int* order, int P, int n_fixed, int n_max, const int* skip,
+                           const int* mode_arr, int iters, double pS, double pE, double lrS,
+                           double lrE, double b1, double b2, int mode_default, int precision,
+                           cudaStream_t st);
 int launch_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
                       float* b_out, cudaStream_t st);
 int launch_lp_forward_tc(const float* a, int n, int P, double p, float* value, float* saved,
@@ -33,16 +37,20 @@ int launch_lp_backward_tc(const float* a, const float* saved, const float* b_in,
 int device_status(int reset);
 int launch_lp_backward(const float* a, const float* saved, const float* b_in, int n, int P,
                        double p, float* grad, cudaStream_t st);
-int launch_eval(const void* pop, int dtype, int n, int P, double* outF, int* outN, double tol,
-                cudaStream_t st);
+int launch_eval(const void* pop, int dtype, const long long* offsets, const int* order, int P,
+                int n_fixed, int n_max, double* outF, int* outN, double tol, cudaStream_t st);
 int launch_certify(const void* pop, int dtype, int n, int P, double* outF, double* outM,
                    double* outS, int* outK, cudaStream_t st);
-int launch_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int pdhg, int nT,
-                       float tMax, float tau, float sig, cudaStream_t st);
+int launch_frank_wolfe(float* pop, const long long* offsets, const int* order, int P, int n_fixed,
+                       int n_max, const int* skip, int rounds, int pdhg, int nT, float tMax,
+                       float tau, float sig, cudaStream_t st);
 int launch_refine(const void* src, int n, int P, void* dst, int dtype, cudaStream_t st);
 int launch_coarsen(const void* src, int n2, int P, void* dst, int dtype, cudaStream_t st);
 int launch_island_migrate(float* pop, int n, double* fit, int P, int NI, int k, int* order,
                           cudaStream_t st);
+int launch_island_migrate_ragged(float* pop, const long long* offsets, double* fit, int P, int NI,
+                                 int k, int* order, cudaStream_t st);
+int launch_ragged_order(const long long* offsets, int P, int* order, cudaStream_t st);
 
 static thread_local int g_last_cuda = 0;
 
@@ -66,6 +74,32 @@ int sm_count() {
   if (cudaGetDevice(&dev) != cudaSuccess) return 1;
   if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 1;
   return v > 0 ? v : 1;
+}
+int set_dyn_smem(const void* fn, size_t smem) {
+  if ((long long)smem > (long long)smem_optin()) return SIDON_ERR_SMEM;
+  struct Entry {
+    int dev;
+    const void* fn;
+    size_t smem;
+  };
+  static std::mutex mu;
+  static std::vector<Entry> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  std::lock_guard<std::mutex> lock(mu);
+  for (Entry& x : done)
+    if (x.dev == dev && x.fn == fn) {
+      if (x.smem >= smem) return SIDON_OK;
+      e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return set_cuda_error(e);
+      x.smem = smem;
+      return SIDON_OK;
+    }
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  done.push_back({dev, fn, smem});
+  return SIDON_OK;
 }
 int device_ok() {
   int dev = 0, major = 0;
@@ -166,7 +200,8 @@ int sidon_eval(const void* pop, int dtype, int n, int P, double* out_F, int* out
   if (P == 0) return SIDON_OK;
   if (!pop || !out_F) return SIDON_ERR_ARG;
   if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
-  return launch_eval(pop, dtype, n, P, out_F, out_nactive, active_tol, S(stream));
+  return launch_eval(pop, dtype, nullptr, nullptr, P, n, n, out_F, out_nactive, active_tol,
+                     S(stream));
 }
 
 int sidon_certify(const void* pop, int dtype, int n, int P, double* out_F, double* out_M,
@@ -191,17 +226,19 @@ int sidon_local_search(void* pop, void* mom, void* vel, const int* skip, const i
     return SIDON_ERR_ARG;
   if (dtype == SIDON_F32) {
     if (precision == SIDON_PREC_FP32_SIMT)
-      return launch_local_search(pop, mom, vel, skip, mode_arr, n, P, iters, p_start, p_end,
-                                 lr_start, lr_end, beta1, beta2, mode_default, dtype, S(stream));
+      return launch_local_search(pop, mom, vel, nullptr, nullptr, P, n, n, skip, mode_arr, iters,
+                                 p_start, p_end, lr_start, lr_end, beta1, beta2, mode_default,
+                                 dtype, S(stream));
     if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
-      return launch_local_search_tc((float*)pop, (float*)mom, (float*)vel, skip, mode_arr, n, P,
-                                    iters, p_start, p_end, lr_start, lr_end, beta1, beta2,
-                                    mode_default, precision, S(stream));
+      return launch_local_search_tc((float*)pop, (float*)mom, (float*)vel, nullptr, nullptr, P,
+                                    n, n, skip, mode_arr, iters, p_start, p_end, lr_start, lr_end,
+                                    beta1, beta2, mode_default, precision, S(stream));
     return SIDON_ERR_DTYPE;
   }
   if (dtype == SIDON_F64 && precision == SIDON_PREC_FP64_SIMT)
-    return launch_local_search(pop, mom, vel, skip, mode_arr, n, P, iters, p_start, p_end,
-                               lr_start, lr_end, beta1, beta2, mode_default, dtype, S(stream));
+    return launch_local_search(pop, mom, vel, nullptr, nullptr, P, n, n, skip, mode_arr, iters,
+                               p_start, p_end, lr_start, lr_end, beta1, beta2, mode_default,
+                               dtype, S(stream));
   return SIDON_ERR_DTYPE;
 }
 
@@ -237,7 +274,8 @@ int sidon_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int
   if (rc) return rc;
   if (P == 0 || rounds <= 0) return SIDON_OK;
   if (!pop || pdhg_iters < 0 || nT < 1 || !(t_max > 0.f) || !(t_max <= 1.f)) return SIDON_ERR_ARG;
-  return launch_frank_wolfe(pop, skip, n, P, rounds, pdhg_iters, nT, t_max, tau, sigma, S(stream));
+  return launch_frank_wolfe(pop, nullptr, nullptr, P, n, n, skip, rounds, pdhg_iters, nT, t_max,
+                            tau, sigma, S(stream));
 }
 
 int sidon_refine(const void* src, int n, int P, void* dst, int dtype, void* stream) {
@@ -269,6 +307,74 @@ int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, i
   const int PI = P / n_islands;
   if (PI > 1024 || 2 * k_migrate > PI) return SIDON_ERR_ARG;
   return launch_island_migrate(pop, n, fit, P, n_islands, k_migrate, order_out, S(stream));
+}
+
+int sidon_ragged_order(const long long* offsets, int P, int* order_out, void* stream) {
+  int rc = pre(1, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!offsets || !order_out) return SIDON_ERR_ARG;
+  return launch_ragged_order(offsets, P, order_out, S(stream));
+}
+
+int sidon_local_search_ragged(float* pop, float* mom, float* vel, const long long* offsets,
+                              const int* order, int n_max, const int* skip, const int* mode_arr,
+                              int P, int iters, double p_start, double p_end, double lr_start,
+                              double lr_end, double beta1, double beta2, int mode_default,
+                              int precision, void* stream) {
+  int rc = pre(n_max, P);
+  if (rc) return rc;
+  if (P == 0 || iters <= 0) return SIDON_OK;
+  if (!pop || !mom || !vel || !offsets) return SIDON_ERR_ARG;
+  if (!(p_start > 0.0) || !(p_end > 0.0) || !(lr_start > 0.0) || !(lr_end > 0.0))
+    return SIDON_ERR_ARG;
+  if (precision == SIDON_PREC_FP32_SIMT)
+    return launch_local_search(pop, mom, vel, offsets, order, P, 0, n_max, skip, mode_arr, iters,
+                               p_start, p_end, lr_start, lr_end, beta1, beta2, mode_default,
+                               SIDON_F32, S(stream));
+  if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
+    return launch_local_search_tc(pop, mom, vel, offsets, order, P, 0, n_max, skip, mode_arr,
+                                  iters, p_start, p_end, lr_start, lr_end, beta1, beta2,
+                                  mode_default, precision, S(stream));
+  return SIDON_ERR_DTYPE;
+}
+
+int sidon_eval_ragged(const void* pop, int dtype, const long long* offsets, const int* order,
+                      int n_max, int P, double* out_F, int* out_nactive, double active_tol,
+                      void* stream) {
+  int rc = pre(n_max, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!pop || !offsets || !out_F) return SIDON_ERR_ARG;
+  if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
+  return launch_eval(pop, dtype, offsets, order, P, 0, n_max, out_F, out_nactive, active_tol,
+                     S(stream));
+}
+
+int sidon_frank_wolfe_ragged(float* pop, const long long* offsets, const int* order, int n_max,
+                             const int* skip, int P, int rounds, int pdhg_iters, int nT,
+                             float t_max, float tau, float sigma, void* stream) {
+  int rc = pre(n_max, P);
+  if (rc) return rc;
+  if (P == 0 || rounds <= 0) return SIDON_OK;
+  if (!pop || !offsets || pdhg_iters < 0 || nT < 1 || !(t_max > 0.f) || !(t_max <= 1.f))
+    return SIDON_ERR_ARG;
+  return launch_frank_wolfe(pop, offsets, order, P, 0, n_max, skip, rounds, pdhg_iters, nT, t_max,
+                            tau, sigma, S(stream));
+}
+
+int sidon_island_migrate_ragged(float* pop, const long long* offsets, double* fit, int P,
+                                int n_islands, int k_migrate, int* order_out, void* stream) {
+  int rc = pre(1, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!pop || !offsets || !fit || !order_out || n_islands < 1 || k_migrate < 0)
+    return SIDON_ERR_ARG;
+  if (P % n_islands) return SIDON_ERR_ARG;
+  const int PI = P / n_islands;
+  if (PI > 1024 || 2 * k_migrate > PI) return SIDON_ERR_ARG;
+  return launch_island_migrate_ragged(pop, offsets, fit, P, n_islands, k_migrate, order_out,
+                                      S(stream));
 }
 
 }  // extern "C"

@@ -141,10 +141,10 @@ k_certify(const Tin* __restrict__ pop, int n, double* __restrict__ outF, double*
   atomicMax(&sEmax, emax);
   __syncthreads();
   double mloc = 0.0;
-  conv_warp_tiles<kCertTK, false>(sA, sA, n, [&](int, double v) { mloc = v > mloc ? v : mloc; });
+  conv_warp_tiles<kCertTK, false>(sA, sA, n, Team(), [&](int, double v) { mloc = v > mloc ? v : mloc; });
   const double M64 = block_max(mloc, sRed);
   const double thr = M64 * (1.0 - 1e-9);
-  conv_warp_tiles<kCertTK, false>(sA, sA, n, [&](int k, double v) {
+  conv_warp_tiles<kCertTK, false>(sA, sA, n, Team(), [&](int k, double v) {
     if (v >= thr) {
       const int slot = atomicAdd(&sNC, 1);
       if (slot < kMaxCand) sCand[slot] = k;

@@ -115,6 +115,23 @@ __device__ double refine_max(int n, AFn&& aval, BFn&& bval, float approx, float 
   return block_max(best, red);
 }
 
+// A candidate of a uniform batch (offsets == NULL: row pid of n_fixed
+// cells) or of a ragged batch (pop[offsets[pid] .. offsets[pid + 1])).
+// order (NULL = identity) maps a launch slot to the candidate it runs.
+struct Cand {
+  int pid;
+  long long off;
+  int n;
+};
+__device__ __forceinline__ Cand cand_of(int slot, const long long* __restrict__ offsets,
+                                        const int* __restrict__ order, int n_fixed) {
+  Cand c;
+  c.pid = order ? order[slot] : slot;
+  c.off = offsets ? offsets[c.pid] : (long long)c.pid * n_fixed;
+  c.n = offsets ? (int)(offsets[c.pid + 1] - c.off) : n_fixed;
+  return c;
+}
+
 // round-up helper
 __host__ __device__ constexpr inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
@@ -127,4 +144,10 @@ int check_launch();                                  // cudaGetLastError -> stat
 int smem_optin();                                    // per-CTA opt-in of the current device
 int sm_count();                                      // SMs of the current device
 int device_ok();                                     // SIDON_OK if current device is sm_100
+// Dynamic shared memory opt-in of kernel fn for at least smem bytes on the
+// current device; SIDON_ERR_SMEM beyond the device limit.  The attribute is
+// set once per (device, kernel, size class) and remembered, so launches
+// inside a stream capture issue no attribute call once the same launch has
+// run eagerly.
+int set_dyn_smem(const void* fn, size_t smem);
 }  // namespace sidon_host

@@ -52,16 +52,31 @@ __device__ __forceinline__ int conv_tile_at(int p, int c, int Q) {
   return (c >= Q - 1 - c) ? (c - m - extra) : (c + m + extra);
 }
 
+// The threads of a CTA that work on the current candidate: the first nt
+// (a multiple of 32).  A CTA sized for a larger candidate of a ragged batch
+// leaves the others idle except at barriers, where idle warps contribute
+// exact zeros to block reductions, so a candidate's result does not depend on
+// the batch it runs in.
+struct Team {
+  int nt;  // working threads
+  int t0;  // threadIdx.x for a working thread, else past every loop bound
+  __device__ explicit Team(int nthreads)
+      : nt(nthreads), t0((int)threadIdx.x < nthreads ? (int)threadIdx.x : 0x3fffffff) {}
+  __device__ Team() : Team((int)blockDim.x) {}
+  __device__ bool active() const { return t0 < nt; }
+};
+
 // b_k = sum_i x_i y_{k-i}, k in [0, 2n-1).  epi(k, value) is called once per
 // output k < 2n-1 by the lane that owns it.
 template <int TK, bool FUSED, typename T, typename Epi>
 __device__ __forceinline__ void conv_warp_tiles(const T* __restrict__ x, const T* __restrict__ y,
-                                                int n, Epi&& epi) {
+                                                int n, const Team& tm, Epi&& epi) {
   constexpr int W = 32 * TK;
+  if (!tm.active()) return;
   const int nb = 2 * n - 1;
   const int Q = (nb + W - 1) / W;
   const int c = (n - 1) / W;
-  const int NW = blockDim.x >> 5;
+  const int NW = tm.nt >> 5;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int r = 0;; ++r) {
     const int p = r * NW + ((r & 1) ? (NW - 1 - wid) : wid);
@@ -98,10 +113,11 @@ __device__ __forceinline__ void conv_warp_tiles(const T* __restrict__ x, const T
 // c must be valid (zero) up to index 2n - 2 + margin.
 template <int TI, typename T, typename Epi>
 __device__ __forceinline__ void corr_warp_tiles(const T* __restrict__ a, const T* __restrict__ cc,
-                                                int n, Epi&& epi) {
+                                                int n, const Team& tm, Epi&& epi) {
   constexpr int W = 32 * TI;
+  if (!tm.active()) return;
   const int Q = (n + W - 1) / W;
-  const int NW = blockDim.x >> 5;
+  const int NW = tm.nt >> 5;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int trips = (n + TI - 1) / TI;
   for (int q = wid; q < Q; q += NW) {

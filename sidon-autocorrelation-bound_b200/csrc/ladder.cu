@@ -115,6 +115,65 @@ __global__ void k_island_migrate(float* __restrict__ pop, int n, double* __restr
   if (threadIdx.x == 0) fit[dst] = fit[src];
 }
 
+// Ragged batch: as k_island_migrate, rows pop[offsets[p] .. offsets[p+1]).
+// A source of the destination's size is copied with its fit.  Otherwise it
+// is resampled to the destination's size by nearest neighbour,
+// dst[t] = src[min(m-1, floor(t m / n))], and normalised to sum 1 in fp64
+// (S summed in t order, dst[t] = fl(src / S)), the injection of
+// src/main.cu:555-562; fit[dst] becomes NaN (unknown until re-evaluated).
+__global__ void k_island_migrate_ragged(float* __restrict__ pop,
+                                        const long long* __restrict__ offsets,
+                                        double* __restrict__ fit, int NI, int PI, int k,
+                                        const int* __restrict__ order) {
+  __shared__ double sS;
+  const int i = blockIdx.x / k, j = blockIdx.x % k;
+  const int nx = (i + 1) % NI;
+  const int src = order[(size_t)i * PI + j];
+  const int dst = order[(size_t)nx * PI + PI - 1 - j];
+  const long long so = offsets[src], dof = offsets[dst];
+  const int m = (int)(offsets[src + 1] - so), n = (int)(offsets[dst + 1] - dof);
+  const float* s = pop + so;
+  float* d = pop + dof;
+  if (m == n) {
+    for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = s[t];
+    if (threadIdx.x == 0) fit[dst] = fit[src];
+    return;
+  }
+  if (m < 1 || n < 1) return;
+  // the source and destination rows are distinct candidates (disjoint sets)
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const long long q = (long long)t * m / n;
+    d[t] = s[q < m - 1 ? q : m - 1];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double S = 0.0;
+    for (int t = 0; t < n; ++t) S = __dadd_rn(S, (double)d[t]);
+    sS = S;
+    fit[dst] = __longlong_as_double(0x7ff8000000000000ll);
+  }
+  __syncthreads();
+  const double S = sS;
+  if (S > 0.0)
+    for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = (float)__ddiv_rn((double)d[t], S);
+}
+
+// order[r] = candidate of rank r when sorted by size descending, ties by
+// index: the longest-first processing order of a ragged batch.  One thread
+// per candidate counts the candidates ranked before it.
+__global__ void k_ragged_order(const long long* __restrict__ offsets, int P,
+                               int* __restrict__ order) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < P; c += gridDim.x * blockDim.x) {
+    const long long nc = offsets[c + 1] - offsets[c];
+    int r = 0;
+    for (int o = 0; o < P; ++o) {
+      const long long no = offsets[o + 1] - offsets[o];
+      r += (no > nc) || (no == nc && o < c);
+    }
+    order[r] = c;
+  }
+}
+
 }  // namespace sidon
 
 namespace sidon_host {
@@ -166,6 +225,27 @@ int launch_island_migrate(float* pop, int n, double* fit, int P, int NI, int k, 
     rc = check_launch();
   }
   return rc;
+}
+
+int launch_island_migrate_ragged(float* pop, const long long* offsets, double* fit, int P, int NI,
+                                 int k, int* order, cudaStream_t st) {
+  const int PI = P / NI;
+  int L = 1;
+  while (L < PI) L <<= 1;
+  const size_t sm = (size_t)L * (sizeof(double) + sizeof(int));
+  k_island_rank<<<NI, 256, sm, st>>>(fit, PI, order);
+  int rc = check_launch();
+  if (rc) return rc;
+  if (k > 0) {
+    k_island_migrate_ragged<<<NI * k, 256, 0, st>>>(pop, offsets, fit, NI, PI, k, order);
+    rc = check_launch();
+  }
+  return rc;
+}
+
+int launch_ragged_order(const long long* offsets, int P, int* order, cudaStream_t st) {
+  k_ragged_order<<<grid_for((size_t)P, 128), 128, 0, st>>>(offsets, P, order);
+  return check_launch();
 }
 
 }  // namespace sidon_host

@@ -23,13 +23,16 @@
 #include "common.cuh"
 
 namespace sidon_host {
-int launch_local_search(void* pop, void* mom, void* vel, const int* skip, const int* mode_arr,
-                        int n, int P, int iters, double pS, double pE, double lrS, double lrE,
-                        double b1, double b2, int mode_default, int dtype, cudaStream_t st);
-int launch_local_search_tc(float* pop, float* mom, float* vel, const int* skip,
-                           const int* mode_arr, int n, int P, int iters, double pS, double pE,
-                           double lrS, double lrE, double b1, double b2, int mode_default,
-                           int precision, cudaStream_t st);
+int launch_local_search(void* pop, void* mom, void* vel, const long long* offsets,
+                        const int* order, int P, int n_fixed, int n_max, const int* skip,
+                        const int* mode_arr, int iters, double pS, double pE, double lrS,
+                        double lrE, double b1, double b2, int mode_default, int dtype,
+                        cudaStream_t st);
+int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* offsets,
+                           const int* order, int P, int n_fixed, int n_max, const int* skip,
+                           const int* mode_arr, int iters, double pS, double pE, double lrS,
+                           double lrE, double b1, double b2, int mode_default, int precision,
+                           cudaStream_t st);
 }  // namespace sidon_host
 
 namespace {
@@ -87,13 +90,13 @@ int sidon_local_search_noalloc(float* pop, const int* skip, const int* mode_arr,
   float* vel = scratch + kMaxCells;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (precision == SIDON_PREC_FP32_SIMT)
-    return sidon_host::launch_local_search(pop, mom, vel, skip, mode_arr, n, P, iters, p_start,
-                                           p_end, lr_start, lr_end, beta1, beta2, mode_default,
-                                           SIDON_F32, st);
+    return sidon_host::launch_local_search(pop, mom, vel, nullptr, nullptr, P, n, n, skip,
+                                           mode_arr, iters, p_start, p_end, lr_start, lr_end,
+                                           beta1, beta2, mode_default, SIDON_F32, st);
   if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
-    return sidon_host::launch_local_search_tc(pop, mom, vel, skip, mode_arr, n, P, iters,
-                                              p_start, p_end, lr_start, lr_end, beta1, beta2,
-                                              mode_default, precision, st);
+    return sidon_host::launch_local_search_tc(pop, mom, vel, nullptr, nullptr, P, n, n, skip,
+                                              mode_arr, iters, p_start, p_end, lr_start, lr_end,
+                                              beta1, beta2, mode_default, precision, st);
   return SIDON_ERR_DTYPE;
 }
 

@@ -8,7 +8,11 @@
 //                     (src/kernels.cuh:301-377, hostF arithmetic)
 //    k_frank_wolfe    Chambolle-Pock Frank-Wolfe step (src/kernels.cuh:408-532)
 //
-//  One CTA per candidate.  Shared memory (T = element type, MG = margin):
+//  One CTA per candidate; a candidate is a row of a uniform [P][n] batch or
+//  a slice of a ragged batch (offsets[P+1]).  A ragged launch sizes CTAs for
+//  n_max and lets each candidate use the threads a uniform launch at its own
+//  n would have (Team), so results match the uniform kernels bit for bit.
+//  Shared memory (T = element type, MG = margin):
 //    sA [MG | n | MG]        heights (window + broadcast operand)
 //    sC [MG | 2n-1 | MG]     b, then the weights c (correlation window)
 //    sRed[32]                reduction scratch
@@ -30,27 +34,30 @@ __device__ __forceinline__ void zero_fill(T* p, int count) {
 // ------------------------------ local search ------------------------------
 template <typename T, int TK>
 __global__ void __launch_bounds__(1024, 1)
-k_local_search(T* pop, T* mom, T* vel, const int* __restrict__ skip,
-               const int* __restrict__ mode_arr, int n, int iters, T pStart, T pEnd, T lrStart,
-               T lrEnd, T beta1, T beta2, int mode_default) {
+k_local_search(T* pop, T* mom, T* vel, const long long* __restrict__ offsets,
+               const int* __restrict__ order, int n_fixed, int n_max,
+               const int* __restrict__ skip, const int* __restrict__ mode_arr, int iters,
+               T pStart, T pEnd, T lrStart, T lrEnd, T beta1, T beta2, int mode_default) {
   constexpr int MG = margin<TK>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Cand cd = cand_of(blockIdx.x, offsets, order, n_fixed);
+  const int pid = cd.pid, n = cd.n;
+  if (skip && skip[pid]) return;
+  if (n < 1 || n > n_max) return;
+  const Team tm(32 * warps_for<TK>(n));
+  const int mode = mode_arr ? mode_arr[pid] : mode_default;
+  T* a = pop + cd.off;
+  T* m = mom + cd.off;
+  T* v = vel + cd.off;
+  const int nb = 2 * n - 1;
   T* base = reinterpret_cast<T*>(smem_raw);
   T* sA = base + MG;                        // [-MG, n + MG)
   T* sC = base + (n + 2 * MG) + MG;         // [-MG, 2n - 1 + MG)
   T* sRed = base + (n + 2 * MG) + (2 * n - 1 + 2 * MG);
 
-  const int pid = blockIdx.x;
-  if (skip && skip[pid]) return;
-  const int mode = mode_arr ? mode_arr[pid] : mode_default;
-  T* a = pop + (size_t)pid * n;
-  T* m = mom + (size_t)pid * n;
-  T* v = vel + (size_t)pid * n;
-  const int nb = 2 * n - 1;
-
   zero_fill(base, (int)ls_smem_elems<T, TK>(n));
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) { sA[i] = a[i]; m[i] = T(0); v[i] = T(0); }
+  for (int i = tm.t0; i < n; i += tm.nt) { sA[i] = a[i]; m[i] = T(0); v[i] = T(0); }
   __syncthreads();
 
   const T lnPr = T(log(double(pEnd) / double(pStart)));
@@ -64,7 +71,7 @@ k_local_search(T* pop, T* mom, T* vel, const int* __restrict__ skip,
 
     // b = a * a, and the running max in the same pass
     T mloc = T(0);
-    conv_warp_tiles<TK, true>(sA, sA, n, [&](int k, T val) {
+    conv_warp_tiles<TK, true>(sA, sA, n, tm, [&](int k, T val) {
       sC[k] = val;
       mloc = val > mloc ? val : mloc;
     });
@@ -73,7 +80,7 @@ k_local_search(T* pop, T* mom, T* vel, const int* __restrict__ skip,
 
     // c_k = (1+d)^(p-1), R = sum c_k (1+d), d = (b_k - M)/M
     T rloc = T(0);
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    for (int k = tm.t0; k < nb; k += tm.nt) {
       const T d = (sC[k] - M) / M;
       const T cw = d > T(-1) ? pow_from_d(d, pexp - T(1)) : T(0);
       rloc += cw * (T(1) + d);
@@ -88,7 +95,7 @@ k_local_search(T* pop, T* mom, T* vel, const int* __restrict__ skip,
 
     // G = corr(c, a); update fused into the epilogue; the new heights are
     // staged in the candidate's own row of pop (sA is still being read).
-    corr_warp_tiles<TK>(sA, sC, n, [&](int i, T G) {
+    corr_warp_tiles<TK>(sA, sC, n, tm, [&](int i, T G) {
       const T gi = G / R - M;
       T x;
       if (mode == 0) {
@@ -110,21 +117,21 @@ k_local_search(T* pop, T* mom, T* vel, const int* __restrict__ skip,
     __syncthreads();
 
     T sloc = T(0);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int i = tm.t0; i < n; i += tm.nt) {
       const T x = a[i];
       sA[i] = x;
       sloc += x;
     }
     T S = block_sum(sloc, sRed);
     if (!(S > T(0))) {
-      for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = T(1) / T(n);
+      for (int i = tm.t0; i < n; i += tm.nt) sA[i] = T(1) / T(n);
       S = T(1);
     }
     const T inv = T(1) / S;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] *= inv;
+    for (int i = tm.t0; i < n; i += tm.nt) sA[i] *= inv;
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = sA[i];
+  for (int i = tm.t0; i < n; i += tm.nt) a[i] = sA[i];
 }
 
 // ----------------------------- G_p forward --------------------------------
@@ -149,13 +156,14 @@ k_lp_forward(const float* __restrict__ pop, int n, float p, float* __restrict__ 
   const int pid = blockIdx.x;
   const float* a = pop + (size_t)pid * n;
   const int nb = 2 * n - 1;
+  const Team tm;
   zero_fill(base, (int)ls_smem_elems<float, TK>(n));
   __syncthreads();
   double sl = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; sA[i] = x; sl += x; }
+  for (int i = tm.t0; i < n; i += tm.nt) { const float x = a[i]; sA[i] = x; sl += x; }
   const double S = block_sum(sl, s_red);
   float mloc = 0.f;
-  conv_warp_tiles<TK, true>(sA, sA, n, [&](int k, float val) {
+  conv_warp_tiles<TK, true>(sA, sA, n, tm, [&](int k, float val) {
     sC[k] = val;
     mloc = val > mloc ? val : mloc;
   });
@@ -165,7 +173,7 @@ k_lp_forward(const float* __restrict__ pop, int n, float p, float* __restrict__ 
       kRefineCap, &s_cnt, s_red);
   const float M = (float)Md;
   float rloc = 0.f;
-  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+  for (int k = tm.t0; k < nb; k += tm.nt) {
     const float d = (sC[k] - M) / M;
     rloc += d > -1.f ? pow_from_d(d, p) : 0.f;
     if (b_out) b_out[(size_t)pid * nb + k] = sC[k];
@@ -196,17 +204,18 @@ k_lp_backward(const float* __restrict__ pop, const float* __restrict__ saved,
   const float* a = pop + (size_t)pid * n;
   const int nb = 2 * n - 1;
   const float M = saved[4 * pid + 0], S = saved[4 * pid + 1], R = saved[4 * pid + 2];
+  const Team tm;
   zero_fill(base, (int)ls_smem_elems<float, TK>(n));
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = a[i];
+  for (int i = tm.t0; i < n; i += tm.nt) sA[i] = a[i];
   __syncthreads();
   if (b_in) {
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) sC[k] = b_in[(size_t)pid * nb + k];
+    for (int k = tm.t0; k < nb; k += tm.nt) sC[k] = b_in[(size_t)pid * nb + k];
   } else {
-    conv_warp_tiles<TK, true>(sA, sA, n, [&](int k, float val) { sC[k] = val; });
+    conv_warp_tiles<TK, true>(sA, sA, n, tm, [&](int k, float val) { sC[k] = val; });
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+  for (int k = tm.t0; k < nb; k += tm.nt) {
     const float d = (sC[k] - M) / M;
     sC[k] = d > -1.f ? pow_from_d(d, p - 1.f) : 0.f;
   }
@@ -214,7 +223,7 @@ k_lp_backward(const float* __restrict__ pop, const float* __restrict__ saved,
   const float scale = 4.f * (float)n * powf(R, 1.f / p) / (S * S);
   const float MS = M / S;
   float* g = grad + (size_t)pid * n;
-  corr_warp_tiles<TK>(sA, sC, n, [&](int i, float G) { g[i] = scale * (G / R - MS); });
+  corr_warp_tiles<TK>(sA, sC, n, tm, [&](int i, float G) { g[i] = scale * (G / R - MS); });
 }
 
 // ---------------------------- certifying eval -----------------------------
@@ -223,22 +232,26 @@ k_lp_backward(const float* __restrict__ pop, const float* __restrict__ saved,
 // nActive = #{k : b_k >= M (1 - tol)} by a second pass (src/kernels.cuh:347-375).
 template <typename Tin, int TK>
 __global__ void __launch_bounds__(1024, 1)
-k_eval(const Tin* __restrict__ pop, int n, double* __restrict__ outF, int* __restrict__ outN,
-       double tol) {
+k_eval(const Tin* __restrict__ pop, const long long* __restrict__ offsets,
+       const int* __restrict__ order, int n_fixed, int n_max, double* __restrict__ outF,
+       int* __restrict__ outN, double tol) {
   constexpr int MG = margin<TK>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double sS;
+  const Cand cd = cand_of(blockIdx.x, offsets, order, n_fixed);
+  const int pid = cd.pid, n = cd.n;
+  if (n < 1 || n > n_max) return;
+  const Team tm(32 * warps_for<TK>(n));
   double* base = reinterpret_cast<double*>(smem_raw);
   double* sA = base + MG;
   double* sRed = base + (n + 2 * MG);
-  __shared__ double sS;
-  const int pid = blockIdx.x;
-  const Tin* a = pop + (size_t)pid * n;
+  const Tin* a = pop + cd.off;
   zero_fill(base, n + 2 * MG);
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = (double)a[i];
+  for (int i = tm.t0; i < n; i += tm.nt) sA[i] = (double)a[i];
   __syncthreads();
   double mloc = 0.0;
-  conv_warp_tiles<TK, false>(sA, sA, n, [&](int, double val) { mloc = val > mloc ? val : mloc; });
+  conv_warp_tiles<TK, false>(sA, sA, n, tm, [&](int, double val) { mloc = val > mloc ? val : mloc; });
   if (threadIdx.x == 0) {
     double S = 0.0;
     for (int i = 0; i < n; ++i) S = __dadd_rn(S, sA[i]);
@@ -249,7 +262,7 @@ k_eval(const Tin* __restrict__ pop, int n, double* __restrict__ outF, int* __res
   if (outN) {
     const double thr = M * (1.0 - tol);
     double cl = 0.0;
-    conv_warp_tiles<TK, false>(sA, sA, n, [&](int, double val) { cl += (val >= thr) ? 1.0 : 0.0; });
+    conv_warp_tiles<TK, false>(sA, sA, n, tm, [&](int, double val) { cl += (val >= thr) ? 1.0 : 0.0; });
     const double cnt = block_sum(cl, sRed);
     if (threadIdx.x == 0) outN[pid] = (int)(cnt + 0.5);
   }
@@ -267,29 +280,33 @@ __host__ __device__ constexpr size_t fw_smem_elems(int n) {
 
 template <int TK>
 __global__ void __launch_bounds__(1024, 1)
-k_frank_wolfe(float* pop, const int* __restrict__ skip, int n, int rounds, int pdhgIters, int nT,
-              float tMax, float tau, float sig) {
+k_frank_wolfe(float* pop, const long long* __restrict__ offsets, const int* __restrict__ order,
+              int n_fixed, int n_max, const int* __restrict__ skip, int rounds, int pdhgIters,
+              int nT, float tMax, float tau, float sig) {
   constexpr int MG = margin<TK>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Cand cd = cand_of(blockIdx.x, offsets, order, n_fixed);
+  const int pid = cd.pid, n = cd.n;
+  if (skip && skip[pid]) return;
+  if (n < 1 || n > n_max) return;
+  const Team tm(32 * warps_for<TK>(n));
   float* base = reinterpret_cast<float*>(smem_raw);
   float* sA = base + MG;
   float* sGb = base + (n + 2 * MG) + MG;
   float* sG = base + 2 * (n + 2 * MG);
   float* sL = sG + n + MG;
   float* sRed = sG + n + (2 * n - 1 + 2 * MG);
-  const int pid = blockIdx.x;
-  if (skip && skip[pid]) return;
-  float* a = pop + (size_t)pid * n;
+  float* a = pop + cd.off;
   const int nb = 2 * n - 1;
   zero_fill(base, (int)fw_smem_elems<TK>(n));
   __syncthreads();
   float sl = 0.f;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; sA[i] = x; sl += x; }
+  for (int i = tm.t0; i < n; i += tm.nt) { const float x = a[i]; sA[i] = x; sl += x; }
   const float s0 = block_sum(sl, sRed);
   if (!(s0 > 0.f)) return;
   {
     const float inv = 1.f / s0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] *= inv;
+    for (int i = tm.t0; i < n; i += tm.nt) sA[i] *= inv;
     __syncthreads();
   }
   if (!(tau > 0.f)) tau = 0.9f / (float)n;
@@ -297,28 +314,28 @@ k_frank_wolfe(float* pop, const int* __restrict__ skip, int n, int rounds, int p
 
   for (int r = 0; r < rounds; ++r) {
     float ml = 0.f;
-    conv_warp_tiles<TK, true>(sA, sA, n, [&](int, float val) { ml = val > ml ? val : ml; });
+    conv_warp_tiles<TK, true>(sA, sA, n, tm, [&](int, float val) { ml = val > ml ? val : ml; });
     const float M = block_max(ml, sRed);
     if (!(M > 0.f)) break;
 
-    for (int i = threadIdx.x; i < n; i += blockDim.x) { sG[i] = sA[i]; sGb[i] = sA[i]; }
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) sL[k] = 0.f;
+    for (int i = tm.t0; i < n; i += tm.nt) { sG[i] = sA[i]; sGb[i] = sA[i]; }
+    for (int k = tm.t0; k < nb; k += tm.nt) sL[k] = 0.f;
     __syncthreads();
 
     for (int it = 0; it < pdhgIters; ++it) {
       // lambda <- [lambda + sigma (a * gbar - M)]_+   (conv fused)
-      conv_warp_tiles<TK, true>(sA, sGb, n, [&](int k, float val) {
+      conv_warp_tiles<TK, true>(sA, sGb, n, tm, [&](int k, float val) {
         const float l = sL[k] + sig * (val - M);
         sL[k] = l > 0.f ? l : 0.f;
       });
       __syncthreads();
       // g_new <- [g + tau (1 - A^T lambda)]_+  parked in gbar
-      corr_warp_tiles<TK>(sA, sL, n, [&](int i, float cv) {
+      corr_warp_tiles<TK>(sA, sL, n, tm, [&](int i, float cv) {
         const float gn = sG[i] + tau * (1.f - cv);
         sGb[i] = gn > 0.f ? gn : 0.f;
       });
       __syncthreads();
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      for (int i = tm.t0; i < n; i += tm.nt) {
         const float gn = sGb[i], go = sG[i];
         sG[i] = gn;
         sGb[i] = 2.f * gn - go;
@@ -327,30 +344,30 @@ k_frank_wolfe(float* pop, const int* __restrict__ skip, int n, int rounds, int p
     }
 
     float sg = 0.f;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) sg += sG[i];
+    for (int i = tm.t0; i < n; i += tm.nt) sg += sG[i];
     sg = block_sum(sg, sRed);
     if (!(sg > 0.f)) break;
     {
       const float inv = 1.f / sg;
-      for (int i = threadIdx.x; i < n; i += blockDim.x) sG[i] *= inv;
+      for (int i = tm.t0; i < n; i += tm.nt) sG[i] *= inv;
       __syncthreads();
     }
     // sum a = sum g = 1  =>  F(h) = 2n max(h*h) for every t
     float bestT = 0.f, bestM = M;
     for (int s = 1; s <= nT; ++s) {
       const float t = tMax * (float)s / (float)nT;
-      for (int i = threadIdx.x; i < n; i += blockDim.x) sGb[i] = (1.f - t) * sA[i] + t * sG[i];
+      for (int i = tm.t0; i < n; i += tm.nt) sGb[i] = (1.f - t) * sA[i] + t * sG[i];
       __syncthreads();
       float lc = 0.f;
-      conv_warp_tiles<TK, true>(sGb, sGb, n, [&](int, float val) { lc = val > lc ? val : lc; });
+      conv_warp_tiles<TK, true>(sGb, sGb, n, tm, [&](int, float val) { lc = val > lc ? val : lc; });
       const float mm = block_max(lc, sRed);
       if (mm < bestM) { bestM = mm; bestT = t; }
     }
     if (!(bestT > 0.f)) break;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) sA[i] = (1.f - bestT) * sA[i] + bestT * sG[i];
+    for (int i = tm.t0; i < n; i += tm.nt) sA[i] = (1.f - bestT) * sA[i] + bestT * sG[i];
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = sA[i];
+  for (int i = tm.t0; i < n; i += tm.nt) a[i] = sA[i];
 }
 
 }  // namespace sidon
@@ -370,32 +387,41 @@ size_t smem_local_search(int n, int dtype) {
 size_t smem_eval(int n) { return sizeof(double) * ((size_t)n + 2 * margin<kTK64>() + 32); }
 size_t smem_fw(int n) { return sizeof(float) * fw_smem_elems<kTK32>(n); }
 
-static int prep(const void* fn, size_t smem) {
-  if ((long long)smem > (long long)smem_optin()) return SIDON_ERR_SMEM;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return set_cuda_error(e);
-  return SIDON_OK;
+static int prep(const void* fn, size_t smem) { return set_dyn_smem(fn, smem); }
+
+// The shared-memory attributes of the fp32 local search, the fp32-input
+// evaluation and the Frank-Wolfe kernels at n_max, set ahead of a stream
+// capture.
+int prepare_simt(int n_max, bool local_search) {
+  int rc = SIDON_OK;
+  if (local_search)
+    rc = prep((const void*)k_local_search<float, kTK32>, smem_local_search(n_max, SIDON_F32));
+  if (!rc) rc = prep((const void*)k_eval<float, kTK64>, smem_eval(n_max));
+  if (!rc) rc = prep((const void*)k_frank_wolfe<kTK32>, smem_fw(n_max));
+  return rc;
 }
 
-int launch_local_search(void* pop, void* mom, void* vel, const int* skip, const int* mode_arr,
-                        int n, int P, int iters, double pS, double pE, double lrS, double lrE,
-                        double b1, double b2, int mode_default, int dtype, cudaStream_t st) {
+int launch_local_search(void* pop, void* mom, void* vel, const long long* offsets,
+                        const int* order, int P, int n_fixed, int n_max, const int* skip,
+                        const int* mode_arr, int iters, double pS, double pE, double lrS,
+                        double lrE, double b1, double b2, int mode_default, int dtype,
+                        cudaStream_t st) {
   if (dtype == SIDON_F32) {
-    const size_t sm = smem_local_search(n, dtype);
+    const size_t sm = smem_local_search(n_max, dtype);
     const void* fn = (const void*)k_local_search<float, kTK32>;
     int rc = prep(fn, sm);
     if (rc) return rc;
-    k_local_search<float, kTK32><<<P, 32 * warps_for<kTK32>(n), sm, st>>>(
-        (float*)pop, (float*)mom, (float*)vel, skip, mode_arr, n, iters, (float)pS, (float)pE,
-        (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default);
+    k_local_search<float, kTK32><<<P, 32 * warps_for<kTK32>(n_max), sm, st>>>(
+        (float*)pop, (float*)mom, (float*)vel, offsets, order, n_fixed, n_max, skip, mode_arr,
+        iters, (float)pS, (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default);
   } else {
-    const size_t sm = smem_local_search(n, dtype);
+    const size_t sm = smem_local_search(n_max, dtype);
     const void* fn = (const void*)k_local_search<double, kTK64>;
     int rc = prep(fn, sm);
     if (rc) return rc;
-    k_local_search<double, kTK64><<<P, 32 * warps_for<kTK64>(n), sm, st>>>(
-        (double*)pop, (double*)mom, (double*)vel, skip, mode_arr, n, iters, pS, pE, lrS, lrE, b1,
-        b2, mode_default);
+    k_local_search<double, kTK64><<<P, 32 * warps_for<kTK64>(n_max), sm, st>>>(
+        (double*)pop, (double*)mom, (double*)vel, offsets, order, n_fixed, n_max, skip,
+        mode_arr, iters, pS, pE, lrS, lrE, b1, b2, mode_default);
   }
   return check_launch();
 }
@@ -418,29 +444,32 @@ int launch_lp_backward(const float* a, const float* saved, const float* b_in, in
   return check_launch();
 }
 
-int launch_eval(const void* pop, int dtype, int n, int P, double* outF, int* outN, double tol,
-                cudaStream_t st) {
-  const size_t sm = smem_eval(n);
-  const int threads = 32 * warps_for<kTK64>(n);
+int launch_eval(const void* pop, int dtype, const long long* offsets, const int* order, int P,
+                int n_fixed, int n_max, double* outF, int* outN, double tol, cudaStream_t st) {
+  const size_t sm = smem_eval(n_max);
+  const int threads = 32 * warps_for<kTK64>(n_max);
   if (dtype == SIDON_F32) {
     int rc = prep((const void*)k_eval<float, kTK64>, sm);
     if (rc) return rc;
-    k_eval<float, kTK64><<<P, threads, sm, st>>>((const float*)pop, n, outF, outN, tol);
+    k_eval<float, kTK64><<<P, threads, sm, st>>>((const float*)pop, offsets, order, n_fixed,
+                                                 n_max, outF, outN, tol);
   } else {
     int rc = prep((const void*)k_eval<double, kTK64>, sm);
     if (rc) return rc;
-    k_eval<double, kTK64><<<P, threads, sm, st>>>((const double*)pop, n, outF, outN, tol);
+    k_eval<double, kTK64><<<P, threads, sm, st>>>((const double*)pop, offsets, order, n_fixed,
+                                                  n_max, outF, outN, tol);
   }
   return check_launch();
 }
 
-int launch_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int pdhg, int nT,
-                       float tMax, float tau, float sig, cudaStream_t st) {
-  const size_t sm = smem_fw(n);
+int launch_frank_wolfe(float* pop, const long long* offsets, const int* order, int P, int n_fixed,
+                       int n_max, const int* skip, int rounds, int pdhg, int nT, float tMax,
+                       float tau, float sig, cudaStream_t st) {
+  const size_t sm = smem_fw(n_max);
   int rc = prep((const void*)k_frank_wolfe<kTK32>, sm);
   if (rc) return rc;
-  k_frank_wolfe<kTK32><<<P, 32 * warps_for<kTK32>(n), sm, st>>>(pop, skip, n, rounds, pdhg, nT,
-                                                                 tMax, tau, sig);
+  k_frank_wolfe<kTK32><<<P, 32 * warps_for<kTK32>(n_max), sm, st>>>(
+      pop, offsets, order, n_fixed, n_max, skip, rounds, pdhg, nT, tMax, tau, sig);
   return check_launch();
 }
 

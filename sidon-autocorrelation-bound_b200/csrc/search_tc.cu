@@ -21,7 +21,10 @@
 //    cb      fp32 padded scratch: b, then the weights c, then G
 //    red     64 floats of reduction scratch, mbarriers, TMEM address, abort flag
 // ---------------------------------------------------------------------------
+#include <mutex>
+
 #include "conv_simt.cuh"
+
 #include "tc_engine.cuh"
 
 namespace sidon {
@@ -62,8 +65,10 @@ struct Shared {
   float* red;
 };
 
-__device__ __forceinline__ Shared setup(int n, bool three, unsigned char* raw) {
-  const Layout Lo(n);
+// Per-CTA set-up for candidates of up to n_max cells: buffer addresses,
+// barriers, TMEM.  begin() then prepares one candidate.
+__device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* raw) {
+  const Layout Lo(n_max);
   unsigned char* base = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
   Shared S;
   S.C.stages = base;
@@ -82,17 +87,14 @@ __device__ __forceinline__ Shared setup(int n, bool three, unsigned char* raw) {
   S.C.m = Lo.m;
   S.C.rc = Lo.rc;
   S.C.rcc = Lo.rcc;
-  S.C.n = n;
-  S.C.dmax = last_tile(n);
+  S.C.n = n_max;
+  S.C.dmax = last_tile(n_max);
   S.C.three = three;
   S.C.done_use = 0;
   S.C.st_next = 0;
   S.C.bc_uses[0] = S.C.bc_uses[1] = 0;
 #pragma unroll
   for (int s = 0; s < STAGES; ++s) S.C.uses[s] = 0;
-  float* z0 = reinterpret_cast<float*>(base + Lo.off_sa);
-  for (int i = threadIdx.x; i < Lo.sa_len; i += blockDim.x) z0[i] = 0.f;
-  for (int i = threadIdx.x; i < Lo.cb_len; i += blockDim.x) S.cb[i] = 0.f;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&S.C.full[s], NBUILD_WARPS);
@@ -114,6 +116,23 @@ __device__ __forceinline__ Shared setup(int n, bool three, unsigned char* raw) {
   return S;
 }
 
+// Prepare the CTA for a candidate of n cells (n <= n_max of setup): zero the
+// height and scratch buffers (their margins must read as zero) and set the
+// geometry.  Ends synchronised.
+__device__ __forceinline__ void begin(Shared& S, int n, int n_max) {
+  const Layout Lo(n_max), Ln(n);
+  float* z0 = S.sa - 136;
+  __syncthreads();
+  for (int i = threadIdx.x; i < Lo.sa_len; i += blockDim.x) z0[i] = 0.f;
+  for (int i = threadIdx.x; i < Lo.cb_len; i += blockDim.x) S.cb[i] = 0.f;
+  S.C.n = n;
+  S.C.m = Ln.m;
+  S.C.rc = Ln.rc;
+  S.C.rcc = Ln.rcc;
+  S.C.dmax = last_tile(n);
+  __syncthreads();
+}
+
 __device__ __forceinline__ void teardown(Shared& S) {
   fence_before();
   __syncthreads();
@@ -132,24 +151,34 @@ __device__ __forceinline__ void prime(Ctx& C, bool corr_too) {
 }
 
 // ------------------------------ local search ------------------------------
+// Candidates: uniform rows of n_fixed cells (offsets == NULL) or a ragged
+// batch (row p = pop[offsets[p] .. offsets[p+1])).  CTA b runs slots
+// b, b + gridDim.x, ... of `order` (NULL = 0..P-1): launched with one CTA per
+// candidate it is the plain batched kernel, launched with one CTA per SM and
+// a longest-first order it is the persistent ragged kernel.
 __global__ void __launch_bounds__(NTHREADS, 1)
-k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ skip,
-                  const int* __restrict__ mode_arr, int n, int iters, float pStart, float pEnd,
-                  float lrStart, float lrEnd, float beta1, float beta2, int mode_default, int three,
-                  unsigned int* status) {
+k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restrict__ offsets,
+                  const int* __restrict__ order, int P, int n_fixed, int n_max,
+                  const int* __restrict__ skip, const int* __restrict__ mode_arr, int iters,
+                  float pStart, float pEnd, float lrStart, float lrEnd, float beta1, float beta2,
+                  int mode_default, int three, unsigned int* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  const int pid = blockIdx.x;
-  if (skip && skip[pid]) return;
-  const int mode = mode_arr ? mode_arr[pid] : mode_default;
-  float* a = pop + (size_t)pid * n;
-  float* mg = mom + (size_t)pid * n;
-  float* vg = vel + (size_t)pid * n;
-
-  Shared S = setup(n, three != 0, smem_raw);
+  Shared S = setup(n_max, three != 0, smem_raw);
   Ctx& C = S.C;
-  const int nb = 2 * n - 1;
   const Lane ln;
-  __syncthreads();
+  for (int slot = blockIdx.x; slot < P; slot += gridDim.x) {
+  const int pid = order ? order[slot] : slot;
+  if (skip && skip[pid]) continue;
+  const long long off = offsets ? offsets[pid] : (long long)pid * n_fixed;
+  const int n = offsets ? (int)(offsets[pid + 1] - off) : n_fixed;
+  if (n < 1 || n > n_max) continue;
+  if (*((volatile int*)C.abort)) break;
+  const int mode = mode_arr ? mode_arr[pid] : mode_default;
+  float* a = pop + off;
+  float* mg = mom + off;
+  float* vg = vel + off;
+  begin(S, n, n_max);
+  const int nb = 2 * n - 1;
   for (int i = threadIdx.x; i < n; i += blockDim.x) { S.sa[pidx(i)] = a[i]; mg[i] = 0.f; vg[i] = 0.f; }
   __syncthreads();
 
@@ -240,6 +269,7 @@ k_local_search_tc(float* pop, float* mom, float* vel, const int* __restrict__ sk
   }
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = S.sa[pidx(i)];
+  }  // candidates
   teardown(S);
 }
 
@@ -259,10 +289,10 @@ k_lp_forward_tc(const float* __restrict__ pop, int n, float p, float* __restrict
   const int pid = blockIdx.x;
   Shared S = setup(n, three != 0, smem_raw);
   Ctx& C = S.C;
+  begin(S, n, n);
   const int nb = 2 * n - 1;
   const Lane ln;
   const float* a = pop + (size_t)pid * n;
-  __syncthreads();
   double sl = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; S.sa[pidx(i)] = x; sl += x; }
   const double Ssum = block_sum(sl, s_red);
@@ -309,11 +339,11 @@ k_lp_backward_tc(const float* __restrict__ pop, const float* __restrict__ saved,
   const int pid = blockIdx.x;
   Shared S = setup(n, three != 0, smem_raw);
   Ctx& C = S.C;
+  begin(S, n, n);
   const int nb = 2 * n - 1;
   const Lane ln;
   const float* a = pop + (size_t)pid * n;
   const float M = saved[4 * pid + 0], Ssum = saved[4 * pid + 1], R = saved[4 * pid + 2];
-  __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] = a[i];
   __syncthreads();
   prime(C, true);
@@ -348,10 +378,21 @@ k_lp_backward_tc(const float* __restrict__ pop, const float* __restrict__ saved,
 namespace sidon_host {
 using namespace sidon;
 
+// device address of the status word, looked up once per device (so that
+// launches inside a stream capture make no symbol lookup)
 static unsigned int* status_word() {
-  void* p = nullptr;
-  if (cudaGetSymbolAddress(&p, tc::g_status_word) != cudaSuccess) return nullptr;
-  return (unsigned int*)p;
+  constexpr int kMaxDev = 64;
+  static std::mutex mu;
+  static unsigned int* addr[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, tc::g_status_word) != cudaSuccess) return nullptr;
+    addr[dev] = (unsigned int*)p;
+  }
+  return addr[dev];
 }
 
 int device_status(int reset) {
@@ -375,27 +416,38 @@ static int tc_n_ok(int n) {
   return (n >= 1 && tc::conv_width(m) + tc::corr_width(m) <= 512) ? SIDON_OK : SIDON_ERR_N;
 }
 
-static int prep_tc(const void* fn, size_t sm) {
-  if ((long long)sm > (long long)smem_optin()) return SIDON_ERR_SMEM;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return set_cuda_error(e);
-  return SIDON_OK;
+static int prep_tc(const void* fn, size_t sm) { return set_dyn_smem(fn, sm); }
+
+// Everything a local-search launch at n_max sets up on the host side (the
+// shared-memory attribute, the status word's address), done ahead of a
+// stream capture.
+int prepare_local_search_tc(int n_max) {
+  int rc = tc_n_ok(n_max);
+  if (rc) return rc;
+  rc = prep_tc((const void*)tc::k_local_search_tc, smem_local_search_tc(n_max));
+  if (rc) return rc;
+  return status_word() ? SIDON_OK : SIDON_ERR_CUDA;
 }
 
-int launch_local_search_tc(float* pop, float* mom, float* vel, const int* skip,
-                           const int* mode_arr, int n, int P, int iters, double pS, double pE,
-                           double lrS, double lrE, double b1, double b2, int mode_default,
-                           int precision, cudaStream_t st) {
-  int rc = tc_n_ok(n);
+int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* offsets,
+                           const int* order, int P, int n_fixed, int n_max, const int* skip,
+                           const int* mode_arr, int iters, double pS, double pE, double lrS,
+                           double lrE, double b1, double b2, int mode_default, int precision,
+                           cudaStream_t st) {
+  int rc = tc_n_ok(n_max);
   if (rc) return rc;
-  const size_t sm = smem_local_search_tc(n);
+  const size_t sm = smem_local_search_tc(n_max);
   rc = prep_tc((const void*)tc::k_local_search_tc, sm);
   if (rc) return rc;
   unsigned int* sw = status_word();
   if (!sw) return SIDON_ERR_CUDA;
-  tc::k_local_search_tc<<<P, tc::NTHREADS, sm, st>>>(
-      pop, mom, vel, skip, mode_arr, n, iters, (float)pS, (float)pE, (float)lrS, (float)lrE,
-      (float)b1, (float)b2, mode_default, precision == SIDON_PREC_BF16X3 ? 1 : 0, sw);
+  // one CTA per candidate for a uniform batch; persistent (one CTA per SM)
+  // for a ragged batch
+  const int grid = offsets ? (P < sm_count() ? P : sm_count()) : P;
+  tc::k_local_search_tc<<<grid, tc::NTHREADS, sm, st>>>(
+      pop, mom, vel, offsets, order, P, n_fixed, n_max, skip, mode_arr, iters, (float)pS,
+      (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default,
+      precision == SIDON_PREC_BF16X3 ? 1 : 0, sw);
   return check_launch();
 }
 

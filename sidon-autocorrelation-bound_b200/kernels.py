@@ -12,6 +12,8 @@ raise ``SidonError``; where ``runFrankWolfe`` returns false
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import torch
 
@@ -239,3 +241,181 @@ def island_migrate(pop: torch.Tensor, fit: torch.Tensor, n_islands: int, k: int 
               _dev(fit, "fit", torch.float64), P, int(n_islands), int(k),
               _dev(order, "order", torch.int32), _stream(stream))
     return order
+
+
+# ------------------------------ ragged batches ------------------------------
+class RaggedBatch:
+    """P candidates of different sizes back to back in one fp32 tensor:
+    candidate p is ``flat[offsets[p]:offsets[p+1]]``.  ``offsets`` lives on
+    the device (int64, P+1 entries) with a host copy in ``sizes``;
+    ``order`` is the longest-first processing order (device int32)."""
+
+    def __init__(self, rows, device="cuda", dtype=torch.float32):
+        sizes = [int(len(r)) for r in rows]
+        if not sizes or min(sizes) < 1:
+            raise ValueError("a ragged batch needs candidates of at least one cell")
+        self.sizes = sizes
+        self.P = len(sizes)
+        self.n_max = max(sizes)
+        off = np.zeros(self.P + 1, dtype=np.int64)
+        off[1:] = np.cumsum(sizes)
+        self.host_offsets = off
+        flat = np.concatenate([np.asarray(r, dtype=np.float64) for r in rows])
+        self.flat = torch.tensor(flat, dtype=dtype, device=device)
+        self.offsets = torch.tensor(off, device=device)
+        self.order = ragged_order(self.offsets, self.P)
+
+    def rows(self) -> list[np.ndarray]:
+        """The candidates as host arrays (copies)."""
+        h = self.flat.detach().cpu().numpy()
+        return [h[self.host_offsets[p]:self.host_offsets[p + 1]].copy() for p in range(self.P)]
+
+    def row(self, p: int) -> torch.Tensor:
+        """Device view of candidate p."""
+        return self.flat[int(self.host_offsets[p]):int(self.host_offsets[p + 1])]
+
+
+def ragged_order(offsets: torch.Tensor, P: int, out: torch.Tensor | None = None,
+                 stream=None) -> torch.Tensor:
+    """Longest-first order of a ragged batch (ties by index)."""
+    if out is None:
+        out = torch.empty(P, dtype=torch.int32, device=offsets.device)
+    _lib.call("sidon_ragged_order", _dev(offsets, "offsets", torch.int64), int(P),
+              _dev(out, "order", torch.int32), _stream(stream))
+    return out
+
+
+def run_local_search_ragged(batch: RaggedBatch, iters: int, p_start: float, p_end: float,
+                            lr_start: float, lr_end: float, precision: str = "bf16x3",
+                            mode_arr: torch.Tensor | None = None,
+                            skip: torch.Tensor | None = None, mom: torch.Tensor | None = None,
+                            vel: torch.Tensor | None = None, beta1: float = 0.9,
+                            beta2: float = 0.999, mode_default: int = 0, use_order: bool = True,
+                            stream=None) -> None:
+    """run_local_search over a ragged batch, in place."""
+    if mom is None:
+        mom = torch.empty_like(batch.flat)
+    if vel is None:
+        vel = torch.empty_like(batch.flat)
+    _lib.call("sidon_local_search_ragged", _dev(batch.flat, "pop", torch.float32),
+              _dev(mom, "mom", torch.float32), _dev(vel, "vel", torch.float32),
+              batch.offsets.data_ptr(), batch.order.data_ptr() if use_order else None,
+              batch.n_max, _opt(skip, "skip", torch.int32),
+              _opt(mode_arr, "mode_arr", torch.int32), batch.P, int(iters), float(p_start),
+              float(p_end), float(lr_start), float(lr_end), float(beta1), float(beta2),
+              int(mode_default), PRECISIONS[precision], _stream(stream))
+
+
+def run_eval_ragged(batch: RaggedBatch, active_tol: float = 1e-4, with_nactive: bool = True,
+                    stream=None):
+    """run_eval over a ragged batch: (F fp64 [P], nactive int32 [P] | None)."""
+    dev = batch.flat.device
+    F = torch.empty(batch.P, dtype=torch.float64, device=dev)
+    N = torch.empty(batch.P, dtype=torch.int32, device=dev) if with_nactive else None
+    _lib.call("sidon_eval_ragged", batch.flat.data_ptr(), _dtype_code(batch.flat),
+              batch.offsets.data_ptr(), batch.order.data_ptr(), batch.n_max, batch.P,
+              F.data_ptr(), None if N is None else N.data_ptr(), float(active_tol),
+              _stream(stream))
+    return F, N
+
+
+def run_frank_wolfe_ragged(batch: RaggedBatch, rounds: int, pdhg_iters: int, nT: int = 12,
+                           t_max: float = 0.30, skip: torch.Tensor | None = None,
+                           tau: float = 0.0, sigma: float = 0.0, stream=None) -> None:
+    """run_frank_wolfe over a ragged batch, in place."""
+    _lib.call("sidon_frank_wolfe_ragged", _dev(batch.flat, "pop", torch.float32),
+              batch.offsets.data_ptr(), batch.order.data_ptr(), batch.n_max,
+              _opt(skip, "skip", torch.int32), batch.P, int(rounds), int(pdhg_iters), int(nT),
+              float(t_max), float(tau), float(sigma), _stream(stream))
+
+
+def island_migrate_ragged(batch: RaggedBatch, fit: torch.Tensor, n_islands: int, k: int = 1,
+                          order: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """island_migrate over a ragged batch (migrants of another size are
+    resampled and renormalised; their fit becomes NaN).  Returns the ranking."""
+    if order is None:
+        order = torch.empty(batch.P, dtype=torch.int32, device=batch.flat.device)
+    _lib.call("sidon_island_migrate_ragged", _dev(batch.flat, "pop", torch.float32),
+              batch.offsets.data_ptr(), _dev(fit, "fit", torch.float64), batch.P,
+              int(n_islands), int(k), _dev(order, "order", torch.int32), _stream(stream))
+    return order
+
+
+# ------------------------------ anneal driver -------------------------------
+def anneal_config(steps: int = 5000, p_start: float = 2.0, p_end: float = 1024.0,
+                  lr_start: float = 1e-3, lr_end: float = 1e-3, beta1: float = 0.9,
+                  beta2: float = 0.999, precision: str = "bf16x3", fw_every: int = 250,
+                  fw_rounds: int = 1, pdhg_iters: int = 200, fw_nT: int = 12,
+                  fw_t_max: float = 0.30, fw_tau: float = 0.9, fw_sigma: float = 0.9,
+                  n_islands: int = 16, migrate_every: int = 500,
+                  k_migrate: int = 4) -> _lib.AnnealConfig:
+    """struct sidon_anneal_config; the defaults are the batched island anneal
+    (5000 steps, p 2 -> 1024, Frank-Wolfe every 250 steps with 200
+    Chambolle-Pock iterations at tau = sigma = 0.9 / ||a||_1 = 0.9 on the
+    normalised heights, 16 islands, top-4 migration every 500 steps)."""
+    return _lib.AnnealConfig(int(steps), float(p_start), float(p_end), float(lr_start),
+                             float(lr_end), float(beta1), float(beta2), PRECISIONS[precision],
+                             int(fw_every), int(fw_rounds), int(pdhg_iters), int(fw_nT),
+                             float(fw_t_max), float(fw_tau), float(fw_sigma), int(n_islands),
+                             int(migrate_every), int(k_migrate))
+
+
+def _anneal_args(batch, cfg, fit, rank, mom, vel):
+    if isinstance(batch, RaggedBatch):
+        pop, off, order, n_max, P = (batch.flat, batch.offsets.data_ptr(),
+                                     batch.order.data_ptr(), batch.n_max, batch.P)
+    else:
+        n_max, P = _pop_shape(batch)
+        pop, off, order = batch, None, None
+    dev = pop.device
+    if fit is None:
+        fit = torch.empty(P, dtype=torch.float64, device=dev)
+    if rank is None:
+        rank = torch.empty(P, dtype=torch.int32, device=dev)
+    if mom is None:
+        mom = torch.empty_like(pop)
+    if vel is None:
+        vel = torch.empty_like(pop)
+    args = (_dev(pop, "pop", torch.float32), _dev(mom, "mom", torch.float32),
+            _dev(vel, "vel", torch.float32), off, order, n_max, P,
+            _dev(fit, "fit", torch.float64), _dev(rank, "rank", torch.int32))
+    return args, fit, rank, (mom, vel)
+
+
+def anneal(batch, cfg: _lib.AnnealConfig, fit: torch.Tensor | None = None,
+           rank: torch.Tensor | None = None, mom: torch.Tensor | None = None,
+           vel: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """Enqueue the whole island anneal on a stream (a RaggedBatch or a
+    uniform [P, n] fp32 tensor); returns fit (fp64 F at the end)."""
+    args, fit, rank, _ = _anneal_args(batch, cfg, fit, rank, mom, vel)
+    _lib.call("sidon_anneal", *args, C.byref(cfg), _stream(stream))
+    return fit
+
+
+class AnnealGraph:
+    """The anneal recorded once as a CUDA graph (sidon_anneal_capture);
+    ``launch`` replays it.  Holds the scratch tensors it was recorded with."""
+
+    def __init__(self, batch, cfg: _lib.AnnealConfig, fit=None, rank=None, mom=None, vel=None):
+        args, self.fit, self.rank, self._scratch = _anneal_args(batch, cfg, fit, rank, mom, vel)
+        self._batch = batch
+        self._cfg = cfg
+        h = C.c_void_p()
+        _lib.call("sidon_anneal_capture", *args, C.byref(cfg), C.byref(h))
+        self._h = h
+
+    def launch(self, stream=None) -> None:
+        if not self._h:
+            raise RuntimeError("graph destroyed")
+        _lib.call("sidon_graph_launch", self._h, _stream(stream))
+
+    def close(self) -> None:
+        if self._h:
+            _lib.load().sidon_graph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -62,3 +62,17 @@ def uneven_sizes(P: int, seed: int, levels=(512, 1024, 2048, 4096, 8400)) -> np.
     """n per candidate drawn uniformly from the ladder levels (batched islands)."""
     r = _rng(seed, 1 << 30)
     return np.asarray(levels)[r.integers(0, len(levels), P)]
+
+
+def ragged_population(sizes, seed: int, kind: str = "structured",
+                      normalise: bool = True, dtype=np.float32) -> list[np.ndarray]:
+    """One candidate per entry of sizes (candidate p from stream [seed, p])."""
+    gen = {"structured": structured_one, "lognormal": lognormal_one}[kind]
+    rows = []
+    for p, n in enumerate(sizes):
+        a = gen(int(n), seed, p)
+        if normalise:
+            s = a.sum()
+            a = a / (s if s > 0 else 1.0)
+        rows.append(a.astype(dtype))
+    return rows
