@@ -429,7 +429,8 @@ SO_EXPORT void so_coarsen_f64(const double* src, int n2, int P, double* dst) {
 /* ========================= island ranking + migration ===================== */
 /* src/main.cu:676-692: each island (PI consecutive slots) is ranked by fp64
  * fitness, ascending; ties are broken by slot index (the reference's
- * std::sort leaves tie order unspecified).  Migration: the j-th best of
+ * std::sort leaves tie order unspecified) and NaN ranks last (undefined for
+ * std::sort).  Migration: the j-th best of
  * island i overwrites the j-th worst of island (i+1) mod NI, j < k (k = 1 is
  * the reference's "best of i -> worst of i+1").  order_out[i*PI + r] = slot of
  * rank r in island i, computed before migration.  Requires 2k <= PI. */
@@ -437,8 +438,12 @@ static const double* g_fit_cmp;
 static int cmp_slot(const void* x, const void* y) {
   const int a = *(const int*)x, b = *(const int*)y;
   const double fa = g_fit_cmp[a], fb = g_fit_cmp[b];
-  if (fa < fb) return -1;
-  if (fa > fb) return 1;
+  const int na = fa != fa, nb = fb != fb;   /* NaN ranks after every number */
+  if (na != nb) return na - nb;
+  if (!na) {
+    if (fa < fb) return -1;
+    if (fa > fb) return 1;
+  }
   return (a > b) - (a < b);
 }
 SO_EXPORT int so_island_migrate_f32(float* pop, int n, double* fit, int P, int NI, int k,

@@ -185,3 +185,35 @@ def test_island_migrate_semantics(orc):
     assert np.array_equal(out[4], pop[1]) and f2[4] == fit[1]
     assert np.array_equal(out[11], pop[7]) and f2[11] == fit[7]
     assert np.array_equal(out[0], pop[8]) and f2[0] == fit[8]
+
+
+def test_oracle_resample_restates_injection(orc):
+    """so_resample_f32 against a direct restatement of src/main.cu:555-562
+    (dst_i = src[min(m-1, i m / n)], S = sum in fp64, dst_i = fl32(x_i / S))."""
+    rng = np.random.default_rng(3)
+    for m, n in [(3, 7), (7, 3), (100, 100), (512, 8400), (8400, 512), (1, 9)]:
+        src = rng.uniform(0, 1, m).astype(np.float32)
+        xs = [float(src[min(m - 1, i * m // n)]) for i in range(n)]
+        S = 0.0
+        for x in xs:
+            S += x
+        want = np.array([np.float32(x / S) for x in xs], dtype=np.float32)
+        np.testing.assert_array_equal(orc.resample(src, n), want)
+
+
+def test_oracle_ragged_migration_rules(orc):
+    sizes = [4, 4, 6, 6, 4, 6, 4, 4]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    flat = np.arange(off[-1], dtype=np.float32) + 1
+    fit = np.array([1.0, np.nan, 3.0, 0.5, 2.0, 0.1, 0.2, 0.3])
+    out, f2, order = orc.island_migrate_ragged(flat, off, fit, 2, 1)
+    # island 0 = slots 0..3 ranked 3, 0, 2, 1 (NaN last); island 1 = 5, 6, 7, 4
+    assert order.tolist() == [3, 0, 2, 1, 5, 6, 7, 4]
+    # best of island 0 (slot 3, n=6) -> worst of island 1 (slot 4, n=4): resampled
+    np.testing.assert_array_equal(out[off[4]:off[5]], orc.resample(flat[off[3]:off[4]], 4))
+    assert np.isnan(f2[4])
+    # best of island 1 (slot 5, n=6) -> worst of island 0 (slot 1, n=4): resampled
+    np.testing.assert_array_equal(out[off[1]:off[2]], orc.resample(flat[off[5]:off[6]], 4))
+    # untouched rows keep their values and fitness
+    np.testing.assert_array_equal(out[off[0]:off[1]], flat[off[0]:off[1]])
+    assert f2[0] == 1.0 and f2[5] == 0.1
