@@ -1,15 +1,16 @@
 """Benchmark: batched L^p-annealed projected-Adam steps (forward convolution +
 adjoint correlation + update) at n = 8400 cells, B = 256 candidates per GPU.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|fp32]
-                    [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|bf16x1|fp32]
+                    [--impl ours|reference] [--workload lp_adam|islands]
 
 One *step* = every candidate of the batch advances one Adam step.  The timed
 region is ONE launch of the fused local-search kernel running K steps (the
 population stays resident in shared memory), bracketed by a barrier and
 device synchronisation, timed with CUDA events on the launching stream, max
 over ranks.  ``value`` = whole-job batched steps/s (N GPUs x K steps / max
-time).  ``e2e`` = the same metric through the public call with host buffers:
+time) of the BF16x3 tensor-core step (default ``--precision``); the FP32 SIMT
+form of the same step is timed after it for ``speedup_vs_fp32_simt``.  ``e2e`` = the same metric through the public call with host buffers:
 per step an H2D copy of the population from pinned memory, one
 ``run_local_search`` step and a D2H copy of the updated population.
 
@@ -237,6 +238,23 @@ def our_arm(args) -> None:
     ms_max = t.item()
     launches = 1
 
+    # the FP32 SIMT form of the same step, for the speed-up the metric names
+    simt = None
+    if prec != "fp32":
+        k32 = max(3, min(args.steps, 20))
+        kernels.run_local_search(pop, 3, mom=mom, vel=vel, precision="fp32", **ANNEAL)
+        pop.copy_(torch.as_tensor(host, device=dev))
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        kernels.run_local_search(pop, k32, mom=mom, vel=vel, precision="fp32", **ANNEAL)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        simt = k32 / (s0.elapsed_time(s1) / 1e3)
+        pop.copy_(torch.as_tensor(host, device=dev))
+        run(pop, args.steps)
+
     # search-time F (the step's own arithmetic) error vs fp64 on the final population
     Fcert, _ = kernels.run_eval(pop, with_nactive=False)
     _, saved, _ = kernels.lp_forward(pop, 2.0, precision=prec)
@@ -300,6 +318,8 @@ def our_arm(args) -> None:
                        "l2": "single launch of K steps, population resident in shared memory; "
                              "L2 flushed (256 MB write) before the timed launch"},
             "candidate_steps_per_s": value * BATCH,
+            "fp32_simt_steps_per_s": simt,
+            "speedup_vs_fp32_simt": (value / ws) / simt if simt else None,
             "f_evals_per_s": value * BATCH,
             "f_rel_err_vs_fp64": f_rel,
             "roofline": roof,
@@ -318,6 +338,109 @@ def our_arm(args) -> None:
         dist.destroy_process_group()
 
 
+# ------------------------------ batched islands -----------------------------
+ISLAND_LEVELS = (512, 1024, 2048, 4096, 8400)
+
+
+def islands_arm(args) -> None:
+    """The batched uneven-island anneal: 1024 candidates with n uniform over
+    the ladder levels (plain-method heights), one CUDA graph holding the
+    5000-step anneal (p 2 -> 1024), a Frank-Wolfe step every 250 steps (200
+    Chambolle-Pock iterations, tau = sigma = 0.9 / ||a||_1), 16 islands with
+    top-4 migration every 500 steps ranked by fp64 F.  Prints one JSON line
+    (its own metric; not the headline line)."""
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import sidon_b200
+    sidon_b200.load(build=not (ROOT / "sidon-autocorrelation-bound_b200" / "libsidon_b200.so").exists())
+    from sidon_b200 import kernels, synth
+
+    P = args.islands_P
+    sizes = synth.uneven_sizes(P, seed=3 + rank, levels=ISLAND_LEVELS)
+    rows = synth.ragged_population(sizes, seed=3 + rank)
+    batch = kernels.RaggedBatch(rows, device=dev)
+    start_flat = batch.flat.clone()
+    cfg = kernels.anneal_config(steps=args.anneal_steps, precision=args.precision,
+                                pdhg_iters=args.pdhg_iters, fw_every=args.fw_every,
+                                fw_tau=0.9, fw_sigma=0.9, fw_precision=args.fw_precision)
+    F0, _ = kernels.run_eval_ragged(batch, with_nactive=False)
+    F0 = F0.cpu().numpy()
+
+    # warm-up: a short anneal with the same kernels (untimed)
+    wcfg = kernels.anneal_config(steps=max(3, args.warmup) * 2, precision=args.precision,
+                                 pdhg_iters=4, fw_every=max(3, args.warmup), migrate_every=0,
+                                 fw_precision=args.fw_precision)
+    kernels.anneal(batch, wcfg)
+    batch.flat.copy_(start_flat)
+    graph = kernels.AnnealGraph(batch, cfg)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    flush.fill_(1.0)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(stream)
+        graph.launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = e0.elapsed_time(e1)
+    F1 = graph.fit.cpu().numpy()
+    assert bool((batch.flat >= 0).all())
+
+    # phase split: one 250-step local-search segment and one Frank-Wolfe step
+    batch.flat.copy_(start_flat)
+    seg = min(cfg.fw_every or cfg.steps, cfg.steps)
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+    ls_ms = timed(lambda: kernels.run_local_search_ragged(batch, seg, 2.0, 4.0, 1e-3, 1e-3,
+                                                           precision=args.precision))
+    fw_ms = timed(lambda: kernels.run_frank_wolfe_tc_ragged(
+        batch, 1, cfg.pdhg_iters, cfg.fw_nT, cfg.fw_t_max, tau=0.9, sigma=0.9,
+        precision=args.precision if args.precision != "fp32" else "bf16x3"))
+    fw_simt_ms = timed(lambda: kernels.run_frank_wolfe_ragged(batch, 1, cfg.pdhg_iters, cfg.fw_nT,
+                                                               cfg.fw_t_max, tau=0.9, sigma=0.9))
+    graph.close()
+
+    n2 = float(np.sum(np.asarray(sizes, dtype=np.float64) ** 2))
+    adam_flop = 4.0 * n2 * cfg.steps
+    n_fw = cfg.steps // cfg.fw_every if cfg.fw_every else 0
+    fw_flop = (4.0 * n2 * cfg.pdhg_iters + 26.0 * n2) * n_fw
+    ck = clk.summary()
+    if rank == 0:
+        line = {
+            "metric": "island_anneal_candidate_steps_per_s",
+            "value": P * cfg.steps / (total_ms / 1e3), "unit": "candidate-steps/s",
+            "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "anneal_seconds": total_ms / 1e3,
+            "config": {"workload": f"batched uneven islands: P={P}, n uniform over "
+                                   f"{list(ISLAND_LEVELS)}, {cfg.steps} steps p 2->1024, "
+                                   f"FW every {cfg.fw_every} ({cfg.pdhg_iters} PDHG), "
+                                   f"16 islands top-4 every 500, one CUDA graph",
+                       "precision": args.precision, "sizes_hist":
+                       {int(l): int(np.sum(sizes == l)) for l in ISLAND_LEVELS}},
+            "flop": {"adam": adam_flop, "frank_wolfe": fw_flop,
+                     "tflops_overall": (adam_flop + fw_flop) / (total_ms / 1e3) / 1e12},
+            "fw_precision": args.fw_precision,
+            "phase_ms": {"local_search_segment": ls_ms, "segment_steps": seg,
+                         "frank_wolfe_step": fw_ms, "frank_wolfe_step_fp32_simt": fw_simt_ms,
+                         "adam_tflops": 4.0 * n2 * seg / (ls_ms / 1e3) / 1e12,
+                         "fw_tflops": (4.0 * n2 * cfg.pdhg_iters + 26.0 * n2) / (fw_ms / 1e3) / 1e12},
+            "F": {"start_median": float(np.median(F0)), "end_median": float(np.nanmedian(F1)),
+                  "end_best": float(np.nanmin(F1))},
+            "clocks": {"sm_mhz": ck["sm_mhz"], "sm_max_mhz": ck["sm_max_mhz"],
+                       "reasons": ck["reasons"]},
+        }
+        print(json.dumps(line))
+
+
 def _traffic(prec: str):
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
@@ -332,8 +455,14 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default=os.environ.get("SIDON_BENCH_PRECISION", "fp32"),
+    ap.add_argument("--precision", default=os.environ.get("SIDON_BENCH_PRECISION", "bf16x3"),
                     choices=["fp32", "bf16x3", "bf16x1"])
+    ap.add_argument("--workload", default="lp_adam", choices=["lp_adam", "islands"])
+    ap.add_argument("--islands-P", type=int, default=1024)
+    ap.add_argument("--anneal-steps", type=int, default=5000)
+    ap.add_argument("--fw-every", type=int, default=250)
+    ap.add_argument("--pdhg-iters", type=int, default=200)
+    ap.add_argument("--fw-precision", default="bf16x3", choices=["fp32", "bf16x3", "bf16x1"])
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -341,6 +470,8 @@ def main() -> None:
         args.warmup = 3
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload == "islands":
+        islands_arm(args)
     else:
         our_arm(args)
 

@@ -176,6 +176,19 @@ SIDON_API int sidon_lp_backward(const float* a, const float* saved, const float*
 SIDON_API int sidon_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int pdhg_iters,
                       int nT, float t_max, float tau, float sigma, void* stream);
 
+/* sidon_frank_wolfe with the Chambolle-Pock convolutions and correlations
+ * on the tensor cores (precision BF16X3 or BF16X1): the same rounds,
+ * iterations, steps and line search; the round's M and every line-search
+ * maximum are refined in fp64 over the near-maximal k, so a move is taken
+ * only when it lowers the refined max_k b_k.  g_scratch / gbar_scratch:
+ * device fp32 [P][n] work rows (the primal iterate and its extrapolation;
+ * their contents on entry are ignored).  Not bit-identical to the fp32 step:
+ * the products round differently.  Same counterpart as sidon_frank_wolfe. */
+SIDON_API int sidon_frank_wolfe_tc(float* pop, float* g_scratch, float* gbar_scratch,
+                                   const int* skip, int n, int P, int rounds, int pdhg_iters,
+                                   int nT, float t_max, float tau, float sigma, int precision,
+                                   void* stream);
+
 /* Cell split n -> 2n: dst[p][2i] = dst[p][2i+1] = src[p][i].
  * Replaces kRefine<T> (src/kernels.cuh:538-547) and the host refine
  * (src/main.cu:491-495). */
@@ -230,6 +243,14 @@ SIDON_API int sidon_frank_wolfe_ragged(float* pop, const long long* offsets, con
                                        int pdhg_iters, int nT, float t_max, float tau,
                                        float sigma, void* stream);
 
+/* sidon_frank_wolfe_tc over a ragged fp32 batch (g_scratch / gbar_scratch
+ * in pop's layout); persistent, one CTA per SM. */
+SIDON_API int sidon_frank_wolfe_tc_ragged(float* pop, float* g_scratch, float* gbar_scratch,
+                                          const long long* offsets, const int* order, int n_max,
+                                          const int* skip, int P, int rounds, int pdhg_iters,
+                                          int nT, float t_max, float tau, float sigma,
+                                          int precision, void* stream);
+
 /* sidon_island_migrate over a ragged fp32 batch: a migrant of another size
  * is resampled by nearest neighbour, dst[t] = src[min(m-1, t m / n)], and
  * normalised to sum 1 in fp64 (the injection of src/main.cu:555-562); its
@@ -262,6 +283,7 @@ typedef struct sidon_anneal_config {
   int fw_every;              /* Frank-Wolfe after every fw_every steps (0 = never) */
   int fw_rounds, pdhg_iters, fw_nT;
   float fw_t_max, fw_tau, fw_sigma;  /* tau, sigma <= 0: the reference steps */
+  int fw_precision;          /* FP32_SIMT, or BF16X1 / BF16X3 (tensor cores, mom/vel as scratch) */
   int n_islands;             /* islands of P / n_islands consecutive candidates */
   int migrate_every;         /* migration after every migrate_every steps (0 = never) */
   int k_migrate;

@@ -39,6 +39,7 @@ SIGNATURES = {
     "sidon_lp_forward": (_i, [_vp, _i, _i, _d, _vp, _vp, _vp, _i, _vp]),
     "sidon_lp_backward": (_i, [_vp, _vp, _vp, _i, _i, _d, _vp, _i, _vp]),
     "sidon_frank_wolfe": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _vp]),
+    "sidon_frank_wolfe_tc": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _i, _vp]),
     "sidon_refine": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "sidon_coarsen": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "sidon_island_migrate": (_i, [_vp, _i, _vp, _i, _i, _i, _vp, _vp]),
@@ -47,6 +48,8 @@ SIGNATURES = {
                                        _d, _d, _d, _i, _i, _vp]),
     "sidon_eval_ragged": (_i, [_vp, _i, _vp, _vp, _i, _i, _vp, _vp, _d, _vp]),
     "sidon_frank_wolfe_ragged": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, _i, _i, _f, _f, _f, _vp]),
+    "sidon_frank_wolfe_tc_ragged": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp, _i, _i, _i, _i, _f,
+                                         _f, _f, _i, _vp]),
     "sidon_island_migrate_ragged": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _vp]),
     "sidon_anneal": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
     "sidon_anneal_capture": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
@@ -67,6 +70,7 @@ class AnnealConfig(C.Structure):
         ("fw_every", _i),
         ("fw_rounds", _i), ("pdhg_iters", _i), ("fw_nT", _i),
         ("fw_t_max", _f), ("fw_tau", _f), ("fw_sigma", _f),
+        ("fw_precision", _i),
         ("n_islands", _i),
         ("migrate_every", _i),
         ("k_migrate", _i),

@@ -32,7 +32,12 @@ int launch_island_migrate(float* pop, int n, double* fit, int P, int NI, int k, 
                           cudaStream_t st);
 int launch_island_migrate_ragged(float* pop, const long long* offsets, double* fit, int P, int NI,
                                  int k, int* order, cudaStream_t st);
+int launch_frank_wolfe_tc(float* pop, float* gbuf, float* gbbuf, const long long* offsets,
+                          const int* order, int P, int n_fixed, int n_max, const int* skip,
+                          int rounds, int pdhg, int nT, float tMax, float tau, float sig,
+                          int precision, cudaStream_t st);
 int prepare_local_search_tc(int n_max);
+int prepare_frank_wolfe_tc(int n_max);
 int prepare_simt(int n_max, bool local_search);
 }  // namespace sidon_host
 
@@ -73,6 +78,9 @@ int check_args(const Args& a) {
   if (c.fw_every > 0 && (c.fw_rounds < 0 || c.pdhg_iters < 0 || c.fw_nT < 1 ||
                          !(c.fw_t_max > 0.f) || !(c.fw_t_max <= 1.f)))
     return SIDON_ERR_ARG;
+  if (c.fw_every > 0 && c.fw_precision != SIDON_PREC_FP32_SIMT &&
+      c.fw_precision != SIDON_PREC_BF16X1 && c.fw_precision != SIDON_PREC_BF16X3)
+    return SIDON_ERR_DTYPE;
   if (c.migrate_every > 0) {
     if (!a.rank || c.n_islands < 1 || c.k_migrate < 0 || a.P % c.n_islands) return SIDON_ERR_ARG;
     const int PI = a.P / c.n_islands;
@@ -115,9 +123,15 @@ int enqueue(const Args& a, cudaStream_t st) {
                                SIDON_F32, st);
     if (rc) return rc;
     if (c.fw_every > 0 && s1 % c.fw_every == 0 && c.fw_rounds > 0) {
-      rc = launch_frank_wolfe(a.pop, a.offsets, a.order, a.P, n_fixed, a.n_max, nullptr,
-                              c.fw_rounds, c.pdhg_iters, c.fw_nT, c.fw_t_max, c.fw_tau,
-                              c.fw_sigma, st);
+      // the Adam moments are dead between local-search launches: they are
+      // the tensor-core step's g / gbar rows
+      rc = c.fw_precision == SIDON_PREC_FP32_SIMT
+               ? launch_frank_wolfe(a.pop, a.offsets, a.order, a.P, n_fixed, a.n_max, nullptr,
+                                   c.fw_rounds, c.pdhg_iters, c.fw_nT, c.fw_t_max, c.fw_tau,
+                                   c.fw_sigma, st)
+               : launch_frank_wolfe_tc(a.pop, a.mom, a.vel, a.offsets, a.order, a.P, n_fixed,
+                                       a.n_max, nullptr, c.fw_rounds, c.pdhg_iters, c.fw_nT,
+                                       c.fw_t_max, c.fw_tau, c.fw_sigma, c.fw_precision, st);
       if (rc) return rc;
     }
     if (c.migrate_every > 0 && s1 % c.migrate_every == 0 && s1 < c.steps) {
@@ -167,6 +181,8 @@ int sidon_anneal_capture(float* pop, float* mom, float* vel, const long long* of
   const bool tc = cfg->precision != SIDON_PREC_FP32_SIMT;
   rc = prepare_simt(n_max, !tc);
   if (!rc && tc) rc = prepare_local_search_tc(n_max);
+  if (!rc && cfg->fw_every > 0 && cfg->fw_precision != SIDON_PREC_FP32_SIMT)
+    rc = prepare_frank_wolfe_tc(n_max);
   if (rc) return rc;
   sidon_graph_s* g = new (std::nothrow) sidon_graph_s;
   if (!g) return SIDON_ERR_ARG;

@@ -44,6 +44,10 @@ int launch_certify(const void* pop, int dtype, int n, int P, double* outF, doubl
 int launch_frank_wolfe(float* pop, const long long* offsets, const int* order, int P, int n_fixed,
                        int n_max, const int* skip, int rounds, int pdhg, int nT, float tMax,
                        float tau, float sig, cudaStream_t st);
+int launch_frank_wolfe_tc(float* pop, float* gbuf, float* gbbuf, const long long* offsets,
+                          const int* order, int P, int n_fixed, int n_max, const int* skip,
+                          int rounds, int pdhg, int nT, float tMax, float tau, float sig,
+                          int precision, cudaStream_t st);
 int launch_refine(const void* src, int n, int P, void* dst, int dtype, cudaStream_t st);
 int launch_coarsen(const void* src, int n2, int P, void* dst, int dtype, cudaStream_t st);
 int launch_island_migrate(float* pop, int n, double* fit, int P, int NI, int k, int* order,
@@ -278,6 +282,20 @@ int sidon_frank_wolfe(float* pop, const int* skip, int n, int P, int rounds, int
                             tau, sigma, S(stream));
 }
 
+int sidon_frank_wolfe_tc(float* pop, float* g_scratch, float* gbar_scratch, const int* skip, int n,
+                         int P, int rounds, int pdhg_iters, int nT, float t_max, float tau,
+                         float sigma, int precision, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0 || rounds <= 0) return SIDON_OK;
+  if (!pop || !g_scratch || !gbar_scratch || pdhg_iters < 0 || nT < 1 || !(t_max > 0.f) ||
+      !(t_max <= 1.f))
+    return SIDON_ERR_ARG;
+  if (precision != SIDON_PREC_BF16X1 && precision != SIDON_PREC_BF16X3) return SIDON_ERR_DTYPE;
+  return launch_frank_wolfe_tc(pop, g_scratch, gbar_scratch, nullptr, nullptr, P, n, n, skip,
+                               rounds, pdhg_iters, nT, t_max, tau, sigma, precision, S(stream));
+}
+
 int sidon_refine(const void* src, int n, int P, void* dst, int dtype, void* stream) {
   int rc = pre(n, P);
   if (rc) return rc;
@@ -361,6 +379,21 @@ int sidon_frank_wolfe_ragged(float* pop, const long long* offsets, const int* or
     return SIDON_ERR_ARG;
   return launch_frank_wolfe(pop, offsets, order, P, 0, n_max, skip, rounds, pdhg_iters, nT, t_max,
                             tau, sigma, S(stream));
+}
+
+int sidon_frank_wolfe_tc_ragged(float* pop, float* g_scratch, float* gbar_scratch,
+                                const long long* offsets, const int* order, int n_max,
+                                const int* skip, int P, int rounds, int pdhg_iters, int nT,
+                                float t_max, float tau, float sigma, int precision, void* stream) {
+  int rc = pre(n_max, P);
+  if (rc) return rc;
+  if (P == 0 || rounds <= 0) return SIDON_OK;
+  if (!pop || !g_scratch || !gbar_scratch || !offsets || pdhg_iters < 0 || nT < 1 ||
+      !(t_max > 0.f) || !(t_max <= 1.f))
+    return SIDON_ERR_ARG;
+  if (precision != SIDON_PREC_BF16X1 && precision != SIDON_PREC_BF16X3) return SIDON_ERR_DTYPE;
+  return launch_frank_wolfe_tc(pop, g_scratch, gbar_scratch, offsets, order, P, 0, n_max, skip,
+                               rounds, pdhg_iters, nT, t_max, tau, sigma, precision, S(stream));
 }
 
 int sidon_island_migrate_ragged(float* pop, const long long* offsets, double* fit, int P,

@@ -45,7 +45,10 @@ struct Layout {
     size_t o = (size_t)STAGES * STAGE_BYTES;
     off_bc = o;
     const int rows = rcc > rc ? rcc : rc;
-    o += (size_t)2 * rows * 128;           // two conv slots or one corr hi|lo pair
+    // two conv slots or one hi|lo pair; after a tile phase, gather scratch
+    // for up to 2n-1 outputs in the padded layout
+    const size_t region = (size_t)2 * rows * 128;
+    o += region > (size_t)cb_len * 4 ? region : (size_t)cb_len * 4;
     off_sa = o;
     o += (size_t)sa_len * 4;
     o = (o + 15) & ~(size_t)15;
@@ -371,6 +374,140 @@ k_lp_backward_tc(const float* __restrict__ pop, const float* __restrict__ saved,
   teardown(S);
 }
 
+// --------------------------- Frank-Wolfe / PDHG ---------------------------
+// The Chambolle-Pock Frank-Wolfe step of k_frank_wolfe (src/kernels.cuh:408-532)
+// with its convolutions and correlations on the tensor cores:
+//   lambda <- [lambda + sigma (a * gbar - M)]_+     a * gbar: CONV_X
+//   g <- [g + tau (1 - corr(lambda, a))]_+           corr:     CORR
+//   line search maxima of h * h, h = (1-t) a + t g:  CONV_SYM
+// a stays in shared memory during the iterations, lambda in the weight
+// buffer, the gather scratch in the copy region; g and gbar are plain global
+// rows (caller scratch in pop's layout) that the copies read through L2.
+// M and the line-search maxima are refined in fp64 over the near-maximal k
+// (the tensor-core b is within 3e-5 of max b), so a move is accepted only if
+// it lowers the refined maximum.
+constexpr int kFwRefineCap = 1024;
+
+__device__ __forceinline__ double refined_max_sa(const Shared& S, int n, float* X, int* list,
+                                                 int* cnt, double* red) {
+  const int nb = 2 * n - 1;
+  float mloc = 0.f;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) mloc = fmaxf(mloc, X[pidx(k)]);
+  const float approx = block_max(mloc, S.red);
+  if (!(approx > 0.f)) return 0.0;
+  return refine_max(
+      n, [&](int i) { return S.sa[pidx(i)]; }, [&](int k) { return X[pidx(k)]; }, approx, 2e-4f,
+      list, kFwRefineCap, cnt, red);
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+k_frank_wolfe_tc(float* pop, float* gbuf, float* gbbuf, const long long* __restrict__ offsets,
+                 const int* __restrict__ order, int P, int n_fixed, int n_max,
+                 const int* __restrict__ skip, int rounds, int pdhgIters, int nT, float tMax,
+                 float tau_in, float sig_in, int three, unsigned int* status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ int s_list[kFwRefineCap];
+  __shared__ int s_cnt;
+  __shared__ double s_red[32];
+  Shared S = setup(n_max, three != 0, smem_raw);
+  Ctx& C = S.C;
+  const Lane ln;
+  float* X = reinterpret_cast<float*>(C.bc);   // gather scratch (after a tile phase)
+  bool alive = true;
+  for (int slot = blockIdx.x; slot < P && alive; slot += gridDim.x) {
+    const Cand cd = cand_of(slot, offsets, order, n_fixed);
+    const int n = cd.n;
+    if (skip && skip[cd.pid]) continue;
+    if (n < 1 || n > n_max) continue;
+    float* a = pop + cd.off;
+    float* g = gbuf + cd.off;
+    float* gb = gbbuf + cd.off;
+    begin(S, n, n_max);
+    const int nb = 2 * n - 1;
+    float sl = 0.f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; S.sa[pidx(i)] = x; sl += x; }
+    const float s0 = block_sum(sl, S.red);
+    if (!(s0 > 0.f)) continue;
+    {
+      const float inv = 1.f / s0;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] *= inv;
+      __syncthreads();
+    }
+    const float tau = tau_in > 0.f ? tau_in : 0.9f / (float)n;
+    const float sig = sig_in > 0.f ? sig_in : 0.9f * (float)n;
+
+    for (int r = 0; r < rounds; ++r) {
+      prime(C, false);
+      if (!conv_tc(C, S.sa, status)) { alive = false; break; }
+      gather_conv(C, ln, X);
+      const double Mref = refined_max_sa(S, n, X, s_list, &s_cnt, s_red);
+      if (!(Mref > 0.0)) break;
+      const float M = (float)Mref;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float x = S.sa[pidx(i)];
+        g[i] = x;
+        gb[i] = x;
+        a[i] = x;                                  // the round's start, for the line search
+      }
+      for (int k = threadIdx.x; k < nb; k += blockDim.x) S.cb[pidx(k)] = 0.f;
+      __syncthreads();
+
+      for (int it = 0; it < pdhgIters; ++it) {
+        prime(C, true);
+        if (!convx_tc(C, S.sa, gb, n, status)) { alive = false; break; }
+        gather_conv(C, ln, X);
+        for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+          const float l = S.cb[pidx(k)] + sig * (X[pidx(k)] - M);
+          S.cb[pidx(k)] = l > 0.f ? l : 0.f;
+        }
+        fence_before();
+        __syncthreads();
+        if (!corr_tc(C, S.sa, S.cb, status)) { alive = false; break; }
+        gather_corr(C, ln, X);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+          const float go = g[i];
+          float gn = go + tau * (1.f - X[pidx(i)]);
+          gn = gn > 0.f ? gn : 0.f;
+          g[i] = gn;
+          gb[i] = 2.f * gn - go;
+        }
+        __syncthreads();
+      }
+      if (!alive) break;
+
+      float sg = 0.f;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) sg += g[i];
+      sg = block_sum(sg, S.red);
+      if (!(sg > 0.f)) break;
+      const float ginv = 1.f / sg;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) g[i] *= ginv;
+      __syncthreads();
+      // sum a = sum g = 1  =>  F(h) = 2n max(h*h) for every t
+      float bestT = 0.f;
+      double bestM = Mref;
+      for (int s = 1; s <= nT; ++s) {
+        const float t = tMax * (float)s / (float)nT;
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+          S.sa[pidx(i)] = (1.f - t) * __ldcg(a + i) + t * __ldcg(g + i);
+        __syncthreads();
+        prime(C, false);
+        if (!conv_tc(C, S.sa, status)) { alive = false; break; }
+        gather_conv(C, ln, X);
+        const double mm = refined_max_sa(S, n, X, s_list, &s_cnt, s_red);
+        if (mm < bestM) { bestM = mm; bestT = t; }
+      }
+      if (!alive) break;
+      for (int i = threadIdx.x; i < n; i += blockDim.x)
+        S.sa[pidx(i)] = (1.f - bestT) * __ldcg(a + i) + bestT * __ldcg(g + i);
+      __syncthreads();
+      if (!(bestT > 0.f)) break;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = S.sa[pidx(i)];
+  }
+  teardown(S);
+}
+
 }  // namespace tc
 }  // namespace sidon
 
@@ -449,6 +586,34 @@ int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* 
       (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default,
       precision == SIDON_PREC_BF16X3 ? 1 : 0, sw);
   return check_launch();
+}
+
+size_t smem_frank_wolfe_tc(int n) { return tc::Layout(n).total; }
+
+int launch_frank_wolfe_tc(float* pop, float* gbuf, float* gbbuf, const long long* offsets,
+                          const int* order, int P, int n_fixed, int n_max, const int* skip,
+                          int rounds, int pdhg, int nT, float tMax, float tau, float sig,
+                          int precision, cudaStream_t st) {
+  int rc = tc_n_ok(n_max);
+  if (rc) return rc;
+  const size_t sm = smem_frank_wolfe_tc(n_max);
+  rc = prep_tc((const void*)tc::k_frank_wolfe_tc, sm);
+  if (rc) return rc;
+  unsigned int* sw = status_word();
+  if (!sw) return SIDON_ERR_CUDA;
+  const int grid = offsets ? (P < sm_count() ? P : sm_count()) : P;
+  tc::k_frank_wolfe_tc<<<grid, tc::NTHREADS, sm, st>>>(
+      pop, gbuf, gbbuf, offsets, order, P, n_fixed, n_max, skip, rounds, pdhg, nT, tMax, tau,
+      sig, precision == SIDON_PREC_BF16X3 ? 1 : 0, sw);
+  return check_launch();
+}
+
+int prepare_frank_wolfe_tc(int n_max) {
+  int rc = tc_n_ok(n_max);
+  if (rc) return rc;
+  rc = prep_tc((const void*)tc::k_frank_wolfe_tc, smem_frank_wolfe_tc(n_max));
+  if (rc) return rc;
+  return status_word() ? SIDON_OK : SIDON_ERR_CUDA;
 }
 
 int launch_lp_forward_tc(const float* a, int n, int P, double p, float* value, float* saved,

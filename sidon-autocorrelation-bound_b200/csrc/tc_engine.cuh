@@ -38,11 +38,11 @@
 //  CM[q][i][j] = a[start + 8q + i + j] addressed with LBO = SBO = 128 B.
 //
 //  Arithmetic: x = x_hi + x_lo with x_hi = bf16(x), x_lo = bf16(x - x_hi).
-//  The convolution is symmetric (sum_{i+j=k} h_i l_j = sum_{i+j=k} l_i h_j),
+//  The autoconvolution is symmetric (sum_{i+j=k} h_i l_j = sum_{i+j=k} l_i h_j),
 //  so BF16x3 needs two products: b = A_hi B_hi + A_lo2 B_hi with the window
-//  plane A_lo2 = bf16(2 x_lo) (exact doubling); the correlation uses
-//  A_hi B_hi + A_lo B_hi + A_hi B_lo.  BF16x1 keeps A_hi B_hi.  fp32
-//  accumulation in TMEM.
+//  plane A_lo2 = bf16(2 x_lo) (exact doubling); the cross convolution a * y
+//  (B from y) and the correlation use A_hi B_hi + A_lo B_hi + A_hi B_lo.
+//  BF16x1 keeps A_hi B_hi.  fp32 accumulation in TMEM.
 //
 //  Pipeline: one MMA warp (one elected lane issues every MMA) and builder
 //  warps; a ring of STAGES window buffers and two copy slots, each guarded by
@@ -270,25 +270,38 @@ __device__ __forceinline__ void chunk_xh(int c, int& x, int& h) {
   h = (c >> 3) & 7;
 }
 
-// Convolution copy in slot `slot` (hi plane only):
-// BC[x][s] = a[64 (x - rho - ZP) + 63 - s] for block rows in [0, m).
-__device__ __forceinline__ void build_conv_copy(Ctx& C, const float* sa, int rho, int slot, int bt) {
-  unsigned char* hi = C.bc + (size_t)slot * C.rc * 128;
+// Convolution copy (hi plane at `hi`, lo plane at `lo` when want_lo):
+// BC[x][s] = y[64 (x - rho - ZP) + 63 - s] for block rows in [0, m).  y is
+// either a padded shared-memory array (ylen < 0; zero beyond its cells) or a
+// plain global row of ylen cells read through L2 (cells >= ylen read as 0;
+// the row may be written by this CTA between phases, so no read-only path).
+__device__ __forceinline__ void build_conv_copy(Ctx& C, const float* y, int ylen, int rho,
+                                                unsigned char* hi, unsigned char* lo,
+                                                bool want_lo, int bt) {
   const int chunks = C.rc * 8;
   for (int c = bt; c < chunks; c += NBUILD) {
     int x, h;
     chunk_xh(c, x, h);
     const int J = x - rho - ZP;
-    uint4 vh = make_uint4(0, 0, 0, 0), vl;
+    uint4 vh = make_uint4(0, 0, 0, 0), vl = vh;
     if (J >= 0 && J < C.m) {
       // s = 8h .. 8h+7  <->  cells 64J + 63 - 8h down to 64J + 56 - 8h
-      const float* src = sa + pidx(64 * J + 56 - 8 * h);
-      const float4 u0 = *reinterpret_cast<const float4*>(src);
-      const float4 u1 = *reinterpret_cast<const float4*>(src + 4);
-      const float v[8] = {u1.w, u1.z, u1.y, u1.x, u0.w, u0.z, u0.y, u0.x};
+      float v[8];
+      if (ylen < 0) {
+        const float* src = y + pidx(64 * J + 56 - 8 * h);
+        const float4 u0 = *reinterpret_cast<const float4*>(src);
+        const float4 u1 = *reinterpret_cast<const float4*>(src + 4);
+        v[0] = u1.w; v[1] = u1.z; v[2] = u1.y; v[3] = u1.x;
+        v[4] = u0.w; v[5] = u0.z; v[6] = u0.y; v[7] = u0.x;
+      } else {
+        const int c0 = 64 * J + 63 - 8 * h;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = (c0 - j < ylen) ? __ldcg(y + (c0 - j)) : 0.f;
+      }
       split8(v, 1.f, vh, vl);
     }
     *reinterpret_cast<uint4*>(hi + 16 * c) = vh;
+    if (want_lo) *reinterpret_cast<uint4*>(lo + 16 * c) = vl;
   }
 }
 
@@ -353,10 +366,19 @@ struct Tile {
 constexpr int COL_CONV = 0;
 __device__ __forceinline__ int col_corr(int m) { return conv_width(m); }
 
-// Issue the MMAs of one tile (one thread).  corr selects the 3-product
-// correlation arithmetic, otherwise the 2-product symmetric convolution.
+// What a tile sequence computes.
+//   CONV_SYM  b = a * a: windows and copies from the heights, 2 products
+//             (A_hi B_hi + A_lo2 B_hi), two hi-only copy slots;
+//   CONV_X    b = a * y: windows from a, copies from y (hi | lo, one slot),
+//             3 products;
+//   CORR      G = corr(c, a): windows from a, copies from the weights c
+//             (hi | lo, one slot), 3 products.
+enum TileMode { CONV_SYM = 0, CONV_X = 1, CORR = 2 };
+
+// Issue the MMAs of one tile (one thread).  three_prod selects the
+// 3-product arithmetic, otherwise the 2-product symmetric convolution.
 __device__ __forceinline__ void issue_tile(Ctx& C, int st, uint32_t b_hi, uint32_t b_lo,
-                                           const Tile& T, bool corr) {
+                                           const Tile& T, bool three_prod) {
   const uint32_t a_hi = smem_u32(C.stages + st * STAGE_BYTES);
   const uint32_t a_lo = a_hi + PLANE;
   const uint32_t bh0 = b_hi + (uint32_t)(T.x0 >> 3) * B_SBO;
@@ -371,7 +393,7 @@ __device__ __forceinline__ void issue_tile(Ctx& C, int st, uint32_t b_hi, uint32
     if (C.three) {
       const uint64_t al = sdesc(a_lo + kc * 256, 128, 128);
       mma_bf16(d, al, bh, id, 1u);
-      if (corr) {
+      if (three_prod) {
         const uint64_t bl = sdesc(bl0 + kc * 256, 128, B_SBO);
         mma_bf16(d, ah, bl, id, 1u);
       }
@@ -382,25 +404,30 @@ __device__ __forceinline__ void issue_tile(Ctx& C, int st, uint32_t b_hi, uint32
 // Run the tiles w = 0, 2, ..., dmax in residue classes w mod 8 through the
 // warp-specialised pipeline.  Ends with every MMA of the sequence complete
 // (bar_done) and the accumulator readable by all warps.
-//   corr = false: convolution, copies from the heights sa (two slots);
-//   corr = true:  correlation, copies from the padded weights cb (one slot).
-__device__ bool run_tiles(Ctx& C, const float* sa, const float* cb, bool corr,
+//   wsrc: padded shared heights (windows; the copies too for CONV_SYM);
+//   bsrc / blen: the copy source of CONV_X (see build_conv_copy) or the
+//   padded shared weights of CORR.
+template <int MODE>
+__device__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen,
                           unsigned int* status) {
+  constexpr bool corr = MODE == CORR;
+  constexpr bool three_prod = MODE != CONV_SYM;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bool want_lo = corr && C.three;
-  const float lsc = corr ? 1.f : 2.f;
+  const bool want_lo = three_prod && C.three;
+  const float lsc = MODE == CONV_SYM ? 2.f : 1.f;
   const int m = C.m;
+  const int lo_off = (corr ? C.rcc : C.rc) * 128;   // lo plane after hi (one-slot modes)
   int st = C.st_next;
   if (warp == MMA_WARP) {
     if (lane == 0) {
       fence_after();
       const int cb_cols = corr_n(m);
       for (int rho = 0; rho < 8 && rho <= C.dmax; rho += 2) {
-        const int slot = corr ? 0 : ((rho >> 1) & 1);
+        const int slot = MODE == CONV_SYM ? ((rho >> 1) & 1) : 0;
         if (!wait_phase(C, &C.bc_full[slot], (uint32_t)(C.bc_uses[slot] & 1), status)) break;
         C.bc_uses[slot] += 1;
-        const uint32_t bbase = smem_u32(C.bc) + (corr ? 0u : (uint32_t)slot * C.rc * 128u);
-        const uint32_t blo = bbase + (uint32_t)C.rcc * 128u;
+        const uint32_t bbase = smem_u32(C.bc) + (uint32_t)slot * C.rc * 128u;
+        const uint32_t blo = bbase + (uint32_t)lo_off;
         bool ok = true;
         for (int w = rho; w <= C.dmax; w += 8) {
           Tile T;
@@ -417,7 +444,7 @@ __device__ bool run_tiles(Ctx& C, const float* sa, const float* cb, bool corr,
           if (!wait_phase(C, &C.full[st], (uint32_t)(C.uses[st] & 1), status)) { ok = false; break; }
           C.uses[st] += 1;
           fence_after();
-          issue_tile(C, st, bbase, blo, T, corr);
+          issue_tile(C, st, bbase, blo, T, three_prod);
           mma_commit(&C.empty[st]);
           st = (st + 1 == STAGES) ? 0 : st + 1;
         }
@@ -430,12 +457,14 @@ __device__ bool run_tiles(Ctx& C, const float* sa, const float* cb, bool corr,
   } else {
     const int bt = threadIdx.x - (warp > MMA_WARP ? 32 : 0);   // 0 .. NBUILD-1
     for (int rho = 0; rho < 8 && rho <= C.dmax; rho += 2) {
-      const int slot = corr ? 0 : ((rho >> 1) & 1);
+      const int slot = MODE == CONV_SYM ? ((rho >> 1) & 1) : 0;
       const int u = C.bc_uses[slot];
       if (u > 0 && !wait_phase(C, &C.bc_empty[slot], (uint32_t)((u - 1) & 1), status)) break;
       C.bc_uses[slot] = u + 1;
-      if (corr) build_corr_copy(C, cb, rho, want_lo, bt);
-      else build_conv_copy(C, sa, rho, slot, bt);
+      unsigned char* hi = C.bc + (size_t)slot * C.rc * 128;
+      if (corr) build_corr_copy(C, bsrc, rho, want_lo, bt);
+      else if (MODE == CONV_X) build_conv_copy(C, bsrc, blen, rho, hi, hi + lo_off, want_lo, bt);
+      else build_conv_copy(C, wsrc, -1, rho, hi, hi, false, bt);
       fence_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&C.bc_full[slot]);
@@ -447,7 +476,7 @@ __device__ bool run_tiles(Ctx& C, const float* sa, const float* cb, bool corr,
           break;
         }
         C.uses[st] = us + 1;
-        build_window(C, st, sa, w, lsc, bt);
+        build_window(C, st, wsrc, w, lsc, bt);
         fence_async_smem();
         __syncwarp();
         if (lane == 0) mbar_arrive(&C.full[st]);
@@ -532,12 +561,17 @@ __device__ __forceinline__ void gather_corr(Ctx& C, const Lane& ln, float* Y) {
 
 // b = a * a (accumulator at COL_CONV)
 __device__ __forceinline__ bool conv_tc(Ctx& C, const float* sa, unsigned int* status) {
-  return run_tiles(C, sa, nullptr, false, status);
+  return run_tiles<CONV_SYM>(C, sa, nullptr, 0, status);
+}
+// b = a * y (accumulator at COL_CONV); y: a plain global row of ylen cells
+__device__ __forceinline__ bool convx_tc(Ctx& C, const float* sa, const float* y, int ylen,
+                                         unsigned int* status) {
+  return run_tiles<CONV_X>(C, sa, y, ylen, status);
 }
 // G = corr(c, a) (accumulator at col_corr); cb: padded weights (zero beyond 2n-1)
 __device__ __forceinline__ bool corr_tc(Ctx& C, const float* sa, const float* cb,
                                         unsigned int* status) {
-  return run_tiles(C, sa, cb, true, status);
+  return run_tiles<CORR>(C, sa, cb, 0, status);
 }
 
 }  // namespace tc

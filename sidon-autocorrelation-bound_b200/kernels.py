@@ -185,6 +185,24 @@ def run_frank_wolfe(pop: torch.Tensor, rounds: int, pdhg_iters: int, nT: int = 1
     return True
 
 
+def run_frank_wolfe_tc(pop: torch.Tensor, rounds: int, pdhg_iters: int, nT: int = 12,
+                       t_max: float = 0.30, skip: torch.Tensor | None = None, tau: float = 0.0,
+                       sigma: float = 0.0, precision: str = "bf16x3",
+                       g_scratch: torch.Tensor | None = None,
+                       gbar_scratch: torch.Tensor | None = None, stream=None) -> None:
+    """run_frank_wolfe with the Chambolle-Pock convolutions on the tensor cores."""
+    n, P = _pop_shape(pop)
+    if g_scratch is None:
+        g_scratch = torch.empty_like(pop)
+    if gbar_scratch is None:
+        gbar_scratch = torch.empty_like(pop)
+    _lib.call("sidon_frank_wolfe_tc", _dev(pop, "pop", torch.float32),
+              _dev(g_scratch, "g_scratch", torch.float32),
+              _dev(gbar_scratch, "gbar_scratch", torch.float32), _opt(skip, "skip", torch.int32),
+              n, P, int(rounds), int(pdhg_iters), int(nT), float(t_max), float(tau), float(sigma),
+              PRECISIONS[precision], _stream(stream))
+
+
 def refine(pop: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
     """n -> 2n cell split (kRefine, src/kernels.cuh:538-547)."""
     n, P = _pop_shape(pop)
@@ -329,6 +347,20 @@ def run_frank_wolfe_ragged(batch: RaggedBatch, rounds: int, pdhg_iters: int, nT:
               float(t_max), float(tau), float(sigma), _stream(stream))
 
 
+def run_frank_wolfe_tc_ragged(batch: RaggedBatch, rounds: int, pdhg_iters: int, nT: int = 12,
+                              t_max: float = 0.30, skip: torch.Tensor | None = None,
+                              tau: float = 0.0, sigma: float = 0.0, precision: str = "bf16x3",
+                              stream=None) -> None:
+    """run_frank_wolfe_tc over a ragged batch, in place."""
+    g = torch.empty_like(batch.flat)
+    gb = torch.empty_like(batch.flat)
+    _lib.call("sidon_frank_wolfe_tc_ragged", _dev(batch.flat, "pop", torch.float32),
+              g.data_ptr(), gb.data_ptr(), batch.offsets.data_ptr(), batch.order.data_ptr(),
+              batch.n_max, _opt(skip, "skip", torch.int32), batch.P, int(rounds),
+              int(pdhg_iters), int(nT), float(t_max), float(tau), float(sigma),
+              PRECISIONS[precision], _stream(stream))
+
+
 def island_migrate_ragged(batch: RaggedBatch, fit: torch.Tensor, n_islands: int, k: int = 1,
                           order: torch.Tensor | None = None, stream=None) -> torch.Tensor:
     """island_migrate over a ragged batch (migrants of another size are
@@ -347,7 +379,7 @@ def anneal_config(steps: int = 5000, p_start: float = 2.0, p_end: float = 1024.0
                   beta2: float = 0.999, precision: str = "bf16x3", fw_every: int = 250,
                   fw_rounds: int = 1, pdhg_iters: int = 200, fw_nT: int = 12,
                   fw_t_max: float = 0.30, fw_tau: float = 0.9, fw_sigma: float = 0.9,
-                  n_islands: int = 16, migrate_every: int = 500,
+                  fw_precision: str = "bf16x3", n_islands: int = 16, migrate_every: int = 500,
                   k_migrate: int = 4) -> _lib.AnnealConfig:
     """struct sidon_anneal_config; the defaults are the batched island anneal
     (5000 steps, p 2 -> 1024, Frank-Wolfe every 250 steps with 200
@@ -356,8 +388,9 @@ def anneal_config(steps: int = 5000, p_start: float = 2.0, p_end: float = 1024.0
     return _lib.AnnealConfig(int(steps), float(p_start), float(p_end), float(lr_start),
                              float(lr_end), float(beta1), float(beta2), PRECISIONS[precision],
                              int(fw_every), int(fw_rounds), int(pdhg_iters), int(fw_nT),
-                             float(fw_t_max), float(fw_tau), float(fw_sigma), int(n_islands),
-                             int(migrate_every), int(k_migrate))
+                             float(fw_t_max), float(fw_tau), float(fw_sigma),
+                             PRECISIONS[fw_precision], int(n_islands), int(migrate_every),
+                             int(k_migrate))
 
 
 def _anneal_args(batch, cfg, fit, rank, mom, vel):

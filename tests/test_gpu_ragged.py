@@ -92,6 +92,18 @@ def test_ragged_frank_wolfe_matches_uniform(cuda):
         np.testing.assert_array_equal(got[p], u.cpu().numpy()[0], err_msg=f"candidate {p}")
 
 
+def test_ragged_frank_wolfe_tc_matches_uniform(cuda):
+    sizes = [64, 300, 1000, 129, 2048]
+    rows, b = _batch(sizes, 13, cuda)
+    K().run_frank_wolfe_tc_ragged(b, 2, 20, 6, 0.3, tau=0.9, sigma=0.9)
+    got = b.rows()
+    assert _status() == 0
+    for p, r in enumerate(rows):
+        u = torch.as_tensor(r[None, :], device=cuda)
+        K().run_frank_wolfe_tc(u, 2, 20, 6, 0.3, tau=0.9, sigma=0.9)
+        np.testing.assert_array_equal(got[p], u.cpu().numpy()[0], err_msg=f"candidate {p}")
+
+
 def test_ragged_migrate_vs_oracle(cuda, orc):
     rng = np.random.default_rng(5)
     sizes = [int(x) for x in rng.choice([16, 40, 64, 100], 24)]
@@ -108,17 +120,18 @@ def test_ragged_migrate_vs_oracle(cuda, orc):
     np.testing.assert_array_equal(f.cpu().numpy(), want_fit)     # NaN == NaN here
 
 
-def _small_cfg(precision="bf16x3"):
+def _small_cfg(precision="bf16x3", fw_precision="bf16x3"):
     return K().anneal_config(steps=60, p_start=2.0, p_end=64.0, precision=precision,
-                             fw_every=20, pdhg_iters=10, fw_nT=4, n_islands=3,
-                             migrate_every=30, k_migrate=1)
+                             fw_every=20, pdhg_iters=10, fw_nT=4, fw_precision=fw_precision,
+                             n_islands=3, migrate_every=30, k_migrate=1)
 
 
-def test_anneal_matches_manual_schedule(cuda):
+@pytest.mark.parametrize("fw_precision", ["bf16x3", "fp32"])
+def test_anneal_matches_manual_schedule(cuda, fw_precision):
     sizes = [64, 300, 129, 1000, 64, 512]
     _, b1 = _batch(sizes, 21, cuda)
     _, b2 = _batch(sizes, 21, cuda)
-    cfg = _small_cfg()
+    cfg = _small_cfg(fw_precision=fw_precision)
     fit = K().anneal(b1, cfg)
     # the same schedule by hand: cuts at 20, 30, 40, 60
     steps, pS, pE, lr = 60, 2.0, 64.0, 1e-3
@@ -129,7 +142,10 @@ def test_anneal_matches_manual_schedule(cuda):
     for s0, s1 in [(0, 20), (20, 30), (30, 40), (40, 60)]:
         K().run_local_search_ragged(b2, s1 - s0, sch(s0), sch(s1 - 1), lr, lr)
         if s1 % 20 == 0:
-            K().run_frank_wolfe_ragged(b2, 1, 10, 4, 0.3, tau=0.9, sigma=0.9)
+            if fw_precision == "fp32":
+                K().run_frank_wolfe_ragged(b2, 1, 10, 4, 0.3, tau=0.9, sigma=0.9)
+            else:
+                K().run_frank_wolfe_tc_ragged(b2, 1, 10, 4, 0.3, tau=0.9, sigma=0.9)
         if s1 % 30 == 0 and s1 < steps:
             f2, _ = K().run_eval_ragged(b2, with_nactive=False)
             K().island_migrate_ragged(b2, f2, 3, 1)
