@@ -90,6 +90,7 @@ SIDON_API double sidon_hostF(const double* a, int n);
  * as in hostF: each product rounded, then added in i order; S summed in i
  * order -- so F equals hostF bit for bit) and, if out_nactive != NULL, the
  * number of k with b_k >= M (1 - active_tol).  F = 1e30 when S <= 0.
+ * Any n: beyond shared memory the heights are streamed through it.
  * pop: device [P][n] of dtype; out_F: device [P]; out_nactive: device [P].
  * Replaces kEval<T,double> + runEval (src/kernels.cuh:301-377,
  * src/main.cu:161-166). */
@@ -207,6 +208,42 @@ SIDON_API int sidon_coarsen(const void* src, int n2, int P, void* dst, int dtype
  * Replaces the host ranking and D2D migration (src/main.cu:676-692). */
 SIDON_API int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, int k_migrate,
                          int* order_out, void* stream);
+
+/* ---------------------------- large candidates -----------------------------
+ * Candidates longer than one CTA's shared memory (the ladder's 16384,
+ * 32768, 65536, ...): the heights are cut into super-blocks of q cells (a
+ * multiple of 64 that the single-CTA tensor-core kernels accept; q <= 0
+ * picks 8192 or the largest accepted size below it) and every pair of
+ * super-blocks is one tensor-core job; stream-ordered elementwise launches
+ * combine the jobs' outputs in a fixed order.  Works for any n >= 1 (for
+ * n <= q it is one job per product).  precision BF16X3 or BF16X1.  The
+ * caller provides the workspace (sidon_large_workspace_bytes; no
+ * allocation inside).  No reference counterpart: the reference refuses n
+ * whose working set exceeds shared memory (src/main.cu:391-399). */
+SIDON_API size_t sidon_large_workspace_bytes(int n, int P, int q);
+
+/* sidon_local_search (fp32 [P][n], Adam moments in mom/vel) for any n. */
+SIDON_API int sidon_local_search_large(float* pop, float* mom, float* vel, const int* skip,
+                                       const int* mode_arr, int n, int P, int iters,
+                                       double p_start, double p_end, double lr_start,
+                                       double lr_end, double beta1, double beta2,
+                                       int mode_default, int precision, int q, void* workspace,
+                                       size_t workspace_bytes, void* stream);
+
+/* sidon_frank_wolfe_tc for any n (moves accepted on fp64-refined maxima). */
+SIDON_API int sidon_frank_wolfe_large(float* pop, const int* skip, int n, int P, int rounds,
+                                      int pdhg_iters, int nT, float t_max, float tau,
+                                      float sigma, int precision, int q, void* workspace,
+                                      size_t workspace_bytes, void* stream);
+
+/* sidon_certify for any n: a streamed fp64 pass finds the near-maximal k,
+ * which are then summed exactly; more than 4096 near-maximal k gives
+ * F = NaN.  workspace: sidon_certify_workspace_bytes(P) bytes.  (sidon_eval
+ * itself streams automatically when n exceeds shared memory.) */
+SIDON_API size_t sidon_certify_workspace_bytes(int P);
+SIDON_API int sidon_certify_large(const void* pop, int dtype, int n, int P, double* out_F,
+                                  double* out_M, double* out_S, int* out_kmax, void* workspace,
+                                  void* stream);
 
 /* ---------------------------- ragged batches ------------------------------
  * A ragged batch holds P candidates of different sizes back to back:

@@ -49,6 +49,20 @@ int launch_frank_wolfe_tc(float* pop, float* gbuf, float* gbbuf, const long long
                           int rounds, int pdhg, int nT, float tMax, float tau, float sig,
                           int precision, cudaStream_t st);
 int launch_refine(const void* src, int n, int P, void* dst, int dtype, cudaStream_t st);
+int launch_eval_stream(const void* pop, int dtype, int n, int P, double* outF, int* outN,
+                       double tol, cudaStream_t st);
+size_t certify_workspace_bytes(int P);
+int launch_certify_large(const void* pop, int dtype, int n, int P, double* outF, double* outM,
+                         double* outS, int* outK, void* ws, cudaStream_t st);
+size_t big_workspace_bytes(int n, int P, int Q);
+int big_default_q(int n);
+int launch_local_search_big(float* pop, float* mom, float* vel, const int* skip,
+                            const int* mode_arr, int n, int P, int iters, double pS, double pE,
+                            double lrS, double lrE, double b1, double b2, int mode_default,
+                            int precision, int Q, void* ws, size_t ws_bytes, cudaStream_t st);
+int launch_frank_wolfe_big(float* pop, const int* skip, int n, int P, int rounds, int pdhg,
+                           int nT, float tMax, float tau, float sig, int precision, int Q,
+                           void* ws, size_t ws_bytes, cudaStream_t st);
 int launch_coarsen(const void* src, int n2, int P, void* dst, int dtype, cudaStream_t st);
 int launch_island_migrate(float* pop, int n, double* fit, int P, int NI, int k, int* order,
                           cudaStream_t st);
@@ -204,6 +218,8 @@ int sidon_eval(const void* pop, int dtype, int n, int P, double* out_F, int* out
   if (P == 0) return SIDON_OK;
   if (!pop || !out_F) return SIDON_ERR_ARG;
   if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
+  if ((long long)smem_eval(n) > (long long)smem_optin())
+    return launch_eval_stream(pop, dtype, n, P, out_F, out_nactive, active_tol, S(stream));
   return launch_eval(pop, dtype, nullptr, nullptr, P, n, n, out_F, out_nactive, active_tol,
                      S(stream));
 }
@@ -325,6 +341,53 @@ int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, i
   const int PI = P / n_islands;
   if (PI > 1024 || 2 * k_migrate > PI) return SIDON_ERR_ARG;
   return launch_island_migrate(pop, n, fit, P, n_islands, k_migrate, order_out, S(stream));
+}
+
+size_t sidon_large_workspace_bytes(int n, int P, int q) {
+  if (q <= 0) q = big_default_q(n);
+  return big_workspace_bytes(n, P, q);
+}
+
+int sidon_local_search_large(float* pop, float* mom, float* vel, const int* skip,
+                             const int* mode_arr, int n, int P, int iters, double p_start,
+                             double p_end, double lr_start, double lr_end, double beta1,
+                             double beta2, int mode_default, int precision, int q,
+                             void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0 || iters <= 0) return SIDON_OK;
+  if (!pop || !mom || !vel) return SIDON_ERR_ARG;
+  if (!(p_start > 0.0) || !(p_end > 0.0) || !(lr_start > 0.0) || !(lr_end > 0.0))
+    return SIDON_ERR_ARG;
+  if (precision != SIDON_PREC_BF16X1 && precision != SIDON_PREC_BF16X3) return SIDON_ERR_DTYPE;
+  return launch_local_search_big(pop, mom, vel, skip, mode_arr, n, P, iters, p_start, p_end,
+                                 lr_start, lr_end, beta1, beta2, mode_default, precision, q,
+                                 workspace, workspace_bytes, S(stream));
+}
+
+int sidon_frank_wolfe_large(float* pop, const int* skip, int n, int P, int rounds, int pdhg_iters,
+                            int nT, float t_max, float tau, float sigma, int precision, int q,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0 || rounds <= 0) return SIDON_OK;
+  if (!pop || pdhg_iters < 0 || nT < 1 || !(t_max > 0.f) || !(t_max <= 1.f)) return SIDON_ERR_ARG;
+  if (precision != SIDON_PREC_BF16X1 && precision != SIDON_PREC_BF16X3) return SIDON_ERR_DTYPE;
+  return launch_frank_wolfe_big(pop, skip, n, P, rounds, pdhg_iters, nT, t_max, tau, sigma,
+                                precision, q, workspace, workspace_bytes, S(stream));
+}
+
+size_t sidon_certify_workspace_bytes(int P) { return P < 0 ? 0 : certify_workspace_bytes(P); }
+
+int sidon_certify_large(const void* pop, int dtype, int n, int P, double* out_F, double* out_M,
+                        double* out_S, int* out_kmax, void* workspace, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!pop || !out_F || !workspace) return SIDON_ERR_ARG;
+  if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
+  return launch_certify_large(pop, dtype, n, P, out_F, out_M, out_S, out_kmax, workspace,
+                              S(stream));
 }
 
 int sidon_ragged_order(const long long* offsets, int P, int* order_out, void* stream) {

@@ -225,6 +225,100 @@ k_certify(const Tin* __restrict__ pop, int n, double* __restrict__ outF, double*
   }
 }
 
+// The same certification for a candidate of any n, from the near-maximal k
+// found by the streamed fp64 pass (list[p][0 .. count[p])): the heights are
+// read from global memory.  More than `cap` near-maximal k: F = NaN (the
+// streamed pass would have to certify every k).
+template <typename Tin>
+__global__ void __launch_bounds__(512, 1)
+k_certify_list(const Tin* __restrict__ pop, int n, const int* __restrict__ list,
+               const int* __restrict__ count, int cap, double* __restrict__ outF,
+               double* __restrict__ outM, double* __restrict__ outS, int* __restrict__ outK) {
+  __shared__ int sEmin, sEmax;
+  __shared__ unsigned long long sBest;
+  __shared__ int sBestK;
+  __shared__ double sSexact;
+  const int pid = blockIdx.x;
+  const Tin* a = pop + (size_t)pid * n;
+  const int ncand = count[pid];
+  if (ncand > cap || ncand < 1) {
+    if (threadIdx.x == 0) outF[pid] = __longlong_as_double(0x7ff8000000000000ll);
+    return;
+  }
+  const int* cand = list + (size_t)pid * cap;
+  if (threadIdx.x == 0) { sEmin = 1 << 20; sEmax = -(1 << 20); sBest = 0ull; sBestK = 0x7fffffff; }
+  __syncthreads();
+  int emin = 1 << 20, emax = -(1 << 20);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double x = (double)a[i];
+    if (x != 0.0) {
+      const int ex = (int)((__double_as_longlong(x) >> 52) & 0x7ff);
+      const int e = (ex == 0 ? 1 : ex) - 1075;
+      emin = min(emin, e);
+      emax = max(emax, e + 53);
+    }
+  }
+  atomicMin(&sEmin, emin);
+  atomicMax(&sEmax, emax);
+  __syncthreads();
+  XWin w;
+  w.lo = 2 * sEmin - 64;
+  w.limbs = (2 * sEmax + 40 - w.lo) / 32 + 3;
+  if (sEmin > sEmax) w.limbs = 3;
+  if (w.limbs > kMaxLimbs) {
+    if (threadIdx.x == 0) outF[pid] = __longlong_as_double(0x7ff8000000000000ll);
+    return;
+  }
+  long long acc[kMaxLimbs];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, NW = blockDim.x >> 5;
+  for (int sweep = 0; sweep < 2; ++sweep) {
+    const double Mx = __longlong_as_double((long long)sBest);
+    for (int c = wid; c < ncand; c += NW) {
+      const int k = cand[c];
+      for (int j = 0; j < w.limbs; ++j) acc[j] = 0;
+      const int ilo = max(0, k - (n - 1)), ihi = min(k, n - 1);
+      for (int i = ilo + lane; i <= ihi; i += 32) {
+        const double x = (double)a[i], y = (double)a[k - i];
+        if (x == 0.0 || y == 0.0) continue;
+        const double pr = x * y;
+        const double e = fma(x, y, -pr);
+        xadd(acc, w, pr, false);
+        if (e > 0.0) xadd(acc, w, e, false);
+        else if (e < 0.0) xadd(acc, w, -e, true);
+      }
+      const double bk = xreduce_round(acc, w);
+      if (lane == 0) {
+        if (sweep == 0) atomicMax(&sBest, (unsigned long long)__double_as_longlong(bk));
+        else if (bk == Mx) atomicMin(&sBestK, k);
+      }
+    }
+    __syncthreads();
+  }
+  if (wid == 0) {
+    XWin ws;
+    ws.lo = sEmin - 8;
+    ws.limbs = (sEmax + 40 - ws.lo) / 32 + 3;
+    if (sEmin > sEmax) ws.limbs = 3;
+    if (ws.limbs > kMaxLimbs) ws.limbs = kMaxLimbs;
+    for (int j = 0; j < ws.limbs; ++j) acc[j] = 0;
+    for (int i = lane; i < n; i += 32) {
+      const double x = (double)a[i];
+      if (x > 0.0) xadd(acc, ws, x, false);
+    }
+    const double S = xreduce_round(acc, ws);
+    if (lane == 0) sSexact = S;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double S = sSexact;
+    const double Mx = __longlong_as_double((long long)sBest);
+    outF[pid] = (S > 0.0) ? (2.0 * (double)n * Mx / (S * S)) : 1e30;
+    if (outM) outM[pid] = Mx;
+    if (outS) outS[pid] = S;
+    if (outK) outK[pid] = (sBestK == 0x7fffffff) ? 0 : sBestK;
+  }
+}
+
 }  // namespace sidon
 
 namespace sidon_host {
@@ -232,6 +326,32 @@ using namespace sidon;
 
 size_t smem_certify(int n) {
   return sizeof(double) * ((size_t)n + 2 * margin<kCertTK>() + 32) + sizeof(int) * kMaxCand;
+}
+
+int launch_eval_stream_list(const void* pop, int dtype, int n, int P, double* mbits, int* list,
+                            int* list_count, int cap, cudaStream_t st);
+
+// near-maximal k per candidate kept by the large-n certification
+constexpr int kListCap = 4096;
+size_t certify_workspace_bytes(int P) {
+  return (size_t)P * (kListCap + 1) * sizeof(int) + (size_t)P * sizeof(double);
+}
+
+// any n: streamed fp64 pass for the near-maximal k, then the exact sums
+int launch_certify_large(const void* pop, int dtype, int n, int P, double* outF, double* outM,
+                         double* outS, int* outK, void* ws, cudaStream_t st) {
+  double* mbits = reinterpret_cast<double*>(ws);
+  int* cnt = reinterpret_cast<int*>(mbits + P);
+  int* list = cnt + P;
+  int rc = launch_eval_stream_list(pop, dtype, n, P, mbits, list, cnt, kListCap, st);
+  if (rc) return rc;
+  if (dtype == SIDON_F32)
+    k_certify_list<float><<<P, 512, 0, st>>>((const float*)pop, n, list, cnt, kListCap, outF,
+                                              outM, outS, outK);
+  else
+    k_certify_list<double><<<P, 512, 0, st>>>((const double*)pop, n, list, cnt, kListCap, outF,
+                                               outM, outS, outK);
+  return check_launch();
 }
 
 int launch_certify(const void* pop, int dtype, int n, int P, double* outF, double* outM,

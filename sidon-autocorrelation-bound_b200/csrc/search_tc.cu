@@ -6,152 +6,24 @@
 //    k_lp_forward_tc    G_p(a) and {M, S, R}, optionally b
 //    k_lp_backward_tc   dG_p/da with b recomputed on the tensor cores
 //
-//  One CTA (8 warps) per candidate, one CTA per SM (the shared-memory
-//  working set is ~24 n bytes), 512 TMEM columns: the convolution
-//  accumulator at column 0, the correlation accumulator after it.  The
-//  elementwise work (max, weights, Adam) runs on all 8 warps; the weights
-//  beyond 2n-1 stay zero for the whole launch (the correlation copies read
-//  whole blocks).
+//    k_frank_wolfe_tc   Chambolle-Pock Frank-Wolfe (src/kernels.cuh:408-532)
 //
-//  Shared memory (see Layout):
-//    stages  STAGES x 6 KB   Hankel windows (hi | lo planes)
-//    bc      B-matrix copies: two conv slots (hi) or one corr hi|lo pair
-//    sa      fp32 heights, padded block layout (cell i at i + 4 floor(i/64)),
-//            zero margins on both sides
-//    cb      fp32 padded scratch: b, then the weights c, then G
-//    red     64 floats of reduction scratch, mbarriers, TMEM address, abort flag
+//  One CTA (8 warps) per candidate, one CTA per SM (the shared-memory
+//  working set is ~24 n bytes, tc_cta.cuh), 512 TMEM columns: the
+//  convolution accumulator at column 0, the correlation accumulator after
+//  it.  The elementwise work (max, weights, Adam) runs on all 8 warps; the
+//  weights beyond 2n-1 stay zero for the whole launch (the correlation
+//  copies read whole blocks).
 // ---------------------------------------------------------------------------
 #include <mutex>
 
 #include "conv_simt.cuh"
-
-#include "tc_engine.cuh"
+#include "tc_cta.cuh"
 
 namespace sidon {
 namespace tc {
 
 __device__ unsigned int g_status_word = 0u;   // SIDON_ERR_TIMEOUT after a timed-out wait
-
-// dynamic shared memory plan (byte offsets from a 1 KB aligned base)
-struct Layout {
-  int m, rc, rcc, sa_len, cb_len;
-  size_t off_bc, off_sa, off_cb, off_red, total;
-  __host__ __device__ Layout(int n) {
-    m = (n + BL - 1) / BL;
-    rc = conv_copy_rows(m);
-    rcc = corr_copy_rows(m);
-    sa_len = 68 * (m + 8);                 // padded heights, 136 cells of margin in front
-    cb_len = 68 * (2 * m + 2);             // padded weights / gather scratch
-    size_t o = (size_t)STAGES * STAGE_BYTES;
-    off_bc = o;
-    const int rows = rcc > rc ? rcc : rc;
-    // two conv slots or one hi|lo pair; after a tile phase, gather scratch
-    // for up to 2n-1 outputs in the padded layout
-    const size_t region = (size_t)2 * rows * 128;
-    o += region > (size_t)cb_len * 4 ? region : (size_t)cb_len * 4;
-    off_sa = o;
-    o += (size_t)sa_len * 4;
-    o = (o + 15) & ~(size_t)15;
-    off_cb = o;
-    o += (size_t)cb_len * 4;
-    o = (o + 15) & ~(size_t)15;
-    off_red = o;
-    o += 64 * 4 + (2 * STAGES + 5) * 8 + 16;
-    total = o + 1024;                      // slack for aligning the dynamic base to 1 KB
-  }
-};
-
-struct Shared {
-  Ctx C;
-  float* sa;     // padded heights, logical cell 0
-  float* cb;     // padded weights / gather scratch, logical index 0
-  float* red;
-};
-
-// Per-CTA set-up for candidates of up to n_max cells: buffer addresses,
-// barriers, TMEM.  begin() then prepares one candidate.
-__device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* raw) {
-  const Layout Lo(n_max);
-  unsigned char* base = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
-  Shared S;
-  S.C.stages = base;
-  S.C.bc = base + Lo.off_bc;
-  S.sa = reinterpret_cast<float*>(base + Lo.off_sa) + 136;
-  S.cb = reinterpret_cast<float*>(base + Lo.off_cb);
-  S.red = reinterpret_cast<float*>(base + Lo.off_red);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(S.red + 64);
-  S.C.full = bars;
-  S.C.empty = bars + STAGES;
-  S.C.bc_full = bars + 2 * STAGES;
-  S.C.bc_empty = bars + 2 * STAGES + 2;
-  S.C.bar_done = bars + 2 * STAGES + 4;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
-  S.C.abort = reinterpret_cast<int*>(tslot + 1);
-  S.C.m = Lo.m;
-  S.C.rc = Lo.rc;
-  S.C.rcc = Lo.rcc;
-  S.C.n = n_max;
-  S.C.dmax = last_tile(n_max);
-  S.C.three = three;
-  S.C.done_use = 0;
-  S.C.st_next = 0;
-  S.C.bc_uses[0] = S.C.bc_uses[1] = 0;
-#pragma unroll
-  for (int s = 0; s < STAGES; ++s) S.C.uses[s] = 0;
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&S.C.full[s], NBUILD_WARPS);
-      mbar_init(&S.C.empty[s], 1);
-    }
-    for (int s = 0; s < 2; ++s) {
-      mbar_init(&S.C.bc_full[s], NBUILD_WARPS);
-      mbar_init(&S.C.bc_empty[s], 1);
-    }
-    mbar_init(S.C.bar_done, 1);
-    mbar_fence_init();
-    *S.C.abort = 0;
-  }
-  if ((threadIdx.x >> 5) == 0) tmem_alloc(tslot, 512);
-  fence_before();
-  __syncthreads();
-  fence_after();
-  S.C.tmem = *tslot;
-  return S;
-}
-
-// Prepare the CTA for a candidate of n cells (n <= n_max of setup): zero the
-// height and scratch buffers (their margins must read as zero) and set the
-// geometry.  Ends synchronised.
-__device__ __forceinline__ void begin(Shared& S, int n, int n_max) {
-  const Layout Lo(n_max), Ln(n);
-  float* z0 = S.sa - 136;
-  __syncthreads();
-  for (int i = threadIdx.x; i < Lo.sa_len; i += blockDim.x) z0[i] = 0.f;
-  for (int i = threadIdx.x; i < Lo.cb_len; i += blockDim.x) S.cb[i] = 0.f;
-  S.C.n = n;
-  S.C.m = Ln.m;
-  S.C.rc = Ln.rc;
-  S.C.rcc = Ln.rcc;
-  S.C.dmax = last_tile(n);
-  __syncthreads();
-}
-
-__device__ __forceinline__ void teardown(Shared& S) {
-  fence_before();
-  __syncthreads();
-  if ((threadIdx.x >> 5) == 0) {
-    fence_after();
-    tmem_dealloc(S.C.tmem, 512);
-  }
-}
-
-// zero both accumulators and hand the tensor memory to the MMA warp
-__device__ __forceinline__ void prime(Ctx& C, bool corr_too) {
-  zero_acc(C, COL_CONV, conv_width(C.m));
-  if (corr_too) zero_acc(C, col_corr(C.m), corr_width(C.m));
-  fence_before();
-  __syncthreads();
-}
 
 // ------------------------------ local search ------------------------------
 // Candidates: uniform rows of n_fixed cells (offsets == NULL) or a ragged
@@ -532,6 +404,8 @@ static unsigned int* status_word() {
   return addr[dev];
 }
 
+unsigned int* tc_status_word() { return status_word(); }
+
 int device_status(int reset) {
   unsigned int v = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&v, tc::g_status_word, sizeof(v));
@@ -554,6 +428,7 @@ static int tc_n_ok(int n) {
 }
 
 static int prep_tc(const void* fn, size_t sm) { return set_dyn_smem(fn, sm); }
+int tc_n_ok_public(int n) { return tc_n_ok(n); }
 
 // Everything a local-search launch at n_max sets up on the host side (the
 // shared-memory attribute, the status word's address), done ahead of a

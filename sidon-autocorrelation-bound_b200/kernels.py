@@ -261,6 +261,68 @@ def island_migrate(pop: torch.Tensor, fit: torch.Tensor, n_islands: int, k: int 
     return order
 
 
+# ----------------------------- large candidates ----------------------------
+def large_workspace(n: int, P: int, q: int = 0, device="cuda") -> torch.Tensor:
+    """Workspace for run_local_search_large / run_frank_wolfe_large."""
+    nbytes = _lib.load().sidon_large_workspace_bytes(int(n), int(P), int(q))
+    if nbytes == 0:
+        raise ValueError("bad large-candidate geometry")
+    return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+
+def run_local_search_large(pop: torch.Tensor, iters: int, p_start: float, p_end: float,
+                           lr_start: float, lr_end: float, precision: str = "bf16x3",
+                           q: int = 0, workspace: torch.Tensor | None = None,
+                           mode_arr: torch.Tensor | None = None,
+                           skip: torch.Tensor | None = None, mom: torch.Tensor | None = None,
+                           vel: torch.Tensor | None = None, beta1: float = 0.9,
+                           beta2: float = 0.999, mode_default: int = 0, stream=None) -> None:
+    """run_local_search for candidates of any n (super-block tensor-core jobs)."""
+    n, P = _pop_shape(pop)
+    if workspace is None:
+        workspace = large_workspace(n, P, q, pop.device)
+    if mom is None:
+        mom = torch.empty_like(pop)
+    if vel is None:
+        vel = torch.empty_like(pop)
+    _lib.call("sidon_local_search_large", _dev(pop, "pop", torch.float32),
+              _dev(mom, "mom", torch.float32), _dev(vel, "vel", torch.float32),
+              _opt(skip, "skip", torch.int32), _opt(mode_arr, "mode_arr", torch.int32), n, P,
+              int(iters), float(p_start), float(p_end), float(lr_start), float(lr_end),
+              float(beta1), float(beta2), int(mode_default), PRECISIONS[precision], int(q),
+              workspace.data_ptr(), workspace.numel(), _stream(stream))
+
+
+def run_frank_wolfe_large(pop: torch.Tensor, rounds: int, pdhg_iters: int, nT: int = 12,
+                          t_max: float = 0.30, skip: torch.Tensor | None = None,
+                          tau: float = 0.0, sigma: float = 0.0, precision: str = "bf16x3",
+                          q: int = 0, workspace: torch.Tensor | None = None,
+                          stream=None) -> None:
+    """run_frank_wolfe_tc for candidates of any n."""
+    n, P = _pop_shape(pop)
+    if workspace is None:
+        workspace = large_workspace(n, P, q, pop.device)
+    _lib.call("sidon_frank_wolfe_large", _dev(pop, "pop", torch.float32),
+              _opt(skip, "skip", torch.int32), n, P, int(rounds), int(pdhg_iters), int(nT),
+              float(t_max), float(tau), float(sigma), PRECISIONS[precision], int(q),
+              workspace.data_ptr(), workspace.numel(), _stream(stream))
+
+
+def certify_large(pop: torch.Tensor, stream=None):
+    """certify for candidates of any n: (F, M, S, kmax)."""
+    n, P = _pop_shape(pop)
+    code = _dtype_code(pop)
+    dev = pop.device
+    ws = torch.empty(_lib.load().sidon_certify_workspace_bytes(P), dtype=torch.uint8, device=dev)
+    F = torch.empty(P, dtype=torch.float64, device=dev)
+    M = torch.empty(P, dtype=torch.float64, device=dev)
+    S = torch.empty(P, dtype=torch.float64, device=dev)
+    K = torch.empty(P, dtype=torch.int32, device=dev)
+    _lib.call("sidon_certify_large", _dev(pop, "pop"), code, n, P, F.data_ptr(), M.data_ptr(),
+              S.data_ptr(), K.data_ptr(), ws.data_ptr(), _stream(stream))
+    return F, M, S, K
+
+
 # ------------------------------ ragged batches ------------------------------
 class RaggedBatch:
     """P candidates of different sizes back to back in one fp32 tensor:

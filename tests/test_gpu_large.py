@@ -1,0 +1,146 @@
+"""Candidates beyond one CTA: the super-block tensor-core local search and
+Frank-Wolfe, the streamed fp64 evaluation and the list-based exact
+certification.  Needs a B200.
+
+Bars: the streamed evaluation equals hostF bit for bit at any n; the
+certified F is within 1e-12 of hostF and bit-identical across a cell split;
+the super-block search (which sums b and G over super-blocks in another
+order than the single-CTA kernel) tracks the single-CTA BF16x3 search and
+the fp32 oracle to the BF16x3 tolerance.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def K():
+    from sidon_b200 import kernels
+    return kernels
+
+
+def T(x, dev, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype, device=dev)
+
+
+def _status():
+    import sidon_b200
+    return sidon_b200.load().sidon_device_status(1)
+
+
+@pytest.mark.parametrize("n,q", [(1000, 256), (1000, 1024), (2048, 512), (777, 192)])
+def test_large_search_tracks_single_cta(cuda, n, q):
+    from sidon_b200 import synth
+    pop = synth.population("structured", n, 3, seed=50 + n)
+    a = T(pop, cuda)
+    b = T(pop, cuda)
+    K().run_local_search_large(a, 20, 2.0, 64.0, 1e-3, 1e-3, q=q)
+    K().run_local_search(b, 20, 2.0, 64.0, 1e-3, 1e-3, precision="bf16x3")
+    assert _status() == 0
+    A, B = a.cpu().numpy(), b.cpu().numpy()
+    assert (A >= 0).all()
+    for p in range(3):
+        Fa = K().host_f(A[p].astype(np.float64))
+        Fb = K().host_f(B[p].astype(np.float64))
+        assert abs(Fa - Fb) <= 1e-4 * Fb, (p, Fa, Fb)
+        assert abs(A[p].astype(np.float64).sum() - 1.0) < 1e-5
+
+
+def test_large_search_tracks_oracle(cuda, orc):
+    from sidon_b200 import synth
+    n = 1536
+    pop = synth.population("structured", n, 2, seed=61)
+    a = T(pop, cuda)
+    K().run_local_search_large(a, 15, 2.0, 32.0, 1e-3, 1e-3, q=512)
+    want = orc.local_search(pop, 15, 2.0, 32.0, 1e-3, 1e-3)
+    got = a.cpu().numpy()
+    for p in range(2):
+        Fg = orc.host_f(got[p].astype(np.float64))
+        Fw = orc.host_f(want[p].astype(np.float64))
+        assert abs(Fg - Fw) <= 1e-4 * Fw, (p, Fg, Fw)
+
+
+def test_large_search_skip_mode_and_zero(cuda):
+    from sidon_b200 import synth
+    n = 700
+    pop = synth.population("structured", n, 4, seed=63)
+    pop[2] = 0.0                                   # M <= 0: stops at once, untouched
+    a = T(pop, cuda)
+    skip = torch.tensor([0, 1, 0, 0], dtype=torch.int32, device=cuda)
+    mode = torch.tensor([0, 0, 0, 1], dtype=torch.int32, device=cuda)
+    K().run_local_search_large(a, 10, 2.0, 16.0, 1e-3, 1e-3, q=256, skip=skip, mode_arr=mode)
+    got = a.cpu().numpy()
+    np.testing.assert_array_equal(got[1], pop[1])
+    np.testing.assert_array_equal(got[2], pop[2])
+    b = T(pop[3:4], cuda)
+    K().run_local_search(b, 10, 2.0, 16.0, 1e-3, 1e-3, precision="bf16x3", mode_default=1)
+    Fa = K().host_f(got[3].astype(np.float64))
+    Fb = K().host_f(b.cpu().numpy()[0].astype(np.float64))
+    assert abs(Fa - Fb) <= 1e-4 * Fb
+
+
+def test_large_search_at_65536(cuda):
+    """B = 2 at n = 65536 (eight 8192-cell super-blocks): F decreases, the
+    heights stay non-negative with sum 1, the status word stays clean."""
+    from sidon_b200 import synth
+    n = 65536
+    pop = synth.population("structured", n, 2, seed=65)
+    a = T(pop, cuda)
+    F0, _ = K().run_eval(a, with_nactive=False)
+    K().run_local_search_large(a, 4, 2.0, 8.0, 1e-3, 1e-3)
+    F1, _ = K().run_eval(a, with_nactive=False)
+    assert _status() == 0
+    assert bool((a >= 0).all())
+    assert torch.allclose(a.double().sum(1), torch.ones(2, dtype=torch.float64, device=cuda),
+                          atol=1e-5)
+    assert bool((F1 < F0).all()), (F0, F1)
+
+
+@pytest.mark.parametrize("n", [30000, 40000])
+def test_streamed_eval_equals_hostF(cuda, n):
+    from sidon_b200 import synth
+    pop = synth.population("structured", n, 2, seed=n)
+    for dt in (torch.float32, torch.float64):
+        F, N = K().run_eval(T(pop, cuda, dt))
+        for p in range(2):
+            assert F[p].item() == K().host_f(pop[p].astype(np.float64)), (n, dt, p)
+        assert (N.cpu().numpy() >= 1).all()
+
+
+def test_certify_large_split_invariant(cuda):
+    from sidon_b200 import synth
+    n = 20000
+    pop = synth.population("structured", n, 2, seed=71)
+    x = T(pop, cuda)
+    F, M, S, Kx = K().certify_large(x)
+    for p in range(2):
+        h = K().host_f(pop[p].astype(np.float64))
+        assert abs(F[p].item() - h) <= 1e-12 * h
+    F2, M2, S2, _ = K().certify_large(K().refine(x))
+    assert torch.equal(F, F2)
+    assert torch.equal(2 * M, M2) and torch.equal(2 * S, S2)
+    # the shared-memory certification at a size both paths take
+    y = T(synth.population("structured", 4096, 2, seed=72), cuda)
+    Fa = K().certify(y)[0]
+    Fb = K().certify_large(y)[0]
+    assert torch.equal(Fa, Fb)
+
+
+def test_large_frank_wolfe_tracks_single_cta(cuda):
+    from sidon_b200 import synth
+    n = 2048
+    pop = synth.population("structured", n, 3, seed=81)
+    a = T(pop, cuda)
+    b = T(pop, cuda)
+    K().run_frank_wolfe_large(a, 1, 60, 6, 0.3, tau=0.9, sigma=0.9, q=512)
+    K().run_frank_wolfe_tc(b, 1, 60, 6, 0.3, tau=0.9, sigma=0.9)
+    assert _status() == 0
+    A, B = a.cpu().numpy(), b.cpu().numpy()
+    assert (A >= 0).all()
+    for p in range(3):
+        F0 = K().host_f(pop[p].astype(np.float64))
+        Fa = K().host_f(A[p].astype(np.float64))
+        Fb = K().host_f(B[p].astype(np.float64))
+        assert Fa <= F0 * (1 + 1e-9)
+        assert abs(Fa - Fb) <= 2e-3 * Fb, (p, Fa, Fb)
