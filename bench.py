@@ -441,6 +441,111 @@ def islands_arm(args) -> None:
         print(json.dumps(line))
 
 
+# --------------------------------- large ladder -----------------------------
+LADDER = (8192, 16384, 32768, 65536)
+
+
+def ladder_arm(args) -> None:
+    """The large ladder: B = 32 plain-method candidates at n = 8192, cell
+    split n -> 2n up to 65536 with the certified F checked bit for bit at
+    every split; at each level an Adam + adjoint segment (b recomputed every
+    step, never stored), one Chambolle-Pock Frank-Wolfe round and an fp64
+    island ranking + migration (4 islands of 8, top 1); BF16x3 search, exact
+    fp64 certification of the final F.  Prints one JSON line (its own metric)."""
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import sidon_b200
+    sidon_b200.load(build=not (ROOT / "sidon-autocorrelation-bound_b200" / "libsidon_b200.so").exists())
+    from sidon_b200 import kernels, synth
+
+    B = args.ladder_B
+    prec = args.precision if args.precision != "fp32" else "bf16x3"
+    stream = torch.cuda.current_stream()
+    pop = torch.as_tensor(synth.population("structured", LADDER[0], B, seed=4 + rank), device=dev)
+    F_start = kernels.certify(pop)[0].cpu().numpy()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    # warm-up of every kernel on a small case
+    w = torch.as_tensor(synth.population("structured", 1024, 2, seed=1), device=dev)
+    kernels.run_local_search_large(w, 3, 2.0, 4.0, 1e-3, 1e-3, precision=prec, q=512)
+    kernels.run_frank_wolfe_large(w, 1, 2, 2, 0.3, tau=0.9, sigma=0.9, precision=prec, q=512)
+    torch.cuda.synchronize()
+
+    levels = []
+    steps, pdhg = args.ladder_steps, args.ladder_pdhg
+    total_ms = 0.0
+    with Clocks(local) as clk:
+        for li, n in enumerate(LADDER):
+            if li > 0:
+                before = kernels.certify_large(pop)[0]
+                pop = kernels.refine(pop)
+                after = kernels.certify_large(pop)[0]
+                split_exact = bool(torch.equal(before, after))
+            else:
+                split_exact = None
+            q_sel, q_ms = kernels.autotune_large(n, B, prec)
+            ws_t = kernels.large_workspace(n, B, 0, dev, prec)
+            mom, vel = torch.empty_like(pop), torch.empty_like(pop)
+            # p grows geometrically over the ladder, one range per level
+            pA = 2.0 * (512.0 ** (li / len(LADDER)))
+            pB = 2.0 * (512.0 ** ((li + 1) / len(LADDER)))
+            ls_ms = timed(lambda: kernels.run_local_search_large(
+                pop, steps, pA, pB, 1e-3, 1e-3, precision=prec, workspace=ws_t, mom=mom, vel=vel))
+            fw_ms = timed(lambda: kernels.run_frank_wolfe_large(
+                pop, 1, pdhg, 12, 0.3, tau=0.9, sigma=0.9, precision=prec, workspace=ws_t))
+            fit = torch.empty(B, dtype=torch.float64, device=dev)
+
+            def mig():
+                f, _ = kernels.run_eval(pop, with_nactive=False)
+                fit.copy_(f)
+                kernels.island_migrate(pop, fit, 4, 1)
+            mig_ms = timed(mig)
+            total_ms += ls_ms + fw_ms + mig_ms
+            Fl = kernels.certify_large(pop)[0].cpu().numpy()
+            flop = 4.0 * n * n * B * steps
+            levels.append({"n": n, "split_F_bit_exact": split_exact,
+                           "schedule": "fused" if q_sel >= n else f"super-blocks q={q_sel}",
+                           "adam_steps_per_s": steps / (ls_ms / 1e3),
+                           "adam_tflops_algorithmic": flop / (ls_ms / 1e3) / 1e12,
+                           "fw_round_ms": fw_ms, "fw_pdhg_iters": pdhg,
+                           "fw_tflops_algorithmic": (4.0 * n * n * pdhg + 26.0 * n * n) * B
+                           / (fw_ms / 1e3) / 1e12,
+                           "migrate_ms": mig_ms,
+                           "F_median": float(np.nanmedian(Fl)), "F_best": float(np.nanmin(Fl))})
+            del ws_t
+    Fc, _, _, _ = kernels.certify_large(pop)
+    Fe, _ = kernels.run_eval(pop, with_nactive=False)
+    host_check = [abs(Fc[p].item() - kernels.host_f(pop[p].cpu().double().numpy())) /
+                  Fc[p].item() for p in range(min(2, B))]
+    ck = clk.summary()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "ladder_adam_steps_per_s_at_65536", "value": levels[-1]["adam_steps_per_s"],
+            "unit": "batched steps/s", "n_gpus": 1, "higher_is_better": True,
+            "data": "synthetic", "dtype": prec,
+            "config": {"workload": f"large ladder B={B}: {list(LADDER)}, cell splits, "
+                                   f"{steps} Adam steps + 1 FW round ({pdhg} PDHG) + "
+                                   f"migration per level", "precision": prec},
+            "levels": levels, "ladder_seconds": total_ms / 1e3,
+            "F": {"start_median": float(np.median(F_start)),
+                  "final_certified_median": float(np.nanmedian(Fc.cpu().numpy())),
+                  "final_certified_best": float(np.nanmin(Fc.cpu().numpy())),
+                  "certified_vs_eval_max_rel": float(((Fc - Fe).abs() / Fe).max().item()),
+                  "certified_vs_hostF_rel": host_check},
+            "clocks": {"sm_mhz": ck["sm_mhz"], "sm_max_mhz": ck["sm_max_mhz"],
+                       "reasons": ck["reasons"]},
+        }))
+
+
 def _traffic(prec: str):
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
@@ -457,7 +562,10 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=os.environ.get("SIDON_BENCH_PRECISION", "bf16x3"),
                     choices=["fp32", "bf16x3", "bf16x1"])
-    ap.add_argument("--workload", default="lp_adam", choices=["lp_adam", "islands"])
+    ap.add_argument("--workload", default="lp_adam", choices=["lp_adam", "islands", "ladder"])
+    ap.add_argument("--ladder-B", type=int, default=32)
+    ap.add_argument("--ladder-steps", type=int, default=200)
+    ap.add_argument("--ladder-pdhg", type=int, default=100)
     ap.add_argument("--islands-P", type=int, default=1024)
     ap.add_argument("--anneal-steps", type=int, default=5000)
     ap.add_argument("--fw-every", type=int, default=250)
@@ -472,6 +580,8 @@ def main() -> None:
         reference_arm(args)
     elif args.workload == "islands":
         islands_arm(args)
+    elif args.workload == "ladder":
+        ladder_arm(args)
     else:
         our_arm(args)
 

@@ -213,14 +213,25 @@ SIDON_API int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_
  * Candidates longer than one CTA's shared memory (the ladder's 16384,
  * 32768, 65536, ...): the heights are cut into super-blocks of q cells (a
  * multiple of 64 that the single-CTA tensor-core kernels accept; q <= 0
- * picks 8192 or the largest accepted size below it) and every pair of
+ * picks the autotuned size, else 8192 or the largest accepted size below
+ * it; q >= n runs the fused single-CTA kernel when n fits) and every pair of
  * super-blocks is one tensor-core job; stream-ordered elementwise launches
  * combine the jobs' outputs in a fixed order.  Works for any n >= 1 (for
  * n <= q it is one job per product).  precision BF16X3 or BF16X1.  The
  * caller provides the workspace (sidon_large_workspace_bytes; no
  * allocation inside).  No reference counterpart: the reference refuses n
  * whose working set exceeds shared memory (src/main.cu:391-399). */
-SIDON_API size_t sidon_large_workspace_bytes(int n, int P, int q);
+SIDON_API size_t sidon_large_workspace_bytes(int n, int P, int q, int precision);
+
+/* The schedule autotuner: times a short anneal of P candidates of n cells
+ * for the fused single-CTA kernel (when n fits one CTA) and for super-block
+ * sizes 8192 / 4096 / 2048 / 1024, and remembers the fastest for
+ * (device, n, P, precision); q <= 0 in the calls below then uses it (and
+ * sidon_large_workspace_bytes sizes for it).  *out_q: the choice (q >= n =
+ * the fused kernel); *out_ms_per_step: its time.  It allocates scratch with
+ * cudaMalloc and synchronises: call it before any stream capture. */
+SIDON_API int sidon_autotune_large(int n, int P, int precision, int* out_q,
+                                   float* out_ms_per_step);
 
 /* sidon_local_search (fp32 [P][n], Adam moments in mom/vel) for any n. */
 SIDON_API int sidon_local_search_large(float* pop, float* mom, float* vel, const int* skip,

@@ -547,7 +547,7 @@ size_t smem_local_search_tc(int n);
 
 size_t big_workspace_bytes(int n, int P, int Q) {
   if (n < 1 || P < 0 || Q < 64 || Q % 64) return 0;
-  return carve(nullptr, n, P, Q).bytes;
+  return carve(nullptr, n, P, Q < n ? Q : n).bytes;
 }
 
 // the super-block size used when the caller passes 0: the largest multiple
@@ -569,11 +569,25 @@ static int big_prep(int Q) {
   return tc_status_word() ? SIDON_OK : SIDON_ERR_CUDA;
 }
 
+int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* offsets,
+                           const int* order, int P, int n_fixed, int n_max, const int* skip,
+                           const int* mode_arr, int iters, double pS, double pE, double lrS,
+                           double lrE, double b1, double b2, int mode_default, int precision,
+                           cudaStream_t st);
+bool fused_fits(int n);
+int tuned_q(int n, int P, int precision);
+
+// q <= 0: the tuned choice for (n, P, precision) if the tuner has run, else
+// big_default_q; q >= n with n fitting one CTA: the fused kernel
 int launch_local_search_big(float* pop, float* mom, float* vel, const int* skip,
                             const int* mode_arr, int n, int P, int iters, double pS, double pE,
                             double lrS, double lrE, double b1, double b2, int mode_default,
                             int precision, int Q, void* ws, size_t ws_bytes, cudaStream_t st) {
+  if (Q <= 0) Q = tuned_q(n, P, precision);
   if (Q <= 0) Q = big_default_q(n);
+  if (Q >= n && fused_fits(n))
+    return launch_local_search_tc(pop, mom, vel, nullptr, nullptr, P, n, n, skip, mode_arr, iters,
+                                  pS, pE, lrS, lrE, b1, b2, mode_default, precision, st);
   if (Q % 64) return SIDON_ERR_ARG;
   int rc = big_prep(Q);
   if (rc) return rc;
@@ -606,10 +620,24 @@ int launch_local_search_big(float* pop, float* mom, float* vel, const int* skip,
   return rc;
 }
 
+int launch_frank_wolfe_tc(float* pop, float* gbuf, float* gbbuf, const long long* offsets,
+                          const int* order, int P, int n_fixed, int n_max, const int* skip,
+                          int rounds, int pdhg, int nT, float tMax, float tau, float sig,
+                          int precision, cudaStream_t st);
+
+// q as for the local search; the fused kernel takes its g / gbar rows from
+// the workspace
 int launch_frank_wolfe_big(float* pop, const int* skip, int n, int P, int rounds, int pdhg,
                            int nT, float tMax, float tau, float sig, int precision, int Q,
                            void* ws, size_t ws_bytes, cudaStream_t st) {
+  if (Q <= 0) Q = tuned_q(n, P, precision);
   if (Q <= 0) Q = big_default_q(n);
+  if (Q >= n && fused_fits(n)) {
+    Work w = carve(ws, n, P, Q);
+    if (!ws || ws_bytes < w.bytes) return SIDON_ERR_CAPACITY;
+    return launch_frank_wolfe_tc(pop, w.g, w.gb, nullptr, nullptr, P, n, n, skip, rounds, pdhg,
+                                 nT, tMax, tau, sig, precision, st);
+  }
   if (Q % 64) return SIDON_ERR_ARG;
   int rc = big_prep(Q);
   if (rc) return rc;

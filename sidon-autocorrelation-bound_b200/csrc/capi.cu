@@ -56,6 +56,8 @@ int launch_certify_large(const void* pop, int dtype, int n, int P, double* outF,
                          double* outS, int* outK, void* ws, cudaStream_t st);
 size_t big_workspace_bytes(int n, int P, int Q);
 int big_default_q(int n);
+int tuned_q(int n, int P, int precision);
+int autotune_local_search(int n, int P, int precision, int* out_q, float* out_ms);
 int launch_local_search_big(float* pop, float* mom, float* vel, const int* skip,
                             const int* mode_arr, int n, int P, int iters, double pS, double pE,
                             double lrS, double lrE, double b1, double b2, int mode_default,
@@ -343,9 +345,18 @@ int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, i
   return launch_island_migrate(pop, n, fit, P, n_islands, k_migrate, order_out, S(stream));
 }
 
-size_t sidon_large_workspace_bytes(int n, int P, int q) {
+size_t sidon_large_workspace_bytes(int n, int P, int q, int precision) {
+  if (q <= 0) q = tuned_q(n, P, precision);
   if (q <= 0) q = big_default_q(n);
   return big_workspace_bytes(n, P, q);
+}
+
+int sidon_autotune_large(int n, int P, int precision, int* out_q, float* out_ms_per_step) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P < 1) return SIDON_ERR_ARG;
+  if (precision != SIDON_PREC_BF16X1 && precision != SIDON_PREC_BF16X3) return SIDON_ERR_DTYPE;
+  return autotune_local_search(n, P, precision, out_q, out_ms_per_step);
 }
 
 int sidon_local_search_large(float* pop, float* mom, float* vel, const int* skip,

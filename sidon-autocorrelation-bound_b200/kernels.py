@@ -262,9 +262,21 @@ def island_migrate(pop: torch.Tensor, fit: torch.Tensor, n_islands: int, k: int 
 
 
 # ----------------------------- large candidates ----------------------------
-def large_workspace(n: int, P: int, q: int = 0, device="cuda") -> torch.Tensor:
+def autotune_large(n: int, P: int, precision: str = "bf16x3") -> tuple[int, float]:
+    """Measure and remember the fastest schedule for (n, P): returns (q, ms
+    per step); q >= n is the fused single-CTA kernel."""
+    q = C.c_int()
+    ms = C.c_float()
+    _lib.call("sidon_autotune_large", int(n), int(P), PRECISIONS[precision], C.byref(q),
+              C.byref(ms))
+    return q.value, ms.value
+
+
+def large_workspace(n: int, P: int, q: int = 0, device="cuda",
+                    precision: str = "bf16x3") -> torch.Tensor:
     """Workspace for run_local_search_large / run_frank_wolfe_large."""
-    nbytes = _lib.load().sidon_large_workspace_bytes(int(n), int(P), int(q))
+    nbytes = _lib.load().sidon_large_workspace_bytes(int(n), int(P), int(q),
+                                                     PRECISIONS[precision])
     if nbytes == 0:
         raise ValueError("bad large-candidate geometry")
     return torch.empty(nbytes, dtype=torch.uint8, device=device)
@@ -280,7 +292,7 @@ def run_local_search_large(pop: torch.Tensor, iters: int, p_start: float, p_end:
     """run_local_search for candidates of any n (super-block tensor-core jobs)."""
     n, P = _pop_shape(pop)
     if workspace is None:
-        workspace = large_workspace(n, P, q, pop.device)
+        workspace = large_workspace(n, P, q, pop.device, precision)
     if mom is None:
         mom = torch.empty_like(pop)
     if vel is None:
@@ -301,7 +313,7 @@ def run_frank_wolfe_large(pop: torch.Tensor, rounds: int, pdhg_iters: int, nT: i
     """run_frank_wolfe_tc for candidates of any n."""
     n, P = _pop_shape(pop)
     if workspace is None:
-        workspace = large_workspace(n, P, q, pop.device)
+        workspace = large_workspace(n, P, q, pop.device, precision)
     _lib.call("sidon_frank_wolfe_large", _dev(pop, "pop", torch.float32),
               _opt(skip, "skip", torch.int32), n, P, int(rounds), int(pdhg_iters), int(nT),
               float(t_max), float(tau), float(sigma), PRECISIONS[precision], int(q),

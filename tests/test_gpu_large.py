@@ -144,3 +144,19 @@ def test_large_frank_wolfe_tracks_single_cta(cuda):
         Fb = K().host_f(B[p].astype(np.float64))
         assert Fa <= F0 * (1 + 1e-9)
         assert abs(Fa - Fb) <= 2e-3 * Fb, (p, Fa, Fb)
+
+
+def test_autotuner_choice_is_used(cuda):
+    """The tuner returns a valid schedule, q <= 0 then runs it, and the
+    result equals an explicit call with the chosen q bit for bit."""
+    from sidon_b200 import synth
+    n, P = 4096, 4
+    q, ms = K().autotune_large(n, P)
+    assert ms > 0 and (q >= n or (q % 64 == 0 and q < n))
+    assert K().autotune_large(n, P) == (q, ms)           # cached
+    pop = synth.population("structured", n, P, seed=91)
+    a = T(pop, cuda)
+    b = T(pop, cuda)
+    K().run_local_search_large(a, 5, 2.0, 8.0, 1e-3, 1e-3)
+    K().run_local_search_large(b, 5, 2.0, 8.0, 1e-3, 1e-3, q=q)
+    assert torch.equal(a, b)
