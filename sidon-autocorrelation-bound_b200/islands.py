@@ -23,6 +23,8 @@ import torch.distributed as dist
 
 
 def _ws(group):
+    if not dist.is_initialized():
+        return 1, 0
     return dist.get_world_size(group), dist.get_rank(group)
 
 
@@ -65,6 +67,10 @@ def global_best(fit: torch.Tensor, group=None) -> tuple[float, int, int]:
     never wins; ties go to the lower rank, then the lower index."""
     W, r = _ws(group)
     f = fit.detach().double()
+    if W == 1:
+        f1 = torch.where(torch.isnan(f), torch.full_like(f, float("inf")), f)
+        i = int(torch.argmin(f1).item())
+        return (f1[i].item(), 0, i)
     f = torch.where(torch.isnan(f), torch.full_like(f, float("inf")), f)
     idx = int(torch.argmin(f).item())
     mine = torch.tensor([f[idx].item(), float(r), float(idx)], dtype=torch.float64,

@@ -99,3 +99,17 @@ def test_shard_covers_everything():
             assert spans[0][0] == 0 and spans[-1][1] == P
             assert all(spans[i][1] == spans[i + 1][0] for i in range(W - 1))
             assert max(b - a for a, b in spans) - min(b - a for a, b in spans) <= 1
+
+
+def test_single_process_paths_need_no_group(orc):
+    """Without a process group (one GPU) the helpers reduce to local work."""
+    from sidon_b200 import islands
+    rng = np.random.default_rng(1)
+    pop = torch.from_numpy(rng.uniform(0, 1, (12, 4)).astype(np.float32))
+    fit = torch.from_numpy(rng.uniform(1, 2, 12))
+    want_pop, want_fit, _ = orc.island_migrate(pop.numpy(), fit.numpy(), 3, 1)
+    islands.migrate_across_ranks(pop, fit, 3, 1, local_migrate=_oracle_local)
+    np.testing.assert_array_equal(pop.numpy(), want_pop)
+    F, r, i = islands.global_best(fit)
+    assert r == 0 and F == float(np.min(fit.numpy())) and fit[i].item() == F
+    assert islands.max_over_ranks(3.5) == 3.5
