@@ -25,6 +25,11 @@ namespace tc {
 
 __device__ unsigned int g_status_word = 0u;   // SIDON_ERR_TIMEOUT after a timed-out wait
 
+// cells per thread of the fused step's elementwise update: every n the
+// kernels accept (conv + corr accumulators within 512 TMEM columns, n <= 9728)
+// is covered by kCellsPerThread * NTHREADS
+constexpr int kCellsPerThread = 38;
+
 // ------------------------------ local search ------------------------------
 // Candidates: uniform rows of n_fixed cells (offsets == NULL) or a ragged
 // batch (row p = pop[offsets[p] .. offsets[p+1])).  CTA b runs slots
@@ -68,11 +73,7 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
 
     prime(C, true);
     if (!conv_tc(C, S.sa, status)) break;
-    gather_conv(C, ln, S.cb);                     // b in cb
-
-    float mloc = 0.f;
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) mloc = fmaxf(mloc, S.cb[pidx(k)]);
-    const float M = block_max(mloc, S.red);
+    const float M = block_max(gather_conv(C, ln, S.cb), S.red);   // b in cb
     if (!(M > 0.f)) break;
     // c_k = (1+d)^(p-1) in place, R = sum c_k (1+d), d = (b_k - M)/M
     float rloc = 0.f;
@@ -89,49 +90,50 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
     const float bc1 = 1.f / (1.f - b1t), bc2 = 1.f / (1.f - b2t);
     const float lrn = lr / (float)n;
 
+    // the Adam moments of this thread's cells, loaded now so that the
+    // correlation phase hides their L2 / HBM latency
+    float pm[kCellsPerThread], pv[kCellsPerThread];
+    if (mode == 0) {
+#pragma unroll
+      for (int u = 0; u < kCellsPerThread; ++u) {
+        const int i = threadIdx.x + u * NTHREADS;
+        if (i < n) {
+          pm[u] = mg[i];
+          pv[u] = vg[i];
+        }
+      }
+    }
     fence_before();
     __syncthreads();
     if (!corr_tc(C, S.sa, S.cb, status)) break;
     gather_corr(C, ln, S.cb);                     // G in cb (weights no longer needed)
 
-    // Adam / mirror step; four cells per thread per pass so the moment loads
-    // of HBM/L2 overlap
+    // Adam / mirror step (cells i = thread + u * NTHREADS)
     float sloc = 0.f;
     const float invR = 1.f / R;
-    for (int i0 = threadIdx.x; i0 < n; i0 += 4 * blockDim.x) {
-      float g4[4], m4[4], v4[4], x4[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = i0 + u * blockDim.x;
-        if (i < n) {
-          g4[u] = S.cb[pidx(i)] * invR - M;
-          x4[u] = S.sa[pidx(i)];
-          if (mode == 0) { m4[u] = mg[i]; v4[u] = vg[i]; }
-        }
+    for (int u = 0; u < kCellsPerThread; ++u) {
+      const int i = threadIdx.x + u * NTHREADS;
+      if (i >= n) continue;
+      const float gi = S.cb[pidx(i)] * invR - M;
+      const float x0 = S.sa[pidx(i)];
+      float x;
+      if (mode == 0) {
+        const float mm = __fmaf_rn(beta1, pm[u], (1.f - beta1) * gi);
+        const float vv = __fmaf_rn(beta2, pv[u], (1.f - beta2) * gi * gi);
+        mg[i] = mm;
+        vg[i] = vv;
+        const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
+        x = x0 - step;
+        if (x < 0.f) x = 0.f;
+      } else {
+        float e = -lr * (gi * invM);
+        if (e > 4.f) e = 4.f;
+        if (e < -4.f) e = -4.f;
+        x = x0 * __expf(e);
       }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = i0 + u * blockDim.x;
-        if (i >= n) continue;
-        const float gi = g4[u];
-        float x;
-        if (mode == 0) {
-          const float mm = __fmaf_rn(beta1, m4[u], (1.f - beta1) * gi);
-          const float vv = __fmaf_rn(beta2, v4[u], (1.f - beta2) * gi * gi);
-          mg[i] = mm;
-          vg[i] = vv;
-          const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
-          x = x4[u] - step;
-          if (x < 0.f) x = 0.f;
-        } else {
-          float e = -lr * (gi * invM);
-          if (e > 4.f) e = 4.f;
-          if (e < -4.f) e = -4.f;
-          x = x4[u] * __expf(e);
-        }
-        S.sa[pidx(i)] = x;
-        sloc += x;
-      }
+      S.sa[pidx(i)] = x;
+      sloc += x;
     }
     float Ssum = block_sum(sloc, S.red);
     if (!(Ssum > 0.f)) {
@@ -424,7 +426,10 @@ static size_t smem_lp_forward_tc(int n) { return tc::Layout(n).total; }
 // the two accumulators must fit the 512 TMEM columns
 static int tc_n_ok(int n) {
   const int m = (n + tc::BL - 1) / tc::BL;
-  return (n >= 1 && tc::conv_width(m) + tc::corr_width(m) <= 512) ? SIDON_OK : SIDON_ERR_N;
+  return (n >= 1 && n <= tc::kCellsPerThread * tc::NTHREADS &&
+          tc::conv_width(m) + tc::corr_width(m) <= 512)
+             ? SIDON_OK
+             : SIDON_ERR_N;
 }
 
 static int prep_tc(const void* fn, size_t sm) { return set_dyn_smem(fn, sm); }

@@ -505,8 +505,9 @@ struct Lane {
 };
 
 // b = a * a into X (padded layout, k < 2n-1): the two cells of each k are
-// combined through X.  Ends synchronised.
-__device__ __forceinline__ void gather_conv(Ctx& C, const Lane& ln, float* X) {
+// combined through X.  Ends synchronised.  Returns the largest b_k the
+// calling thread finalised (every k is finalised by exactly one thread).
+__device__ __forceinline__ float gather_conv(Ctx& C, const Lane& ln, float* X) {
   const int nb = 2 * C.n - 1, nch = (2 * C.m + 1 + 31) / 32;
   const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16);
   if (ln.quad >= 2) {
@@ -522,6 +523,7 @@ __device__ __forceinline__ void gather_conv(Ctx& C, const Lane& ln, float* X) {
     }
   }
   __syncthreads();
+  float mloc = 0.f;
   if (ln.quad < 2) {
     for (int c = ln.half; c < nch; c += 2) {
       float v[32];
@@ -529,11 +531,16 @@ __device__ __forceinline__ void gather_conv(Ctx& C, const Lane& ln, float* X) {
 #pragma unroll
       for (int t = 0; t < 32; ++t) {
         const int k = 64 * (32 * c + t) + ln.r;
-        if (k < nb) X[pidx(k)] += v[t];
+        if (k < nb) {
+          const float b = X[pidx(k)] + v[t];
+          X[pidx(k)] = b;
+          mloc = fmaxf(mloc, b);
+        }
       }
     }
   }
   __syncthreads();
+  return mloc;
 }
 
 // G_i into Y (padded layout, i < n) from the correlation accumulator.
