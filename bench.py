@@ -116,6 +116,17 @@ def _dist():
     return ws, rank, local
 
 
+def _config(prec: str, ws: int) -> dict:
+    """The workload both arms report (the metric's configuration)."""
+    return {"workload": f"lp_adam n={N_CELLS} B={BATCH}/GPU lognormal heights, "
+                        f"p {ANNEAL['p_start']}->{ANNEAL['p_end']} (one batched step = conv + "
+                        f"adjoint correlation + Adam update of every candidate)",
+            "global_batch": BATCH * ws, "n": N_CELLS, "precision": prec,
+            "parallelism": f"candidates sharded, {ws} x {BATCH}",
+            "l2": "single launch of K steps, population resident in shared memory; "
+                  "L2 flushed (256 MB write) before the timed launch"}
+
+
 # --------------------------------- reference arm ---------------------------
 def reference_arm(args) -> None:
     ws, rank, _ = _dist()
@@ -151,8 +162,7 @@ def reference_arm(args) -> None:
         "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"lp_adam n={N_CELLS} B={BATCH} (lognormal heights)",
-                   "global_batch": BATCH, "n": N_CELLS},
+        "config": _config(args.precision, args.gpus),
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "reference",
                          "sample": f"tools/probe.cpp localSearch (fp64 CPU twin), {sample_c} "
                                    f"candidates x {iters} steps per timed step, OpenMP over "
@@ -339,12 +349,7 @@ def our_arm(args) -> None:
             "vs_baseline": None, "dtype": {"fp32": "f32", "bf16x3": "bf16x3(f32 acc)",
                                             "bf16x1": "bf16(f32 acc)"}[prec],
             "data": "synthetic",
-            "config": {"workload": f"lp_adam n={N_CELLS} B={BATCH}/GPU lognormal heights, "
-                                   f"{prec} conv/corr, p {ANNEAL['p_start']}->{ANNEAL['p_end']}",
-                       "global_batch": BATCH * ws, "n": N_CELLS, "precision": prec,
-                       "parallelism": f"candidates sharded, {ws} x {BATCH}",
-                       "l2": "single launch of K steps, population resident in shared memory; "
-                             "L2 flushed (256 MB write) before the timed launch"},
+            "config": _config(prec, ws),
             "candidate_steps_per_s": value * BATCH,
             "fp32_simt_steps_per_s": simt,
             "speedup_vs_fp32_simt": (value / ws) / simt if simt else None,
