@@ -500,7 +500,8 @@ def ladder_arm(args) -> None:
     B = args.ladder_B
     prec = args.precision if args.precision != "fp32" else "bf16x3"
     stream = torch.cuda.current_stream()
-    pop = torch.as_tensor(synth.population("structured", LADDER[0], B, seed=4 + rank), device=dev)
+    ladder = [int(x) for x in args.ladder_levels.split(",")]
+    pop = torch.as_tensor(synth.population("structured", ladder[0], B, seed=4 + rank), device=dev)
     F_start = kernels.certify(pop)[0].cpu().numpy()
 
     def timed(fn):
@@ -521,7 +522,7 @@ def ladder_arm(args) -> None:
     steps, pdhg = args.ladder_steps, args.ladder_pdhg
     total_ms = 0.0
     with Clocks(local) as clk:
-        for li, n in enumerate(LADDER):
+        for li, n in enumerate(ladder):
             if li > 0:
                 before = kernels.certify_large(pop)[0]
                 pop = kernels.refine(pop)
@@ -529,23 +530,29 @@ def ladder_arm(args) -> None:
                 split_exact = bool(torch.equal(before, after))
             else:
                 split_exact = None
-            q_sel, q_ms = kernels.autotune_large(n, B, prec)
-            ws_t = kernels.large_workspace(n, B, 0, dev, prec)
+            if args.ladder_q > 0:
+                q_sel = args.ladder_q
+            else:
+                q_sel, _ = kernels.autotune_large(n, B, prec)
+            ws_t = kernels.large_workspace(n, B, q_sel, dev, prec)
             mom, vel = torch.empty_like(pop), torch.empty_like(pop)
             # p grows geometrically over the ladder, one range per level
-            pA = 2.0 * (512.0 ** (li / len(LADDER)))
-            pB = 2.0 * (512.0 ** ((li + 1) / len(LADDER)))
+            pA = 2.0 * (512.0 ** (li / len(ladder)))
+            pB = 2.0 * (512.0 ** ((li + 1) / len(ladder)))
             ls_ms = timed(lambda: kernels.run_local_search_large(
-                pop, steps, pA, pB, 1e-3, 1e-3, precision=prec, workspace=ws_t, mom=mom, vel=vel))
+                pop, steps, pA, pB, 1e-3, 1e-3, precision=prec, q=q_sel, workspace=ws_t, mom=mom,
+                vel=vel))
             fw_ms = timed(lambda: kernels.run_frank_wolfe_large(
-                pop, 1, pdhg, 12, 0.3, tau=0.9, sigma=0.9, precision=prec, workspace=ws_t))
+                pop, 1, pdhg, 12, 0.3, tau=0.9, sigma=0.9, precision=prec, q=q_sel,
+                workspace=ws_t))
             fit = torch.empty(B, dtype=torch.float64, device=dev)
+            n_isl = 4 if B % 4 == 0 and B >= 8 else 1
 
             def mig():
                 f, _ = kernels.run_eval(pop, with_nactive=False)
                 fit.copy_(f)
-                # 4 islands per rank on one global ring (NCCL hop between ranks)
-                islands.migrate_across_ranks(pop, fit, 4, 1)
+                # islands per rank on one global ring (NCCL hop between ranks)
+                islands.migrate_across_ranks(pop, fit, n_isl, 1 if B // n_isl >= 2 else 0)
             mig_ms = timed(mig)
             ls_ms = islands.max_over_ranks(ls_ms, dev)
             fw_ms = islands.max_over_ranks(fw_ms, dev)
@@ -578,7 +585,7 @@ def ladder_arm(args) -> None:
             "unit": "batched steps/s (per rank; ranks run B candidates each)", "n_gpus": ws,
             "global_best": best, "higher_is_better": True,
             "data": "synthetic", "dtype": prec,
-            "config": {"workload": f"large ladder B={B}: {list(LADDER)}, cell splits, "
+            "config": {"workload": f"large ladder B={B}: {ladder}, cell splits, "
                                    f"{steps} Adam steps + 1 FW round ({pdhg} PDHG) + "
                                    f"migration per level", "precision": prec},
             "levels": levels, "ladder_seconds": total_ms / 1e3,
@@ -612,6 +619,8 @@ def main() -> None:
     ap.add_argument("--ladder-B", type=int, default=32)
     ap.add_argument("--ladder-steps", type=int, default=200)
     ap.add_argument("--ladder-pdhg", type=int, default=100)
+    ap.add_argument("--ladder-levels", default=",".join(str(x) for x in LADDER))
+    ap.add_argument("--ladder-q", type=int, default=0, help="super-block size (0: autotune)")
     ap.add_argument("--islands-P", type=int, default=1024)
     ap.add_argument("--anneal-steps", type=int, default=5000)
     ap.add_argument("--fw-every", type=int, default=250)

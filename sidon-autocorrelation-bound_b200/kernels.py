@@ -162,8 +162,13 @@ def certify(pop: torch.Tensor, stream=None):
     M = torch.empty(P, dtype=torch.float64, device=dev)
     S = torch.empty(P, dtype=torch.float64, device=dev)
     K = torch.empty(P, dtype=torch.int32, device=dev)
-    _lib.call("sidon_certify", _dev(pop, "pop"), code, n, P, F.data_ptr(), M.data_ptr(),
-              S.data_ptr(), K.data_ptr(), _stream(stream))
+    try:
+        _lib.call("sidon_certify", _dev(pop, "pop"), code, n, P, F.data_ptr(), M.data_ptr(),
+                  S.data_ptr(), K.data_ptr(), _stream(stream))
+    except SidonError as e:
+        if e.status != _lib.ERR_SMEM:
+            raise
+        return certify_large(pop, stream)     # beyond shared memory: streamed + list path
     return F, M, S, K
 
 
