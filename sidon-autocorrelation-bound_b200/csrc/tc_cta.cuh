@@ -79,11 +79,8 @@ __device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* ra
   S.C.n = n_max;
   S.C.dmax = last_tile(n_max);
   S.C.three = three;
-  S.C.done_use = 0;
+  S.C.ph = S.C.started = S.C.bc_ph = S.C.bc_started = S.C.done_ph = 0u;
   S.C.st_next = 0;
-  S.C.bc_uses[0] = S.C.bc_uses[1] = 0;
-#pragma unroll
-  for (int s = 0; s < STAGES; ++s) S.C.uses[s] = 0;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&S.C.full[s], NBUILD_WARPS);

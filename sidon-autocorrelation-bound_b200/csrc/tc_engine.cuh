@@ -208,9 +208,12 @@ struct Ctx {
   uint64_t* bc_empty;      // 2 "copy consumed" barriers (tcgen05.commit)
   uint64_t* bar_done;      // "all MMAs of a phase done"
   uint32_t tmem;           // TMEM base address (512 columns)
-  int uses[STAGES];        // times each stage has been filled (builders) / consumed (MMA)
-  int bc_uses[2];
-  int done_use;
+  // pipeline phases as bit masks (registers, no dynamic indexing): bit s of
+  // ph = parity of this thread's next wait on stage s (full for the MMA
+  // lane, empty for the builders); bit s of started = stage s filled before
+  // (builders skip the first empty wait); bc_ph / bc_started likewise for
+  // the copy slots; done_ph = parity of the next bar_done wait
+  uint32_t ph, started, bc_ph, bc_started, done_ph;
   int st_next;             // next stage in the ring
   int* abort;              // shared abort flag
   int m, rc, rcc, n, dmax; // blocks, conv / corr copy rows, cells, last tile
@@ -408,7 +411,7 @@ __device__ __forceinline__ void issue_tile(Ctx& C, int st, uint32_t b_hi, uint32
 //   bsrc / blen: the copy source of CONV_X (see build_conv_copy) or the
 //   padded shared weights of CORR.
 template <int MODE>
-__device__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen,
+__device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen,
                           unsigned int* status) {
   constexpr bool corr = MODE == CORR;
   constexpr bool three_prod = MODE != CONV_SYM;
@@ -424,8 +427,8 @@ __device__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen
       const int cb_cols = corr_n(m);
       for (int rho = 0; rho < 8 && rho <= C.dmax; rho += 2) {
         const int slot = MODE == CONV_SYM ? ((rho >> 1) & 1) : 0;
-        if (!wait_phase(C, &C.bc_full[slot], (uint32_t)(C.bc_uses[slot] & 1), status)) break;
-        C.bc_uses[slot] += 1;
+        if (!wait_phase(C, &C.bc_full[slot], (C.bc_ph >> slot) & 1u, status)) break;
+        C.bc_ph ^= 1u << slot;
         const uint32_t bbase = smem_u32(C.bc) + (uint32_t)slot * C.rc * 128u;
         const uint32_t blo = bbase + (uint32_t)lo_off;
         bool ok = true;
@@ -441,8 +444,8 @@ __device__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen
             T.x0 = t + rho + ZP;
             T.N = round_up(m - t, 16);
           }
-          if (!wait_phase(C, &C.full[st], (uint32_t)(C.uses[st] & 1), status)) { ok = false; break; }
-          C.uses[st] += 1;
+          if (!wait_phase(C, &C.full[st], (C.ph >> st) & 1u, status)) { ok = false; break; }
+          C.ph ^= 1u << st;
           fence_after();
           issue_tile(C, st, bbase, blo, T, three_prod);
           mma_commit(&C.empty[st]);
@@ -458,9 +461,11 @@ __device__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen
     const int bt = threadIdx.x - (warp > MMA_WARP ? 32 : 0);   // 0 .. NBUILD-1
     for (int rho = 0; rho < 8 && rho <= C.dmax; rho += 2) {
       const int slot = MODE == CONV_SYM ? ((rho >> 1) & 1) : 0;
-      const int u = C.bc_uses[slot];
-      if (u > 0 && !wait_phase(C, &C.bc_empty[slot], (uint32_t)((u - 1) & 1), status)) break;
-      C.bc_uses[slot] = u + 1;
+      if ((C.bc_started >> slot) & 1u) {
+        if (!wait_phase(C, &C.bc_empty[slot], (C.bc_ph >> slot) & 1u, status)) break;
+        C.bc_ph ^= 1u << slot;
+      }
+      C.bc_started |= 1u << slot;
       unsigned char* hi = C.bc + (size_t)slot * C.rc * 128;
       if (corr) build_corr_copy(C, bsrc, rho, want_lo, bt);
       else if (MODE == CONV_X) build_conv_copy(C, bsrc, blen, rho, hi, hi + lo_off, want_lo, bt);
@@ -470,12 +475,14 @@ __device__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen
       if (lane == 0) mbar_arrive(&C.bc_full[slot]);
       bool ok = true;
       for (int w = rho; w <= C.dmax; w += 8) {
-        const int us = C.uses[st];
-        if (us > 0 && !wait_phase(C, &C.empty[st], (uint32_t)((us - 1) & 1), status)) {
-          ok = false;
-          break;
+        if ((C.started >> st) & 1u) {
+          if (!wait_phase(C, &C.empty[st], (C.ph >> st) & 1u, status)) {
+            ok = false;
+            break;
+          }
+          C.ph ^= 1u << st;
         }
-        C.uses[st] = us + 1;
+        C.started |= 1u << st;
         build_window(C, st, wsrc, w, lsc, bt);
         fence_async_smem();
         __syncwarp();
@@ -486,8 +493,8 @@ __device__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen
     }
   }
   C.st_next = st;
-  const bool ok = wait_phase(C, C.bar_done, (uint32_t)(C.done_use & 1), status);
-  C.done_use += 1;
+  const bool ok = wait_phase(C, C.bar_done, C.done_ph, status);
+  C.done_ph ^= 1u;
   fence_after();
   __syncthreads();
   return ok && !*((volatile int*)C.abort);
