@@ -96,11 +96,11 @@ int sm_count() {
   return v > 0 ? v : 1;
 }
 int set_dyn_smem(const void* fn, size_t smem) {
-  if ((long long)smem > (long long)smem_optin()) return SIDON_ERR_SMEM;
   struct Entry {
     int dev;
     const void* fn;
-    size_t smem;
+    size_t smem;     // dynamic bytes granted so far
+    size_t stat;     // the kernel's static shared memory
   };
   static std::mutex mu;
   static std::vector<Entry> done;
@@ -108,17 +108,22 @@ int set_dyn_smem(const void* fn, size_t smem) {
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return set_cuda_error(e);
   std::lock_guard<std::mutex> lock(mu);
-  for (Entry& x : done)
-    if (x.dev == dev && x.fn == fn) {
-      if (x.smem >= smem) return SIDON_OK;
-      e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return set_cuda_error(e);
-      x.smem = smem;
-      return SIDON_OK;
-    }
+  Entry* x = nullptr;
+  for (Entry& y : done)
+    if (y.dev == dev && y.fn == fn) x = &y;
+  if (!x) {
+    // the static shared memory counts against the same per-block limit
+    cudaFuncAttributes attr;
+    e = cudaFuncGetAttributes(&attr, fn);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    done.push_back({dev, fn, 0, attr.sharedSizeBytes});
+    x = &done.back();
+  }
+  if ((long long)(smem + x->stat) > (long long)smem_optin()) return SIDON_ERR_SMEM;
+  if (x->smem >= smem) return SIDON_OK;
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return set_cuda_error(e);
-  done.push_back({dev, fn, smem});
+  x->smem = smem;
   return SIDON_OK;
 }
 int device_ok() {

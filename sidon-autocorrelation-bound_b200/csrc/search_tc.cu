@@ -154,18 +154,20 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
 // As k_lp_forward: M refined in fp64 over the near-maximal k (the split
 // error of b is < 3e-5 of max b), S in fp64, R from the tensor-core b.
 constexpr int kRefineCap = 1024;
+static_assert(kRefineCap * sizeof(int) <= (size_t)STAGES * STAGE_BYTES, "list fits the ring");
 
 __global__ void __launch_bounds__(NTHREADS, 1)
 k_lp_forward_tc(const float* __restrict__ pop, int n, float p, float* __restrict__ value,
                 float* __restrict__ saved, float* __restrict__ b_out, int three,
                 unsigned int* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ int s_list[kRefineCap];
   __shared__ int s_cnt;
   __shared__ double s_red[32];
   const int pid = blockIdx.x;
   Shared S = setup(n, three != 0, smem_raw);
   Ctx& C = S.C;
+  // the refinement list lives in the window ring, idle outside tile phases
+  int* s_list = reinterpret_cast<int*>(C.stages);
   begin(S, n, n);
   const int nb = 2 * n - 1;
   const Lane ln;
@@ -280,11 +282,12 @@ k_frank_wolfe_tc(float* pop, float* gbuf, float* gbbuf, const long long* __restr
                  const int* __restrict__ skip, int rounds, int pdhgIters, int nT, float tMax,
                  float tau_in, float sig_in, int three, unsigned int* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ int s_list[kFwRefineCap];
   __shared__ int s_cnt;
   __shared__ double s_red[32];
   Shared S = setup(n_max, three != 0, smem_raw);
   Ctx& C = S.C;
+  // the refinement list lives in the window ring, idle outside tile phases
+  int* s_list = reinterpret_cast<int*>(C.stages);
   const Lane ln;
   float* X = reinterpret_cast<float*>(C.bc);   // gather scratch (after a tile phase)
   bool alive = true;

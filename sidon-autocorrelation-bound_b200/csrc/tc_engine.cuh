@@ -332,21 +332,47 @@ __device__ __forceinline__ void build_corr_copy(Ctx& C, const float* cb, int rho
   }
 }
 
+// bf16(x) in the low half, bf16(lsc * (x - bf16(x))) in the high half
+__device__ __forceinline__ uint32_t split_pack(float x, float lsc) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  const __nv_bfloat16 l = __float2bfloat16_rn(lsc * (x - __bfloat162float(h)));
+  return (uint32_t)__bfloat16_as_ushort(h) | ((uint32_t)__bfloat16_as_ushort(l) << 16);
+}
+
 // Window of tile w into stage st: CM[q][i][j] = a[64 w - 63 + 8 q + i + j],
-// planes hi and lsc * lo.
+// planes hi and lsc * lo.  Chunk t = 8 q + i (16 bytes at offset 16 t of a
+// plane) holds the 8 cells from 64 w - 63 + t on: consecutive chunks are
+// windows shifted by one cell.  A warp covers 32 chunks: every lane splits
+// two cells (t and t + 32) once, and the 8 cells of its chunk arrive by warp
+// shuffles, so each cell is loaded and split once per warp instead of once
+// per chunk row.  Warp-uniform (all 32 lanes take part in the shuffles).
 __device__ __forceinline__ void build_window(Ctx& C, int st, const float* sa, int w, float lsc,
                                              int bt) {
   unsigned char* hi = C.stages + st * STAGE_BYTES;
   unsigned char* lo = hi + PLANE;
-  for (int t = bt; t < WIN_CM * 8; t += NBUILD) {
-    const int base = 64 * w - 63 + 8 * (t >> 3) + (t & 7);
-    float v[8];
+  const int lane = bt & 31;
+  const int base0 = 64 * w - 63;
+  for (int t0 = bt - lane; t0 < WIN_CM * 8; t0 += NBUILD) {
+    const int c = base0 + t0 + lane;
+    const uint32_t p0 = split_pack(sa[pidx(c)], lsc);
+    const uint32_t p1 = split_pack(sa[pidx(c + 32)], lsc);
+    uint32_t P[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = sa[pidx(base + j)];
-    uint4 vh, vl;
-    split8(v, lsc, vh, vl);
-    *reinterpret_cast<uint4*>(hi + 16 * t) = vh;
-    *reinterpret_cast<uint4*>(lo + 16 * t) = vl;
+    for (int j = 0; j < 8; ++j) {
+      const int src = (lane + j) & 31;
+      const uint32_t x0 = __shfl_sync(0xffffffffu, p0, src);
+      const uint32_t x1 = __shfl_sync(0xffffffffu, p1, src);
+      P[j] = (lane + j < 32) ? x0 : x1;
+    }
+    const uint4 vh = make_uint4(__byte_perm(P[0], P[1], 0x5410), __byte_perm(P[2], P[3], 0x5410),
+                                __byte_perm(P[4], P[5], 0x5410), __byte_perm(P[6], P[7], 0x5410));
+    const uint4 vl = make_uint4(__byte_perm(P[0], P[1], 0x7632), __byte_perm(P[2], P[3], 0x7632),
+                                __byte_perm(P[4], P[5], 0x7632), __byte_perm(P[6], P[7], 0x7632));
+    const int t = t0 + lane;
+    if (t < WIN_CM * 8) {
+      *reinterpret_cast<uint4*>(hi + 16 * t) = vh;
+      *reinterpret_cast<uint4*>(lo + 16 * t) = vl;
+    }
   }
 }
 

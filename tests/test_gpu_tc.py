@@ -173,3 +173,27 @@ def test_frank_wolfe_tc_improves_like_simt(cuda):
     gain_b = (F0 - Fb).cpu().numpy()
     assert (gain_a >= 0).all()
     assert gain_a.sum() >= 0.8 * gain_b.sum(), (gain_a, gain_b)
+
+
+def test_tc_largest_n(cuda):
+    """The top of the single-CTA range (n = 9728: 152 blocks, 512 TMEM
+    columns, all shared memory) runs every tensor-core kernel; one cell more
+    is refused with SIDON_ERR_N."""
+    from sidon_b200 import synth, _lib
+    n = 9728
+    a = T(synth.population("structured", n, 2, seed=97), cuda)
+    _, saved, b = K().lp_forward(a, 8.0, store_b=True, precision="bf16x3")
+    ref = np.convolve(a[0].double().cpu().numpy(), a[0].double().cpu().numpy())
+    assert np.max(np.abs(b[0].cpu().numpy() - ref)) <= 3e-5 * ref.max()
+    x = a.clone()
+    K().run_local_search(x, 2, 2.0, 4.0, 1e-3, 1e-3, precision="bf16x3")
+    y = a.clone()
+    K().run_frank_wolfe_tc(y, 1, 3, 3, 0.3, tau=0.9, sigma=0.9)
+    F0, _ = K().run_eval(a, with_nactive=False)
+    F1, _ = K().run_eval(y, with_nactive=False)
+    assert bool((F1 <= F0 * (1 + 1e-9)).all())
+    assert _status() == 0
+    big = torch.full((1, n + 1), 1.0 / (n + 1), device=cuda)
+    with pytest.raises(_lib.SidonError) as ei:
+        K().run_local_search(big, 1, 2.0, 4.0, 1e-3, 1e-3, precision="bf16x3")
+    assert ei.value.status == _lib.ERR_N
