@@ -76,13 +76,27 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
     const float M = block_max(gather_conv(C, ln, S.cb), S.red);   // b in cb
     if (!(M > 0.f)) break;
     // c_k = (1+d)^(p-1) in place, R = sum c_k (1+d), d = (b_k - M)/M
+    // (four independent k per pass for instruction-level parallelism; each
+    // thread still adds its terms in k order)
     float rloc = 0.f;
     const float invM = 1.f / M, q = pexp - 1.f;
-    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-      const float d = (S.cb[pidx(k)] - M) * invM;
-      const float cw = d > -1.f ? pow_from_d_fast(d, q) : 0.f;
-      rloc += cw * (1.f + d);
-      S.cb[pidx(k)] = cw;
+    for (int k0 = threadIdx.x; k0 < nb; k0 += 4 * NTHREADS) {
+      float d4[4], c4[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = k0 + u * NTHREADS;
+        d4[u] = k < nb ? (S.cb[pidx(k)] - M) * invM : -1.f;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) c4[u] = d4[u] > -1.f ? pow_from_d_fast(d4[u], q) : 0.f;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int k = k0 + u * NTHREADS;
+        if (k < nb) {
+          rloc += c4[u] * (1.f + d4[u]);
+          S.cb[pidx(k)] = c4[u];
+        }
+      }
     }
     const float R = block_sum(rloc, S.red);      // barrier: weights complete
     b1t *= beta1;

@@ -24,13 +24,14 @@
 //  collects the output i = 64 col + 63 - R:
 //        G_i = D2[R0][col0] + D2[R0 + 64][col0 + 1],  R0 = (63 - i) mod 64.
 //
-//  Shifts.  A tile's B rows are shifted by its diagonal.  Shifts in multiples
-//  of 8 rows are descriptor offsets (8-row core-matrix groups); accumulator
-//  column offsets are kept multiples of DG (TMEM alignment); the residue
-//  (tile mod 8, one of 0, 2, 4, 6) is absorbed by a row-shifted copy of the
-//  B matrix, built once per residue class:
-//        conv:  BC_rho[x] = Bt[x - rho - ZP]  (ZP zero rows in front),
-//        corr:  CC_rho[x] = Cb[x + rho].
+//  Shifts.  A tile's B rows are shifted by its diagonal.  The B copies are
+//  stored row-contiguous within each K group (SBO = 128 B), so a shift by
+//  any number of rows is a descriptor start offset of 16 B per row;
+//  accumulator column offsets are kept multiples of DG (TMEM alignment) and
+//  the rest of the shift (tile - offset) moves the B start:
+//        conv:  BC[x] = Bt[x - ZP]  (ZP zero rows in front), rows from
+//               ZP + offset - tile;
+//        corr:  CC[x] = Cb[x], rows from the tile index.
 //
 //  A Hankel window is never materialised as a 128 x 64 matrix.  A K-major
 //  core matrix (row group G, K group S) of it holds a[start + 8(G+S) + i + j],
@@ -45,8 +46,9 @@
 //  BF16x1 keeps A_hi B_hi.  fp32 accumulation in TMEM.
 //
 //  Pipeline: one MMA warp (one elected lane issues every MMA) and builder
-//  warps; a ring of STAGES window buffers and two copy slots, each guarded by
-//  a full barrier (builder arrivals) and an empty barrier (tcgen05.commit).
+//  warps; a ring of STAGES window buffers and one copy slot per phase, each
+//  guarded by a full barrier (builder arrivals) and an empty barrier
+//  (tcgen05.commit).
 //  Every wait gives up after ~2^31 clock cycles, records SIDON_ERR_TIMEOUT in
 //  the library's device status word and unwinds.
 // ---------------------------------------------------------------------------
@@ -88,8 +90,6 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
 __device__ __forceinline__ uint32_t idesc_bf16(int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(L >> 4) << 24);
 }
-// B plane of 64-wide rows: core matrix (row group g, K group h) at g*1024 + h*128
-constexpr uint32_t B_SBO = 1024;
 
 __device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
                                          uint32_t idesc, uint32_t accumulate) {
@@ -267,25 +267,29 @@ __device__ __forceinline__ void split8(const float (&v)[8], float lsc, uint4& hi
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// chunk c of a 64-wide B plane: row x, K group h; byte offset 16 c
-__device__ __forceinline__ void chunk_xh(int c, int& x, int& h) {
-  x = ((c >> 6) << 3) | (c & 7);
-  h = (c >> 3) & 7;
-}
+// B-matrix copies are row-contiguous within each K group: element (row x,
+// K index k) of a plane with `rows` rows sits at byte
+//      (k / 8) * 16 rows + 16 x + 2 (k % 8),
+// i.e. a K-major operand with SBO = 128 B between 8-row groups and
+// LBO = 16 rows bytes between K groups.  A tile whose B rows start at an
+// arbitrary row x0 is then the descriptor start + 16 x0: no residue-class
+// copies are needed, and each phase builds its copy once.
+__host__ __device__ __forceinline__ uint32_t b_lbo(int rows) { return 16u * (uint32_t)rows; }
 
 // Convolution copy (hi plane at `hi`, lo plane at `lo` when want_lo):
-// BC[x][s] = y[64 (x - rho - ZP) + 63 - s] for block rows in [0, m).  y is
-// either a padded shared-memory array (ylen < 0; zero beyond its cells) or a
-// plain global row of ylen cells read through L2 (cells >= ylen read as 0;
-// the row may be written by this CTA between phases, so no read-only path).
-__device__ __forceinline__ void build_conv_copy(Ctx& C, const float* y, int ylen, int rho,
+// BC[x][s] = y[64 (x - ZP) + 63 - s] for block rows x - ZP in [0, m), zero
+// elsewhere, x < rc.  y is either a padded shared-memory array (ylen < 0;
+// zero beyond its cells) or a plain global row of ylen cells read through
+// L2 (cells >= ylen read as 0; the row may be written by this CTA between
+// phases, so no read-only path).
+__device__ __forceinline__ void build_conv_copy(Ctx& C, const float* y, int ylen,
                                                 unsigned char* hi, unsigned char* lo,
                                                 bool want_lo, int bt) {
-  const int chunks = C.rc * 8;
+  const int rows = C.rc;
+  const int chunks = rows * 8;
   for (int c = bt; c < chunks; c += NBUILD) {
-    int x, h;
-    chunk_xh(c, x, h);
-    const int J = x - rho - ZP;
+    const int h = c / rows, x = c - h * rows;
+    const int J = x - ZP;
     uint4 vh = make_uint4(0, 0, 0, 0), vl = vh;
     if (J >= 0 && J < C.m) {
       // s = 8h .. 8h+7  <->  cells 64J + 63 - 8h down to 64J + 56 - 8h
@@ -303,32 +307,32 @@ __device__ __forceinline__ void build_conv_copy(Ctx& C, const float* y, int ylen
       }
       split8(v, 1.f, vh, vl);
     }
-    *reinterpret_cast<uint4*>(hi + 16 * c) = vh;
-    if (want_lo) *reinterpret_cast<uint4*>(lo + 16 * c) = vl;
+    const uint32_t off = (uint32_t)h * b_lbo(rows) + 16u * (uint32_t)x;
+    *reinterpret_cast<uint4*>(hi + off) = vh;
+    if (want_lo) *reinterpret_cast<uint4*>(lo + off) = vl;
   }
 }
 
-// Correlation copy (hi plane, lo plane right after it):
-// CC[x][s] = c[64 (x + rho) + s] for weight blocks in [0, 2m).
-__device__ __forceinline__ void build_corr_copy(Ctx& C, const float* cb, int rho, bool want_lo,
-                                                int bt) {
+// Correlation copy (hi plane at C.bc, lo plane after it):
+// CC[x][s] = c[64 x + s] for weight blocks x < 2m, zero beyond, x < rcc.
+__device__ __forceinline__ void build_corr_copy(Ctx& C, const float* cb, bool want_lo, int bt) {
+  const int rows = C.rcc;
   unsigned char* hi = C.bc;
-  unsigned char* lo = hi + (size_t)C.rcc * 128;
-  const int chunks = C.rcc * 8;
+  unsigned char* lo = hi + (size_t)rows * 128;
+  const int chunks = rows * 8;
   for (int c = bt; c < chunks; c += NBUILD) {
-    int x, h;
-    chunk_xh(c, x, h);
-    const int K = x + rho;
+    const int h = c / rows, x = c - h * rows;
     uint4 vh = make_uint4(0, 0, 0, 0), vl = vh;
-    if (K < 2 * C.m) {
-      const float* src = cb + pidx(64 * K + 8 * h);
+    if (x < 2 * C.m) {
+      const float* src = cb + pidx(64 * x + 8 * h);
       const float4 u0 = *reinterpret_cast<const float4*>(src);
       const float4 u1 = *reinterpret_cast<const float4*>(src + 4);
       const float v[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
       split8(v, 1.f, vh, vl);
     }
-    *reinterpret_cast<uint4*>(hi + 16 * c) = vh;
-    if (want_lo) *reinterpret_cast<uint4*>(lo + 16 * c) = vl;
+    const uint32_t off = (uint32_t)h * b_lbo(rows) + 16u * (uint32_t)x;
+    *reinterpret_cast<uint4*>(hi + off) = vh;
+    if (want_lo) *reinterpret_cast<uint4*>(lo + off) = vl;
   }
 }
 
@@ -407,115 +411,109 @@ enum TileMode { CONV_SYM = 0, CONV_X = 1, CORR = 2 };
 // Issue the MMAs of one tile (one thread).  three_prod selects the
 // 3-product arithmetic, otherwise the 2-product symmetric convolution.
 __device__ __forceinline__ void issue_tile(Ctx& C, int st, uint32_t b_hi, uint32_t b_lo,
-                                           const Tile& T, bool three_prod) {
+                                           uint32_t b_lbo_bytes, const Tile& T, bool three_prod) {
   const uint32_t a_hi = smem_u32(C.stages + st * STAGE_BYTES);
   const uint32_t a_lo = a_hi + PLANE;
-  const uint32_t bh0 = b_hi + (uint32_t)(T.x0 >> 3) * B_SBO;
-  const uint32_t bl0 = b_lo + (uint32_t)(T.x0 >> 3) * B_SBO;
+  const uint32_t bh0 = b_hi + 16u * (uint32_t)T.x0;
+  const uint32_t bl0 = b_lo + 16u * (uint32_t)T.x0;
   const uint32_t id = idesc_bf16(T.N);
   const uint32_t d = C.tmem + (uint32_t)T.dcol;
 #pragma unroll
   for (int kc = 0; kc < KSTEPS; ++kc) {
+    // K16 step kc = K groups 2kc, 2kc+1
     const uint64_t ah = sdesc(a_hi + kc * 256, 128, 128);
-    const uint64_t bh = sdesc(bh0 + kc * 256, 128, B_SBO);
+    const uint64_t bh = sdesc(bh0 + 2u * kc * b_lbo_bytes, b_lbo_bytes, 128);
     mma_bf16(d, ah, bh, id, 1u);
     if (C.three) {
       const uint64_t al = sdesc(a_lo + kc * 256, 128, 128);
       mma_bf16(d, al, bh, id, 1u);
       if (three_prod) {
-        const uint64_t bl = sdesc(bl0 + kc * 256, 128, B_SBO);
+        const uint64_t bl = sdesc(bl0 + 2u * kc * b_lbo_bytes, b_lbo_bytes, 128);
         mma_bf16(d, ah, bl, id, 1u);
       }
     }
   }
 }
 
-// Run the tiles w = 0, 2, ..., dmax in residue classes w mod 8 through the
-// warp-specialised pipeline.  Ends with every MMA of the sequence complete
-// (bar_done) and the accumulator readable by all warps.
-//   wsrc: padded shared heights (windows; the copies too for CONV_SYM);
+// Run the tiles w = 0, 2, ..., dmax through the warp-specialised pipeline:
+// the builders write the phase's B copy once (one copy slot), then a window
+// per tile into the stage ring.  Ends with every MMA of the sequence
+// complete (bar_done) and the accumulator readable by all warps.
+//   wsrc: padded shared heights (windows; the copy too for CONV_SYM);
 //   bsrc / blen: the copy source of CONV_X (see build_conv_copy) or the
 //   padded shared weights of CORR.
 template <int MODE>
 __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen,
-                          unsigned int* status) {
+                                          unsigned int* status) {
   constexpr bool corr = MODE == CORR;
   constexpr bool three_prod = MODE != CONV_SYM;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool want_lo = three_prod && C.three;
   const float lsc = MODE == CONV_SYM ? 2.f : 1.f;
   const int m = C.m;
-  const int lo_off = (corr ? C.rcc : C.rc) * 128;   // lo plane after hi (one-slot modes)
+  const int rows = corr ? C.rcc : C.rc;
+  const uint32_t lbo = b_lbo(rows);
   int st = C.st_next;
   if (warp == MMA_WARP) {
     if (lane == 0) {
       fence_after();
       const int cb_cols = corr_n(m);
-      for (int rho = 0; rho < 8 && rho <= C.dmax; rho += 2) {
-        const int slot = MODE == CONV_SYM ? ((rho >> 1) & 1) : 0;
-        if (!wait_phase(C, &C.bc_full[slot], (C.bc_ph >> slot) & 1u, status)) break;
-        C.bc_ph ^= 1u << slot;
-        const uint32_t bbase = smem_u32(C.bc) + (uint32_t)slot * C.rc * 128u;
-        const uint32_t blo = bbase + (uint32_t)lo_off;
-        bool ok = true;
-        for (int w = rho; w <= C.dmax; w += 8) {
-          Tile T;
-          if (corr) {
-            T.dcol = col_corr(m);
-            T.x0 = w - rho;
-            T.N = cb_cols;
-          } else {
-            const int off = (w / DG) * DG, t = off - w;
-            T.dcol = COL_CONV + off;
-            T.x0 = t + rho + ZP;
-            T.N = round_up(m - t, 16);
-          }
-          if (!wait_phase(C, &C.full[st], (C.ph >> st) & 1u, status)) { ok = false; break; }
-          C.ph ^= 1u << st;
-          fence_after();
-          issue_tile(C, st, bbase, blo, T, three_prod);
-          mma_commit(&C.empty[st]);
-          st = (st + 1 == STAGES) ? 0 : st + 1;
+      bool ok = wait_phase(C, &C.bc_full[0], C.bc_ph & 1u, status);
+      C.bc_ph ^= 1u;
+      const uint32_t bbase = smem_u32(C.bc);
+      const uint32_t blo = bbase + (uint32_t)rows * 128u;
+      for (int w = 0; ok && w <= C.dmax; w += 2) {
+        Tile T;
+        if (corr) {
+          T.dcol = col_corr(m);
+          T.x0 = w;
+          T.N = cb_cols;
+        } else {
+          const int off = (w / DG) * DG, t = off - w;
+          T.dcol = COL_CONV + off;
+          T.x0 = t + ZP;
+          T.N = round_up(m - t, 16);
         }
-        mma_commit(&C.bc_empty[slot]);
-        if (!ok) break;
+        if (!wait_phase(C, &C.full[st], (C.ph >> st) & 1u, status)) { ok = false; break; }
+        C.ph ^= 1u << st;
+        fence_after();
+        issue_tile(C, st, bbase, blo, lbo, T, three_prod);
+        mma_commit(&C.empty[st]);
+        st = (st + 1 == STAGES) ? 0 : st + 1;
       }
+      mma_commit(&C.bc_empty[0]);
       mma_commit(C.bar_done);
     }
     __syncwarp();
   } else {
     const int bt = threadIdx.x - (warp > MMA_WARP ? 32 : 0);   // 0 .. NBUILD-1
-    for (int rho = 0; rho < 8 && rho <= C.dmax; rho += 2) {
-      const int slot = MODE == CONV_SYM ? ((rho >> 1) & 1) : 0;
-      if ((C.bc_started >> slot) & 1u) {
-        if (!wait_phase(C, &C.bc_empty[slot], (C.bc_ph >> slot) & 1u, status)) break;
-        C.bc_ph ^= 1u << slot;
-      }
-      C.bc_started |= 1u << slot;
-      unsigned char* hi = C.bc + (size_t)slot * C.rc * 128;
-      if (corr) build_corr_copy(C, bsrc, rho, want_lo, bt);
-      else if (MODE == CONV_X) build_conv_copy(C, bsrc, blen, rho, hi, hi + lo_off, want_lo, bt);
-      else build_conv_copy(C, wsrc, -1, rho, hi, hi, false, bt);
+    bool ok = true;
+    if ((C.bc_started & 1u) && !wait_phase(C, &C.bc_empty[0], C.bc_ph & 1u, status)) ok = false;
+    if (C.bc_started & 1u) C.bc_ph ^= 1u;
+    C.bc_started |= 1u;
+    if (ok) {
+      unsigned char* hi = C.bc;
+      if (corr) build_corr_copy(C, bsrc, want_lo, bt);
+      else if (MODE == CONV_X) build_conv_copy(C, bsrc, blen, hi, hi + (size_t)rows * 128, want_lo, bt);
+      else build_conv_copy(C, wsrc, -1, hi, hi, false, bt);
       fence_async_smem();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&C.bc_full[slot]);
-      bool ok = true;
-      for (int w = rho; w <= C.dmax; w += 8) {
-        if ((C.started >> st) & 1u) {
-          if (!wait_phase(C, &C.empty[st], (C.ph >> st) & 1u, status)) {
-            ok = false;
-            break;
-          }
-          C.ph ^= 1u << st;
+      if (lane == 0) mbar_arrive(&C.bc_full[0]);
+    }
+    for (int w = 0; ok && w <= C.dmax; w += 2) {
+      if ((C.started >> st) & 1u) {
+        if (!wait_phase(C, &C.empty[st], (C.ph >> st) & 1u, status)) {
+          ok = false;
+          break;
         }
-        C.started |= 1u << st;
-        build_window(C, st, wsrc, w, lsc, bt);
-        fence_async_smem();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&C.full[st]);
-        st = (st + 1 == STAGES) ? 0 : st + 1;
+        C.ph ^= 1u << st;
       }
-      if (!ok) break;
+      C.started |= 1u << st;
+      build_window(C, st, wsrc, w, lsc, bt);
+      fence_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&C.full[st]);
+      st = (st + 1 == STAGES) ? 0 : st + 1;
     }
   }
   C.st_next = st;
