@@ -535,63 +535,94 @@ struct Lane {
   }
 };
 
-// b = a * a into X (padded layout, k < 2n-1): the two cells of each k are
-// combined through X.  Ends synchronised.  Returns the largest b_k the
-// calling thread finalised (every k is finalised by exactly one thread).
+// Column chunks [c0, c1) of an accumulator, warp half h taking chunks
+// c0 + h, c0 + h + 2, ...: visit(c, v, 0) gets chunk c's 32 values (one
+// load and wait per chunk; batching two chunks per wait raised the register
+// pressure of the fused step and ran slower).
+template <typename Visit>
+__device__ __forceinline__ void for_chunks(uint32_t lanebase, int half, int c0, int c1,
+                                           Visit&& visit) {
+  for (int c = c0 + half; c < c1; c += 2) {
+    float v[32];
+    tmem_ld32(lanebase + (uint32_t)(32 * c), v);
+    visit(c, v, 0);
+  }
+}
+
+// b = a * a into X (padded layout, k < 2n-1).  Each k is the sum of two
+// cells, (k mod 64, k / 64) in lanes 0-63 and (k mod 64 + 64, k / 64 - 1) in
+// lanes 64-127, read by different warps: the upper lanes write their cells to
+// X, the lower lanes add theirs.  Three rounds overlap the two: the upper
+// lanes write the first half of the columns, then the second half while the
+// lower lanes finish the first, then the lower lanes finish the second.
+// Ends synchronised.  Returns the largest b_k the calling thread finalised
+// (every k is finalised by exactly one thread).
 __device__ __forceinline__ float gather_conv(Ctx& C, const Lane& ln, float* X) {
   const int nb = 2 * C.n - 1, nch = (2 * C.m + 1 + 31) / 32;
-  const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16);
-  if (ln.quad >= 2) {
-    if (ln.half == 0) X[pidx(ln.r - 64)] = 0.f;          // k < 64 has one cell only
-    for (int c = ln.half; c < nch; c += 2) {
-      float v[32];
-      tmem_ld32(lanebase + (uint32_t)(COL_CONV + 32 * c), v);
-#pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int k = 64 * (32 * c + t) + ln.r;             // cell (r, col) -> k = 64 col + r
-        if (k < nb) X[pidx(k)] = v[t];
-      }
-    }
-  }
-  __syncthreads();
+  const int mid = (nch + 1) / 2;                        // first half: chunks [0, mid)
+  const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)COL_CONV;
+  const bool upper = ln.quad >= 2;
   float mloc = 0.f;
-  if (ln.quad < 2) {
-    for (int c = ln.half; c < nch; c += 2) {
-      float v[32];
-      tmem_ld32(lanebase + (uint32_t)(COL_CONV + 32 * c), v);
+  for (int round = 0; round < 3; ++round) {
+    if (upper && round < 2) {
+      if (round == 0 && ln.half == 0) X[pidx(ln.r - 64)] = 0.f;   // k < 64: one cell only
+      for_chunks(lanebase, ln.half, round == 0 ? 0 : mid, round == 0 ? mid : nch,
+                 [&](int c, const float (&v)[32], int o) {
 #pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int k = 64 * (32 * c + t) + ln.r;
-        if (k < nb) {
-          const float b = X[pidx(k)] + v[t];
-          X[pidx(k)] = b;
-          mloc = fmaxf(mloc, b);
-        }
-      }
+                   for (int t = 0; t < 32; ++t) {
+                     const int k = 64 * (32 * c + t) + ln.r;   // cell (r, col): k = 64 col + r
+                     if (k < nb) X[pidx(k)] = v[o + t];
+                   }
+                 });
     }
+    if (!upper && round > 0) {
+      for_chunks(lanebase, ln.half, round == 1 ? 0 : mid, round == 1 ? mid : nch,
+                 [&](int c, const float (&v)[32], int o) {
+#pragma unroll
+                   for (int t = 0; t < 32; ++t) {
+                     const int k = 64 * (32 * c + t) + ln.r;
+                     if (k < nb) {
+                       const float b = X[pidx(k)] + v[o + t];
+                       X[pidx(k)] = b;
+                       mloc = fmaxf(mloc, b);
+                     }
+                   }
+                 });
+    }
+    __syncthreads();
   }
-  __syncthreads();
   return mloc;
 }
 
-// G_i into Y (padded layout, i < n) from the correlation accumulator.
+// G_i into Y (padded layout, i < n) from the correlation accumulator: cell
+// (r, col) holds a part of i = 64 col + 63 - r; the upper-lane cell of i sits
+// one column right of its lower-lane cell, so the rounds run the halves in
+// the opposite order to gather_conv.
 __device__ __forceinline__ void gather_corr(Ctx& C, const Lane& ln, float* Y) {
   const int n = C.n, nch = (corr_n(C.m) + 31) / 32;
+  const int mid = (nch + 1) / 2;
   const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)col_corr(C.m);
-  for (int pass = 0; pass < 2; ++pass) {
-    if ((pass == 0) == (ln.quad >= 2)) {
-      for (int c = ln.half; c < nch; c += 2) {
-        float v[32];
-        tmem_ld32(lanebase + (uint32_t)(32 * c), v);
+  const bool upper = ln.quad >= 2;
+  for (int round = 0; round < 3; ++round) {
+    if (upper && round < 2) {
+      for_chunks(lanebase, ln.half, round == 0 ? mid : 0, round == 0 ? nch : mid,
+                 [&](int c, const float (&v)[32], int o) {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
-          const int i = 64 * (32 * c + t) + 63 - ln.r;   // cell (r, col) -> i = 64 col + 63 - r
-          if (i >= 0 && i < n) {
-            if (pass == 0) Y[pidx(i)] = v[t];
-            else Y[pidx(i)] += v[t];
-          }
-        }
-      }
+                   for (int t = 0; t < 32; ++t) {
+                     const int i = 64 * (32 * c + t) + 63 - ln.r;
+                     if (i >= 0 && i < n) Y[pidx(i)] = v[o + t];
+                   }
+                 });
+    }
+    if (!upper && round > 0) {
+      for_chunks(lanebase, ln.half, round == 1 ? mid : 0, round == 1 ? nch : mid,
+                 [&](int c, const float (&v)[32], int o) {
+#pragma unroll
+                   for (int t = 0; t < 32; ++t) {
+                     const int i = 64 * (32 * c + t) + 63 - ln.r;
+                     if (i >= 0 && i < n) Y[pidx(i)] += v[o + t];
+                   }
+                 });
     }
     __syncthreads();
   }
