@@ -75,28 +75,36 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
     if (!conv_tc(C, S.sa, status)) break;
     const float M = block_max(gather_conv(C, ln, S.cb), S.red);   // b in cb
     if (!(M > 0.f)) break;
-    // c_k = (1+d)^(p-1) in place, R = sum c_k (1+d), d = (b_k - M)/M
-    // (four independent k per pass for instruction-level parallelism; each
-    // thread still adds its terms in k order)
+    // c_k = (1+d)^(p-1), R = sum c_k (1+d), d = (b_k - M)/M, written straight
+    // into the correlation's B copy: thread q takes chunks (row x, K group h)
+    // = the 8 weights from 64 x + 8 h on (8 independent k per chunk), rows
+    // beyond the 2m weight blocks are zero
     float rloc = 0.f;
     const float invM = 1.f / M, q = pexp - 1.f;
-    for (int k0 = threadIdx.x; k0 < nb; k0 += 4 * NTHREADS) {
-      float d4[4], c4[4];
+    {
+      const int rows = C.rcc, nch8 = rows * 8;
+      for (int cq = threadIdx.x; cq < nch8; cq += NTHREADS) {
+        const int h = cq / rows, x = cq - h * rows;
+        const int k0 = 64 * x + 8 * h;
+        float v[8];
+        if (k0 < nb) {
+          const float4 u0 = *reinterpret_cast<const float4*>(S.cb + pidx(k0));
+          const float4 u1 = *reinterpret_cast<const float4*>(S.cb + pidx(k0) + 4);
+          const float bv[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int k = k0 + u * NTHREADS;
-        d4[u] = k < nb ? (S.cb[pidx(k)] - M) * invM : -1.f;
-      }
+          for (int j = 0; j < 8; ++j) {
+            const float d = (bv[j] - M) * invM;
+            const float cw = (k0 + j < nb && d > -1.f) ? pow_from_d_fast(d, q) : 0.f;
+            rloc += cw * (1.f + d);
+            v[j] = cw;
+          }
+        } else {
 #pragma unroll
-      for (int u = 0; u < 4; ++u) c4[u] = d4[u] > -1.f ? pow_from_d_fast(d4[u], q) : 0.f;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int k = k0 + u * NTHREADS;
-        if (k < nb) {
-          rloc += c4[u] * (1.f + d4[u]);
-          S.cb[pidx(k)] = c4[u];
+          for (int j = 0; j < 8; ++j) v[j] = 0.f;
         }
+        corr_copy_chunk(C, x, h, v);
       }
+      fence_async_smem();
     }
     const float R = block_sum(rloc, S.red);      // barrier: weights complete
     b1t *= beta1;
@@ -119,8 +127,8 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
     }
     fence_before();
     __syncthreads();
-    if (!corr_tc(C, S.sa, S.cb, status)) break;
-    gather_corr(C, ln, S.cb);                     // G in cb (weights no longer needed)
+    if (!corr_tc_prebuilt(C, S.sa, status)) break;
+    gather_corr(C, ln, S.cb);                     // G in cb
 
     // Adam / mirror step (cells i = thread + u * NTHREADS)
     float sloc = 0.f;

@@ -442,7 +442,7 @@ __device__ __forceinline__ void issue_tile(Ctx& C, int st, uint32_t b_hi, uint32
 //   wsrc: padded shared heights (windows; the copy too for CONV_SYM);
 //   bsrc / blen: the copy source of CONV_X (see build_conv_copy) or the
 //   padded shared weights of CORR.
-template <int MODE>
+template <int MODE, bool PREBUILT = false>
 __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen,
                                           unsigned int* status) {
   constexpr bool corr = MODE == CORR;
@@ -493,7 +493,9 @@ __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float
     C.bc_started |= 1u;
     if (ok) {
       unsigned char* hi = C.bc;
-      if (corr) build_corr_copy(C, bsrc, want_lo, bt);
+      if (PREBUILT) {
+        // the copy was written (and fenced) by the caller before this phase
+      } else if (corr) build_corr_copy(C, bsrc, want_lo, bt);
       else if (MODE == CONV_X) build_conv_copy(C, bsrc, blen, hi, hi + (size_t)rows * 128, want_lo, bt);
       else build_conv_copy(C, wsrc, -1, hi, hi, false, bt);
       fence_async_smem();
@@ -641,6 +643,22 @@ __device__ __forceinline__ bool convx_tc(Ctx& C, const float* sa, const float* y
 __device__ __forceinline__ bool corr_tc(Ctx& C, const float* sa, const float* cb,
                                         unsigned int* status) {
   return run_tiles<CORR>(C, sa, cb, 0, status);
+}
+// the same with the B copy already in place (corr_copy_chunk, then
+// fence_async_smem and a barrier by the writers)
+__device__ __forceinline__ bool corr_tc_prebuilt(Ctx& C, const float* sa, unsigned int* status) {
+  return run_tiles<CORR, true>(C, sa, nullptr, 0, status);
+}
+
+// Write chunk (row x, K group h) of the correlation copy: the weights
+// c[64 x + 8 h + j], j < 8, as hi and lo planes (layout of build_corr_copy).
+__device__ __forceinline__ void corr_copy_chunk(Ctx& C, int x, int h, const float (&v)[8]) {
+  const int rows = C.rcc;
+  uint4 vh, vl;
+  split8(v, 1.f, vh, vl);
+  const uint32_t off = (uint32_t)h * b_lbo(rows) + 16u * (uint32_t)x;
+  *reinterpret_cast<uint4*>(C.bc + off) = vh;
+  if (C.three) *reinterpret_cast<uint4*>(C.bc + (size_t)rows * 128 + off) = vl;
 }
 
 }  // namespace tc
