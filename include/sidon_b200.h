@@ -209,6 +209,19 @@ SIDON_API int sidon_coarsen(const void* src, int n2, int P, void* dst, int dtype
 SIDON_API int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, int k_migrate,
                          int* order_out, void* stream);
 
+/* fp64 polish of the elite: K candidates (device fp64 [K][n], usually small
+ * perturbations of the best vector), `passes` passes of iters/passes fp64
+ * Adam steps with p from 200*4^q to 30x that and lr from 0.01*0.45^q to
+ * 0.02x that (pass q); after each pass the certifying evaluation (fit[K],
+ * nactive[K] with active tolerance 1e-6, nactive may be NULL) and, if the
+ * pass's best F is below *best_F (device double, set by the caller), that
+ * candidate's heights are copied to best_a (device [n]) and *best_F updated.
+ * mom/vel: fp64 [K][n] scratch.  Stream-ordered, no host round trip.
+ * Replaces the polish of src/main.cu:798-874 (6 passes there). */
+SIDON_API int sidon_polish(double* pop, double* mom, double* vel, int n, int K, int iters,
+                           int passes, double* fit, int* nactive, double* best_a,
+                           double* best_F, void* stream);
+
 /* ---------------------------- large candidates -----------------------------
  * Candidates longer than one CTA's shared memory (the ladder's 16384,
  * 32768, 65536, ...): the heights are cut into super-blocks of q cells (a

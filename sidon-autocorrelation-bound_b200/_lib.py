@@ -43,6 +43,7 @@ SIGNATURES = {
     "sidon_refine": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "sidon_coarsen": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "sidon_island_migrate": (_i, [_vp, _i, _vp, _i, _i, _i, _vp, _vp]),
+    "sidon_polish": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "sidon_large_workspace_bytes": (_sz, [_i, _i, _i, _i]),
     "sidon_autotune_large": (_i, [_i, _i, _i, _vp, _vp]),
     "sidon_local_search_large": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _d,

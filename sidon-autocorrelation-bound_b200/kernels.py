@@ -266,6 +266,46 @@ def island_migrate(pop: torch.Tensor, fit: torch.Tensor, n_islands: int, k: int 
     return order
 
 
+# ------------------------------- fp64 polish -------------------------------
+def polish_population(best_a, K: int = 8, seed: int = 0) -> np.ndarray:
+    """The polish's starting candidates (src/main.cu:810-821): candidate 0 is
+    the best vector, candidate k > 0 multiplies every height by
+    exp(0.003 (1 + k mod 8) z) with z standard normal (basin hopping), all
+    clipped at 0 and normalised to sum 1.  z comes from numpy's PCG64 with
+    the given seed (the reference draws it from std::mt19937_64)."""
+    a = np.asarray(best_a, dtype=np.float64)
+    rng = np.random.Generator(np.random.PCG64(np.random.SeedSequence([int(seed), 0xABCDEF])))
+    out = np.empty((K, a.size))
+    for k in range(K):
+        x = a.copy()
+        if k:
+            x = x * np.exp(0.003 * (1 + (k % 8)) * rng.standard_normal(a.size))
+        x = np.maximum(x, 0.0)
+        out[k] = x / x.sum()
+    return out
+
+
+def polish(best_a, K: int = 8, iters: int = 40000, passes: int = 6, seed: int = 0,
+           best_F: float | None = None, device="cuda", stream=None):
+    """fp64 polish of the elite (src/main.cu:798-874) on the device: returns
+    (best heights, best F, per-candidate F after the last pass).  best_F
+    (default: the certifying F of best_a) is what a pass must beat."""
+    a = np.asarray(best_a, dtype=np.float64)
+    n = a.size
+    pop = torch.as_tensor(polish_population(a, K, seed), device=device)
+    mom, vel = torch.empty_like(pop), torch.empty_like(pop)
+    fit = torch.empty(K, dtype=torch.float64, device=device)
+    nact = torch.empty(K, dtype=torch.int32, device=device)
+    best = torch.as_tensor(a, device=device).clone()
+    if best_F is None:
+        best_F = run_eval(best[None, :], with_nactive=False)[0].item()
+    bF = torch.tensor([float(best_F)], dtype=torch.float64, device=device)
+    _lib.call("sidon_polish", pop.data_ptr(), mom.data_ptr(), vel.data_ptr(), n, int(K),
+              int(iters), int(passes), fit.data_ptr(), nact.data_ptr(), best.data_ptr(),
+              bF.data_ptr(), _stream(stream))
+    return best.cpu().numpy(), bF.item(), fit.cpu().numpy()
+
+
 # ----------------------------- large candidates ----------------------------
 def autotune_large(n: int, P: int, precision: str = "bf16x3") -> tuple[int, float]:
     """Measure and remember the fastest schedule for (n, P): returns (q, ms

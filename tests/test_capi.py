@@ -105,3 +105,20 @@ def test_synth_is_deterministic_and_shaped():
     assert np.all(L[:, g0: g0 + 840] == 0)
     frac0 = np.mean(L == 0)
     assert 0.3 < frac0 < 0.5
+
+
+def test_polish_population_shape_and_norm():
+    """Basin-hopping start of the polish: candidate 0 is the input, the rest
+    are bounded multiplicative perturbations; all non-negative, sum 1."""
+    from sidon_b200 import kernels
+    rng = np.random.default_rng(0)
+    a = rng.uniform(0, 1, 200)
+    a[::3] = 0
+    pop = kernels.polish_population(a, 8, seed=2)
+    assert pop.shape == (8, 200)
+    np.testing.assert_allclose(pop[0], a / a.sum(), rtol=0, atol=0)
+    assert (pop >= 0).all()
+    np.testing.assert_allclose(pop.sum(1), 1.0, rtol=1e-12)
+    assert (pop[:, ::3] == 0).all()                 # zeros stay zero
+    r = pop[1:, 1::3] / (a[1::3] / a.sum())
+    assert np.abs(np.log(r)).max() < 0.3            # bounded perturbation
