@@ -209,6 +209,33 @@ SIDON_API int sidon_coarsen(const void* src, int n2, int P, void* dst, int dtype
 SIDON_API int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, int k_migrate,
                          int* order_out, void* stream);
 
+/* Variation operators of the memetic loop: offspring j (one per row of
+ * out, device [n_off][n] of dtype) is operator op[j] applied to parents
+ * p1[j], p2[j] (rows of pop) with strength[j], then renormalised to sum 1:
+ * 0 blend crossover, 1 two-point segment crossover, 2 log-normal
+ * multiplicative noise, 3 smooth low-frequency perturbation, 4 additive
+ * gaussian noise, 5 sparsify, 6 reflect / symmetrise, 7 shift, 8 block
+ * splice from p2, 9 fresh smooth random restart, 10 spike injection,
+ * 11 structured seed (endpoint atom, plateau, depression, hump, band, hard
+ * gap, terminal spike), 12 gap surgery, 13 endpoint atom; any other id
+ * clones p1.  Randomness: Philox4x32-10 keyed by seed, counters by
+ * (gen, offspring, element) -- reproducible per element, not the
+ * reference's curand streams.  out must not overlap pop.
+ * Replaces kVariation<T> (src/kernels.cuh:558-801, launched at
+ * src/main.cu:737-741). */
+SIDON_API int sidon_variation(const void* pop, void* out, int dtype, int n, int n_off,
+                              const int* p1, const int* p2, const int* op,
+                              const float* strength, unsigned long long seed,
+                              unsigned long long gen, void* stream);
+
+/* Support signature per candidate: sig[p] = xor over the indices i with
+ * a_i > tol * mean(a) of a mixed hash of i (equal supports, equal
+ * signatures), nnz[p] = their count.  Replaces kSupportSig<T> + runSig
+ * (src/kernels.cuh:803-849, src/main.cu:180-184; the reference's tol is
+ * 0.02). */
+SIDON_API int sidon_support_sig(const void* pop, int dtype, int n, int P, float tol,
+                                unsigned long long* sig, int* nnz, void* stream);
+
 /* fp64 polish of the elite: K candidates (device fp64 [K][n], usually small
  * perturbations of the best vector), `passes` passes of iters/passes fp64
  * Adam steps with p from 200*4^q to 30x that and lr from 0.01*0.45^q to

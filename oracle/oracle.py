@@ -47,6 +47,10 @@ _SIG = {
     "so_coarsen_f64": (None, [_vp, _i, _i, _vp]),
     "so_island_migrate_f32": (_i, [_vp, _i, _vp, _i, _i, _i, _vp]),
     "so_resample_f32": (None, [_vp, _i, _vp, _i]),
+    "so_philox4x32": (None, [_vp, _vp, _vp]),
+    "so_variation_f32": (None, [_vp, _vp, _i, _i, _vp, _vp, _vp, _vp, C.c_ulonglong,
+                                C.c_ulonglong]),
+    "so_support_sig_f32": (None, [_vp, _i, _i, _f, _vp, _vp]),
     "so_island_migrate_ragged_f32": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp]),
     "so_certify_exact": (_d, [_vp, _i, _vp, _vp, _vp]),
     "so_exact_bk": (_d, [_vp, _i, _i]),
@@ -269,6 +273,34 @@ def island_migrate_ragged(flat, offsets, fit, NI, k):
     if rc:
         raise ValueError(f"island_migrate_ragged: bad arguments ({rc})")
     return flat, fit, order
+
+
+def philox4x32(ctr, key):
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.empty(4, np.uint32)
+    lib().so_philox4x32(c.ctypes.data, k.ctypes.data, out.ctypes.data)
+    return out
+
+
+def variation(pop, p1, p2, op, strength, seed, gen):
+    pop = _c(pop, np.float32)
+    P, n = pop.shape
+    p1, p2, op = (_c(x, np.int32) for x in (p1, p2, op))
+    st = _c(strength, np.float32)
+    out = np.empty((op.size, n), np.float32)
+    lib().so_variation_f32(pop.ctypes.data, out.ctypes.data, n, op.size, p1.ctypes.data,
+                           p2.ctypes.data, op.ctypes.data, st.ctypes.data, int(seed), int(gen))
+    return out
+
+
+def support_sig(pop, tol=0.02):
+    pop = _c(pop, np.float32)
+    P, n = pop.shape
+    sig = np.empty(P, np.uint64)
+    nnz = np.empty(P, np.int32)
+    lib().so_support_sig_f32(pop.ctypes.data, n, P, float(tol), sig.ctypes.data, nnz.ctypes.data)
+    return sig, nnz
 
 
 def certify_exact(a):

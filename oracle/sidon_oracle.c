@@ -669,3 +669,248 @@ SO_EXPORT int so_num_threads(void) {
   return 1;
 #endif
 }
+
+
+/* ========================= variation + support signature ================= */
+/* Test oracle for csrc/variation.cu, which follows the operator semantics of
+ * src/kernels.cuh:558-849 with its own random streams.  Philox4x32-10 is the
+ * published counter-based generator (Salmon, Moraes, Dror, Shaw, SC 2011);
+ * the known-answer vectors of its authors pin this restatement. */
+SO_EXPORT void so_philox4x32(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n1 = (uint32_t)p1;
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1, n3 = (uint32_t)p0;
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+static float var_u01(uint32_t w) { return ((float)(w >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+static void var_params(unsigned long long seed, unsigned long long gen, int j, float* u) {
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  for (int q = 0; q < 16; ++q) {
+    const uint32_t c[4] = {(uint32_t)q, (uint32_t)j, (uint32_t)gen, (uint32_t)(gen >> 32) << 1};
+    uint32_t r[4];
+    so_philox4x32(c, key, r);
+    for (int t = 0; t < 4; ++t) u[4 * q + t] = var_u01(r[t]);
+  }
+}
+static float var_normal(unsigned long long seed, unsigned long long gen, int j, int i) {
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  const uint32_t c[4] = {(uint32_t)i, (uint32_t)j, (uint32_t)gen,
+                         ((uint32_t)(gen >> 32) << 1) | 1u};
+  uint32_t r[4];
+  so_philox4x32(c, key, r);
+  const double a = (double)var_u01(r[0]), b = (double)var_u01(r[1]);
+  return (float)(sqrt(-2.0 * log(a)) * cos(6.283185307179586 * b));
+}
+/* the kernels' fixed-order fp64 block sum: 256 strided partial sums, a
+ * 32-lane xor butterfly per warp (lane 0's value), warps added in order */
+static double var_sum(const double* x, int n, int stride) {
+  double part[256];
+  for (int t = 0; t < 256; ++t) {
+    double s = 0.0;
+    for (int i = t; i < n; i += 256) s += x[(size_t)i * stride];
+    part[t] = s;
+  }
+  double r = 0.0;
+  for (int w = 0; w < 8; ++w) {
+    double v[32], nv[32];
+    for (int l = 0; l < 32; ++l) v[l] = part[32 * w + l];
+    for (int off = 16; off > 0; off >>= 1) {
+      for (int l = 0; l < 32; ++l) nv[l] = v[l] + v[l ^ off];
+      memcpy(v, nv, sizeof v);
+    }
+    r += v[0];
+  }
+  return r;
+}
+static double var_mean_f32(const float* A, int n) {
+  double* x = (double*)malloc(sizeof(double) * (size_t)n);
+  for (int i = 0; i < n; ++i) x[i] = (double)A[i];
+  const double m = var_sum(x, n, 1) / (double)n;
+  free(x);
+  return m;
+}
+SO_EXPORT void so_variation_f32(const float* pop, float* out, int n, int n_off, const int* p1,
+                                const int* p2, const int* opv, const float* strength,
+                                unsigned long long seed, unsigned long long gen) {
+  float u[64];
+  const float fn = (float)n;
+  for (int j = 0; j < n_off; ++j) {
+    const float* A = pop + (size_t)p1[j] * n;
+    const float* B = pop + (size_t)p2[j] * n;
+    float* O = out + (size_t)j * n;
+    const float sg = strength[j];
+    var_params(seed, gen, j, u);
+    switch (opv[j]) {
+      case 0: {
+        const float lam = -0.3f + 1.6f * u[0];
+        for (int i = 0; i < n; ++i) { const float x = lam * A[i] + (1.f - lam) * B[i]; O[i] = x > 0.f ? x : 0.f; }
+        break;
+      }
+      case 1: {
+        int c1 = (int)(u[1] * fn), c2 = (int)(u[2] * fn);
+        if (c1 > c2) { const int t = c1; c1 = c2; c2 = t; }
+        for (int i = 0; i < n; ++i) O[i] = (i >= c1 && i < c2) ? B[i] : A[i];
+        break;
+      }
+      case 2:
+        for (int i = 0; i < n; ++i) O[i] = A[i] * expf(sg * var_normal(seed, gen, j, i));
+        break;
+      case 3: {
+        const int nf = 1 + (int)(u[3] * 5.0f);
+        for (int i = 0; i < n; ++i) {
+          float m = 0.f;
+          for (int f = 0; f < nf; ++f) {
+            const float freq = 1.0f + u[4 + f] * 12.0f, ph = 6.2831853f * u[12 + f];
+            m += cosf(6.2831853f * freq * (float)i / fn + ph) / (float)nf;
+          }
+          const float x = A[i] * (1.0f + sg * 3.0f * m);
+          O[i] = x > 0.f ? x : 0.f;
+        }
+        break;
+      }
+      case 4: {
+        const float mean = (float)var_mean_f32(A, n);
+        for (int i = 0; i < n; ++i) {
+          const float x = A[i] + sg * mean * var_normal(seed, gen, j, i);
+          O[i] = x > 0.f ? x : 0.f;
+        }
+        break;
+      }
+      case 5: {
+        const float mean = (float)var_mean_f32(A, n);
+        const float thr = mean * (0.05f + 0.9f * u[20]);
+        for (int i = 0; i < n; ++i) O[i] = A[i] < thr ? 0.f : A[i];
+        break;
+      }
+      case 6: {
+        const int hard = u[21] < 0.5f;
+        for (int i = 0; i < n; ++i) O[i] = hard ? A[n - 1 - i] : 0.5f * (A[i] + A[n - 1 - i]);
+        break;
+      }
+      case 7: {
+        const int sh = (int)((u[22] - 0.5f) * fn * 0.25f);
+        for (int i = 0; i < n; ++i) { const int k = i - sh; O[i] = (k >= 0 && k < n) ? A[k] : 0.f; }
+        break;
+      }
+      case 8: {
+        const int len = 1 + (int)(u[23] * 0.5f * fn);
+        const int st0 = (int)(u[24] * (float)(n - len > 0 ? n - len : 1));
+        for (int i = 0; i < n; ++i) O[i] = (i >= st0 && i < st0 + len) ? B[i] : A[i];
+        break;
+      }
+      case 9: {
+        const int nf = 2 + (int)(u[25] * 6.0f);
+        const float base = 0.3f + 0.7f * u[26];
+        for (int i = 0; i < n; ++i) {
+          float m = 0.f;
+          for (int f = 0; f < nf; ++f) {
+            const float freq = 1.0f + u[4 + (f % 8)] * 10.0f, ph = 6.2831853f * u[12 + (f % 8)];
+            m += cosf(6.2831853f * freq * (float)i / fn + ph);
+          }
+          const float val = base + m / (float)nf + 0.4f * var_normal(seed, gen, j, i);
+          O[i] = val > 0.f ? val : 0.f;
+        }
+        break;
+      }
+      case 10: {
+        const int loc = (int)(u[27] * fn), wdt = 1 + (int)(u[28] * fn * 0.03f);
+        const float mean = (float)var_mean_f32(A, n);
+        const float amp = mean * (1.0f + 6.0f * u[29]);
+        for (int i = 0; i < n; ++i) { float x = A[i]; if (i >= loc - wdt && i <= loc + wdt) x += amp; O[i] = x; }
+        break;
+      }
+      case 11: {
+        const int flip = u[30] < 0.5f;
+        const float atom = 30.f + 250.f * u[31];
+        const float pl1 = 0.28f + 0.16f * u[32];
+        const float pl2 = pl1 + 0.10f + 0.14f * u[33];
+        const float hump = pl2 + 0.02f + 0.08f * u[34];
+        const float gap0 = 0.70f + 0.16f * u[35];
+        const float gap1 = gap0 + 0.05f + 0.15f * u[36];
+        const float tail = 3.0f + 14.0f * u[37];
+        const int nf = 3 + (int)(u[38] * 6.f);
+        for (int i = 0; i < n; ++i) {
+          const int d = flip ? (n - 1 - i) : i;
+          const float x = ((float)d + 0.5f) / fn;
+          float rough = 0.f;
+          for (int f = 0; f < nf; ++f)
+            rough += cosf(6.2831853f * (2.f + u[40 + f] * 40.f) * x + 6.2831853f * u[48 + f]);
+          rough /= (float)nf;
+          float v;
+          if (x < pl1) v = 4.2f * (1.f + 0.45f * rough);
+          else if (x < pl2) v = 0.7f * (1.f + 0.80f * rough);
+          else if (x < hump) v = 5.2f * (1.f + 0.30f * rough);
+          else if (x < gap0) v = 2.0f * (1.f + 0.70f * rough);
+          else if (x < gap1) v = 0.f;
+          else v = tail * (1.f + 0.20f * rough);
+          if (d == 0) v += atom;
+          else if (d < 4) v += atom * 0.10f / (float)d;
+          O[i] = v > 0.f ? v : 0.f;
+        }
+        break;
+      }
+      case 12: {
+        const float mean = (float)var_mean_f32(A, n);
+        const int len = 1 + (int)((0.015f + 0.13f * u[30]) * fn);
+        const int st0 = (int)(u[31] * (float)(n > len ? n - len : 1));
+        const int carve = u[32] < 0.7f;
+        const float fill = mean * (0.2f + 1.8f * u[33]);
+        for (int i = 0; i < n; ++i) {
+          float x = A[i];
+          if (i >= st0 && i < st0 + len) x = carve ? 0.f : (x + fill);
+          O[i] = x;
+        }
+        break;
+      }
+      case 13: {
+        const float mean = (float)var_mean_f32(A, n);
+        const int left = u[30] < 0.5f;
+        const int w = 1 + (int)(u[31] * 0.012f * fn);
+        const float add = mean * (-20.f + 260.f * u[32]);
+        for (int i = 0; i < n; ++i) {
+          const int d = left ? i : (n - 1 - i);
+          float x = A[i];
+          if (d < w) { x += add / (float)(1 + d); if (x < 0.f) x = 0.f; }
+          O[i] = x;
+        }
+        break;
+      }
+      default:
+        for (int i = 0; i < n; ++i) O[i] = A[i];
+        break;
+    }
+    double* x = (double*)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; ++i) x[i] = (double)O[i];
+    const double S = var_sum(x, n, 1);
+    free(x);
+    if (S > 0.0) {
+      const float inv = (float)(1.0 / S);
+      for (int i = 0; i < n; ++i) O[i] *= inv;
+    } else {
+      for (int i = 0; i < n; ++i) O[i] = 1.f / (float)n;
+    }
+  }
+}
+SO_EXPORT void so_support_sig_f32(const float* pop, int n, int P, float tol,
+                                  unsigned long long* sig, int* nnz) {
+  for (int p = 0; p < P; ++p) {
+    const float* a = pop + (size_t)p * n;
+    const double thr = var_mean_f32(a, n) * (double)tol;
+    unsigned long long h = 0ull;
+    int c = 0;
+    for (int i = 0; i < n; ++i)
+      if ((double)a[i] > thr) {
+        ++c;
+        unsigned long long x = (unsigned long long)i * 0x9E3779B97F4A7C15ull;
+        x ^= x >> 29; x *= 0xBF58476D1CE4E5B9ull; x ^= x >> 32;
+        h ^= x;
+      }
+    sig[p] = h;
+    nnz[p] = c;
+  }
+}

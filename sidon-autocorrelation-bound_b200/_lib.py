@@ -43,6 +43,9 @@ SIGNATURES = {
     "sidon_refine": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "sidon_coarsen": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "sidon_island_migrate": (_i, [_vp, _i, _vp, _i, _i, _i, _vp, _vp]),
+    "sidon_variation": (_i, [_vp, _vp, _i, _i, _i, _vp, _vp, _vp, _vp, C.c_ulonglong,
+                             C.c_ulonglong, _vp]),
+    "sidon_support_sig": (_i, [_vp, _i, _i, _i, _f, _vp, _vp, _vp]),
     "sidon_polish": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "sidon_large_workspace_bytes": (_sz, [_i, _i, _i, _i]),
     "sidon_autotune_large": (_i, [_i, _i, _i, _vp, _vp]),

@@ -28,6 +28,11 @@ NVCC_FLAGS = [
 ]
 
 
+# the variation operators keep each product and sum rounded on its own (no
+# fused multiply-add), so a host restatement reproduces them bit for bit
+PER_FILE_FLAGS = {"variation.cu": ["--fmad=false"]}
+
+
 def nvcc() -> str:
     for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
         if cand and pathlib.Path(cand).exists():
@@ -37,7 +42,8 @@ def nvcc() -> str:
 
 def _compile(src: pathlib.Path, verbose: bool) -> pathlib.Path:
     obj = BUILD / (src.stem + ".o")
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *PER_FILE_FLAGS.get(src.name, []), "-c", str(src), "-o",
+           str(obj)]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -71,6 +71,11 @@ int launch_island_migrate(float* pop, int n, double* fit, int P, int NI, int k, 
 int launch_island_migrate_ragged(float* pop, const long long* offsets, double* fit, int P, int NI,
                                  int k, int* order, cudaStream_t st);
 int launch_ragged_order(const long long* offsets, int P, int* order, cudaStream_t st);
+int launch_variation(const void* pop, void* out, int dtype, int n, int n_off, const int* p1,
+                     const int* p2, const int* op, const float* strength,
+                     unsigned long long seed, unsigned long long gen, cudaStream_t st);
+int launch_support_sig(const void* pop, int dtype, int n, int P, float tol,
+                       unsigned long long* sig, int* nnz, cudaStream_t st);
 
 static thread_local int g_last_cuda = 0;
 
@@ -404,6 +409,27 @@ int sidon_certify_large(const void* pop, int dtype, int n, int P, double* out_F,
   if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
   return launch_certify_large(pop, dtype, n, P, out_F, out_M, out_S, out_kmax, workspace,
                               S(stream));
+}
+
+int sidon_variation(const void* pop, void* out, int dtype, int n, int n_off, const int* p1,
+                    const int* p2, const int* op, const float* strength, unsigned long long seed,
+                    unsigned long long gen, void* stream) {
+  int rc = pre(n, n_off);
+  if (rc) return rc;
+  if (n_off == 0) return SIDON_OK;
+  if (!pop || !out || !p1 || !p2 || !op || !strength || pop == out) return SIDON_ERR_ARG;
+  if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
+  return launch_variation(pop, out, dtype, n, n_off, p1, p2, op, strength, seed, gen, S(stream));
+}
+
+int sidon_support_sig(const void* pop, int dtype, int n, int P, float tol,
+                      unsigned long long* sig, int* nnz, void* stream) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P == 0) return SIDON_OK;
+  if (!pop || !sig || !nnz) return SIDON_ERR_ARG;
+  if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
+  return launch_support_sig(pop, dtype, n, P, tol, sig, nnz, S(stream));
 }
 
 int sidon_ragged_order(const long long* offsets, int P, int* order_out, void* stream) {

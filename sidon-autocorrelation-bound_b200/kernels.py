@@ -266,6 +266,42 @@ def island_migrate(pop: torch.Tensor, fit: torch.Tensor, n_islands: int, k: int 
     return order
 
 
+# ------------------------- variation and signatures -------------------------
+VARIATION_OPS = {
+    "blend": 0, "segment": 1, "lognormal": 2, "smooth": 3, "gaussian": 4, "sparsify": 5,
+    "reflect": 6, "shift": 7, "splice": 8, "restart": 9, "spike": 10, "structured": 11,
+    "gap": 12, "atom": 13, "clone": 20,
+}
+
+
+def variation(pop: torch.Tensor, p1, p2, op, strength, seed: int, gen: int,
+              out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """Offspring of the variation operators (kVariation, src/kernels.cuh:558-801):
+    row j = operator op[j] on parents p1[j], p2[j] with strength[j], sum 1."""
+    n, P = _pop_shape(pop)
+    dev = pop.device
+    p1, p2, op = (torch.as_tensor(x, dtype=torch.int32, device=dev).contiguous()
+                  for x in (p1, p2, op))
+    st = torch.as_tensor(strength, dtype=torch.float32, device=dev).contiguous()
+    if out is None:
+        out = torch.empty((op.numel(), n), dtype=pop.dtype, device=dev)
+    _lib.call("sidon_variation", _dev(pop, "pop"), _dev(out, "out", pop.dtype),
+              _dtype_code(pop), n, op.numel(), p1.data_ptr(), p2.data_ptr(), op.data_ptr(),
+              st.data_ptr(), int(seed) & (2**64 - 1), int(gen) & (2**64 - 1), _stream(stream))
+    return out
+
+
+def support_sig(pop: torch.Tensor, tol: float = 0.02, stream=None):
+    """(signature uint64 as int64 [P], nnz int32 [P]) (kSupportSig + runSig,
+    src/kernels.cuh:803-849, src/main.cu:180-184)."""
+    n, P = _pop_shape(pop)
+    sig = torch.empty(P, dtype=torch.int64, device=pop.device)
+    nnz = torch.empty(P, dtype=torch.int32, device=pop.device)
+    _lib.call("sidon_support_sig", _dev(pop, "pop"), _dtype_code(pop), n, P, float(tol),
+              sig.data_ptr(), nnz.data_ptr(), _stream(stream))
+    return sig, nnz
+
+
 # ------------------------------- fp64 polish -------------------------------
 def polish_population(best_a, K: int = 8, seed: int = 0) -> np.ndarray:
     """The polish's starting candidates (src/main.cu:810-821): candidate 0 is

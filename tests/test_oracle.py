@@ -217,3 +217,45 @@ def test_oracle_ragged_migration_rules(orc):
     # untouched rows keep their values and fitness
     np.testing.assert_array_equal(out[off[0]:off[1]], flat[off[0]:off[1]])
     assert f2[0] == 1.0 and f2[5] == 0.1
+
+
+def test_oracle_philox_known_answers(orc):
+    """Philox4x32-10 against its authors' known-answer vectors (Random123)."""
+    cases = [
+        ([0, 0, 0, 0], [0, 0], [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]),
+        ([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2, [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]),
+        ([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0],
+         [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]),
+    ]
+    for ctr, key, want in cases:
+        assert orc.philox4x32(ctr, key).tolist() == want
+
+
+def test_oracle_variation_semantics(orc):
+    """Operator meanings on the oracle: clone copies, reflect reverses (or
+    symmetrises), segment/splice take cells from the right parent, every
+    offspring sums to 1 and is non-negative."""
+    rng = np.random.default_rng(4)
+    pop = rng.uniform(0, 1, (3, 50)).astype(np.float32)
+    ops = list(range(14)) + [20]
+    J = len(ops)
+    out = orc.variation(pop, [0] * J, [1] * J, ops, [0.2] * J, seed=7, gen=3)
+    assert (out >= 0).all()
+    np.testing.assert_allclose(out.sum(1), 1.0, rtol=1e-5)
+    clone = out[ops.index(20)]
+    np.testing.assert_allclose(clone, pop[0] / pop[0].sum(dtype=np.float64), rtol=1e-6)
+    refl = out[6]
+    hard = np.allclose(refl, (pop[0][::-1] / pop[0].sum()), rtol=1e-5)
+    soft = np.allclose(refl, 0.5 * (pop[0] + pop[0][::-1]) / pop[0].sum(), rtol=1e-5)
+    assert hard or soft
+    for k in (1, 8):                       # each cell from one parent, then one common scale
+        ok = False
+        for c in (out[k][0] / pop[0][0], out[k][0] / pop[1][0]):
+            from_a = np.isclose(out[k], c * pop[0], rtol=1e-5)
+            from_b = np.isclose(out[k], c * pop[1], rtol=1e-5)
+            ok = ok or bool(np.all(from_a | from_b))
+        assert ok, k
+    sig, nnz = orc.support_sig(np.array([[0, 1, 0, 2, 0, 3]], np.float32), tol=0.02)
+    assert nnz[0] == 3 and sig[0] != 0
+    sig2, _ = orc.support_sig(np.array([[0, 5, 0, 1, 0, 9]], np.float32), tol=0.02)
+    assert sig2[0] == sig[0]                # same support, same signature
