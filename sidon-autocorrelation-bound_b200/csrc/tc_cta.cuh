@@ -5,7 +5,7 @@
 //
 //  Shared memory (see Layout):
 //    stages  STAGES x 6 KB   Hankel windows (hi | lo planes)
-//    bc      B-matrix copies: two conv slots (hi) or one hi|lo pair; after a
+//    bc      the tile phase's B-matrix copy (hi, or hi | lo); after a
 //            tile phase, gather scratch for up to 2n-1 outputs
 //    sa      fp32 heights, padded block layout (cell i at i + 4 floor(i/64)),
 //            zero margins on both sides
@@ -31,7 +31,8 @@ struct Layout {
     size_t o = (size_t)STAGES * STAGE_BYTES;
     off_bc = o;
     const int rows = rcc > rc ? rcc : rc;
-    // two conv slots or one hi|lo pair; after a tile phase, gather scratch
+    // one B copy (hi, or hi|lo) of up to max(rc, rcc) rows; after a tile
+    // phase, gather scratch
     // for up to 2n-1 outputs in the padded layout
     const size_t region = (size_t)2 * rows * 128;
     o += region > (size_t)cb_len * 4 ? region : (size_t)cb_len * 4;

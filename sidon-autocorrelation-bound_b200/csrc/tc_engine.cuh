@@ -201,11 +201,11 @@ constexpr int NBUILD = NBUILD_WARPS * 32;
 // of a role are kept identical by every thread of that role.
 struct Ctx {
   unsigned char* stages;   // STAGES x (hi plane | lo plane), 1 KB aligned
-  unsigned char* bc;       // B-matrix copies (two conv slots or one corr hi|lo pair)
+  unsigned char* bc;       // the phase's B-matrix copy (hi plane, lo plane after it)
   uint64_t* full;          // STAGES "window ready" barriers (NBUILD_WARPS arrivals)
   uint64_t* empty;         // STAGES "window consumed" barriers (tcgen05.commit)
-  uint64_t* bc_full;       // 2 "copy ready" barriers (NBUILD_WARPS arrivals)
-  uint64_t* bc_empty;      // 2 "copy consumed" barriers (tcgen05.commit)
+  uint64_t* bc_full;       // "copy ready" barrier (NBUILD_WARPS arrivals; [0] used)
+  uint64_t* bc_empty;      // "copy consumed" barrier (tcgen05.commit; [0] used)
   uint64_t* bar_done;      // "all MMAs of a phase done"
   uint32_t tmem;           // TMEM base address (512 columns)
   // pipeline phases as bit masks (registers, no dynamic indexing): bit s of
