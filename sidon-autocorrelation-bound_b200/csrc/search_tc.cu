@@ -65,6 +65,7 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
   const float lnPr = (float)log((double)pEnd / (double)pStart);
   const float lnLr = (float)log((double)lrEnd / (double)lrStart);
   float b1t = 1.f, b2t = 1.f;
+  bool copy_ready = false;   // the autoconvolution copy of sa is in place
 
   for (int it = 0; it < iters; ++it) {
     const float frac = iters > 1 ? (float)it / (float)(iters - 1) : 0.f;
@@ -72,7 +73,7 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
     const float lr = lrStart * expf(lnLr * frac);
 
     prime(C, true);
-    if (!conv_tc(C, S.sa, status)) break;
+    if (!(copy_ready ? conv_tc_prebuilt(C, S.sa, status) : conv_tc(C, S.sa, status))) break;
     const float M = block_max(gather_conv(C, ln, S.cb), S.red);   // b in cb
     if (!(M > 0.f)) break;
     // c_k = (1+d)^(p-1), R = sum c_k (1+d), d = (b_k - M)/M, written straight
@@ -157,13 +158,41 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
       S.sa[pidx(i)] = x;
       sloc += x;
     }
-    float Ssum = block_sum(sloc, S.red);
-    if (!(Ssum > 0.f)) {
-      for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] = 1.f / (float)n;
-      Ssum = 1.f;
+    // renormalise (sum <= 0: the uniform 1/n), chunk by chunk of 8 cells,
+    // and write the next step's autoconvolution B copy from the same chunks
+    const float Ssum = block_sum(sloc, S.red);
+    const bool reset = !(Ssum > 0.f);
+    const float inv = 1.f / (reset ? 1.f : Ssum);
+    const float uniform = 1.f / (float)n;
+    {
+      const int rows = C.rc;
+      for (int cq = threadIdx.x; cq < rows * 8; cq += NTHREADS) {
+        const int h = cq / rows, x = cq - h * rows, J = x - ZP;
+        float v[8];
+        if (J >= 0 && J < C.m) {
+          const int c0 = 64 * J + 56 - 8 * h;
+          float* q = S.sa + pidx(c0);
+          float4 u0 = *reinterpret_cast<float4*>(q);
+          float4 u1 = *reinterpret_cast<float4*>(q + 4);
+          float w[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            if (c0 + j < n) w[j] = (reset ? uniform : w[j]) * inv;
+          u0 = make_float4(w[0], w[1], w[2], w[3]);
+          u1 = make_float4(w[4], w[5], w[6], w[7]);
+          *reinterpret_cast<float4*>(q) = u0;
+          *reinterpret_cast<float4*>(q + 4) = u1;
+#pragma unroll
+          for (int t = 0; t < 8; ++t) v[t] = w[7 - t];
+        } else {
+#pragma unroll
+          for (int t = 0; t < 8; ++t) v[t] = 0.f;
+        }
+        conv_copy_chunk(C, x, h, v);
+      }
+      fence_async_smem();
     }
-    const float inv = 1.f / Ssum;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] *= inv;
+    copy_ready = true;
     __syncthreads();
   }
   __syncthreads();

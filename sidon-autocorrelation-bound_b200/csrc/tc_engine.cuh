@@ -634,6 +634,18 @@ __device__ __forceinline__ void gather_corr(Ctx& C, const Lane& ln, float* Y) {
 __device__ __forceinline__ bool conv_tc(Ctx& C, const float* sa, unsigned int* status) {
   return run_tiles<CONV_SYM>(C, sa, nullptr, 0, status);
 }
+// the same with the B copy already in place (conv_copy_chunk, then
+// fence_async_smem and a barrier by the writers)
+__device__ __forceinline__ bool conv_tc_prebuilt(Ctx& C, const float* sa, unsigned int* status) {
+  return run_tiles<CONV_SYM, true>(C, sa, nullptr, 0, status);
+}
+// Write chunk (row x, K group h) of the autoconvolution copy (hi plane):
+// v[s] = a[64 (x - ZP) + 63 - 8 h - s], s < 8 (layout of build_conv_copy).
+__device__ __forceinline__ void conv_copy_chunk(Ctx& C, int x, int h, const float (&v)[8]) {
+  uint4 vh, vl;
+  split8(v, 1.f, vh, vl);
+  *reinterpret_cast<uint4*>(C.bc + (uint32_t)h * b_lbo(C.rc) + 16u * (uint32_t)x) = vh;
+}
 // b = a * y (accumulator at COL_CONV); y: a plain global row of ylen cells
 __device__ __forceinline__ bool convx_tc(Ctx& C, const float* sa, const float* y, int ylen,
                                          unsigned int* status) {
