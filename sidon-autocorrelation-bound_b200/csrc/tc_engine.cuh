@@ -301,9 +301,18 @@ __device__ __forceinline__ void build_conv_copy(Ctx& C, const float* y, int ylen
         v[0] = u1.w; v[1] = u1.z; v[2] = u1.y; v[3] = u1.x;
         v[4] = u0.w; v[5] = u0.z; v[6] = u0.y; v[7] = u0.x;
       } else {
-        const int c0 = 64 * J + 63 - 8 * h;
+        // cells base .. base + 7 (base a multiple of 8): two 16-byte loads
+        // when the row allows, else one load per cell
+        const int base = 64 * J + 56 - 8 * h;
+        if (base + 8 <= ylen && (reinterpret_cast<uintptr_t>(y + base) & 15) == 0) {
+          const float4 u0 = __ldcg(reinterpret_cast<const float4*>(y + base));
+          const float4 u1 = __ldcg(reinterpret_cast<const float4*>(y + base + 4));
+          v[0] = u1.w; v[1] = u1.z; v[2] = u1.y; v[3] = u1.x;
+          v[4] = u0.w; v[5] = u0.z; v[6] = u0.y; v[7] = u0.x;
+        } else {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = (c0 - j < ylen) ? __ldcg(y + (c0 - j)) : 0.f;
+          for (int j = 0; j < 8; ++j) v[j] = (base + 7 - j < ylen) ? __ldcg(y + (base + 7 - j)) : 0.f;
+        }
       }
       split8(v, 1.f, vh, vl);
     }
