@@ -31,6 +31,142 @@ __device__ unsigned int g_status_word = 0u;   // SIDON_ERR_TIMEOUT after a timed
 constexpr int kCellsPerThread = 38;
 
 // ------------------------------ local search ------------------------------
+// One L^p-Adam / mirror step of the candidate resident in S (n cells; its
+// Adam moments in the global rows mg, vg): convolution, max, weights written
+// into the correlation copy, correlation, update, renormalisation, and the
+// next step's autoconvolution copy (copy_ready).  b1t / b2t are beta^(step+1).
+// Returns 0, or 1 when M <= 0 stops the anneal (nothing changed), or 2 when a
+// tile phase was aborted.  Ends synchronised.
+__device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, int mode,
+                                            float pexp, float lr, float beta1, float beta2,
+                                            float b1t, float b2t, float* mg, float* vg,
+                                            bool& copy_ready, unsigned int* status) {
+  Ctx& C = S.C;
+  const int nb = 2 * n - 1;
+  prime(C, true);
+  if (!(copy_ready ? conv_tc_prebuilt(C, S.sa, status) : conv_tc(C, S.sa, status))) return 2;
+  const float M = block_max(gather_conv(C, ln, S.cb), S.red);   // b in cb
+  if (!(M > 0.f)) return 1;
+  // c_k = (1+d)^(p-1), R = sum c_k (1+d), d = (b_k - M)/M, written straight
+  // into the correlation's B copy: thread q takes chunks (row x, K group h)
+  // = the 8 weights from 64 x + 8 h on (8 independent k per chunk), rows
+  // beyond the 2m weight blocks are zero
+  float rloc = 0.f;
+  const float invM = 1.f / M, q = pexp - 1.f;
+  {
+    const int rows = C.rcc, nch8 = rows * 8;
+    for (int cq = threadIdx.x; cq < nch8; cq += NTHREADS) {
+      const int h = cq / rows, x = cq - h * rows;
+      const int k0 = 64 * x + 8 * h;
+      float v[8];
+      if (k0 < nb) {
+        const float4 u0 = *reinterpret_cast<const float4*>(S.cb + pidx(k0));
+        const float4 u1 = *reinterpret_cast<const float4*>(S.cb + pidx(k0) + 4);
+        const float bv[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const float d = (bv[j] - M) * invM;
+          const float cw = (k0 + j < nb && d > -1.f) ? pow_from_d_fast(d, q) : 0.f;
+          rloc += cw * (1.f + d);
+          v[j] = cw;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = 0.f;
+      }
+      corr_copy_chunk(C, x, h, v);
+    }
+    fence_async_smem();
+  }
+  const float R = block_sum(rloc, S.red);      // barrier: weights complete
+  const float bc1 = 1.f / (1.f - b1t), bc2 = 1.f / (1.f - b2t);
+  const float lrn = lr / (float)n;
+
+  // the Adam moments of this thread's cells, loaded now so that the
+  // correlation phase hides their L2 / HBM latency
+  float pm[kCellsPerThread], pv[kCellsPerThread];
+  if (mode == 0) {
+#pragma unroll
+    for (int u = 0; u < kCellsPerThread; ++u) {
+      const int i = threadIdx.x + u * NTHREADS;
+      if (i < n) {
+        pm[u] = __ldcg(mg + i);
+        pv[u] = __ldcg(vg + i);
+      }
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (!corr_tc_prebuilt(C, S.sa, status)) return 2;
+  gather_corr(C, ln, S.cb);                     // G in cb
+
+  // Adam / mirror step (cells i = thread + u * NTHREADS)
+  float sloc = 0.f;
+  const float invR = 1.f / R;
+#pragma unroll
+  for (int u = 0; u < kCellsPerThread; ++u) {
+    const int i = threadIdx.x + u * NTHREADS;
+    if (i >= n) continue;
+    const float gi = S.cb[pidx(i)] * invR - M;
+    const float x0 = S.sa[pidx(i)];
+    float x;
+    if (mode == 0) {
+      const float mm = __fmaf_rn(beta1, pm[u], (1.f - beta1) * gi);
+      const float vv = __fmaf_rn(beta2, pv[u], (1.f - beta2) * gi * gi);
+      mg[i] = mm;
+      vg[i] = vv;
+      const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
+      x = x0 - step;
+      if (x < 0.f) x = 0.f;
+    } else {
+      float e = -lr * (gi * invM);
+      if (e > 4.f) e = 4.f;
+      if (e < -4.f) e = -4.f;
+      x = x0 * __expf(e);
+    }
+    S.sa[pidx(i)] = x;
+    sloc += x;
+  }
+  // renormalise (sum <= 0: the uniform 1/n), chunk by chunk of 8 cells,
+  // and write the next step's autoconvolution B copy from the same chunks
+  const float Ssum = block_sum(sloc, S.red);
+  const bool reset = !(Ssum > 0.f);
+  const float inv = 1.f / (reset ? 1.f : Ssum);
+  const float uniform = 1.f / (float)n;
+  {
+    const int rows = C.rc;
+    for (int cq = threadIdx.x; cq < rows * 8; cq += NTHREADS) {
+      const int h = cq / rows, x = cq - h * rows, J = x - ZP;
+      float v[8];
+      if (J >= 0 && J < C.m) {
+        const int c0 = 64 * J + 56 - 8 * h;
+        float* q = S.sa + pidx(c0);
+        float4 u0 = *reinterpret_cast<float4*>(q);
+        float4 u1 = *reinterpret_cast<float4*>(q + 4);
+        float w[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (c0 + j < n) w[j] = (reset ? uniform : w[j]) * inv;
+        u0 = make_float4(w[0], w[1], w[2], w[3]);
+        u1 = make_float4(w[4], w[5], w[6], w[7]);
+        *reinterpret_cast<float4*>(q) = u0;
+        *reinterpret_cast<float4*>(q + 4) = u1;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) v[t] = w[7 - t];
+      } else {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) v[t] = 0.f;
+      }
+      conv_copy_chunk(C, x, h, v);
+    }
+    fence_async_smem();
+  }
+  copy_ready = true;
+  __syncthreads();
+  return 0;
+}
+
+
 // Candidates: uniform rows of n_fixed cells (offsets == NULL) or a ragged
 // batch (row p = pop[offsets[p] .. offsets[p+1])).  CTA b runs slots
 // b, b + gridDim.x, ... of `order` (NULL = 0..P-1): launched with one CTA per
@@ -58,7 +194,6 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
   float* mg = mom + off;
   float* vg = vel + off;
   begin(S, n, n_max);
-  const int nb = 2 * n - 1;
   for (int i = threadIdx.x; i < n; i += blockDim.x) { S.sa[pidx(i)] = a[i]; mg[i] = 0.f; vg[i] = 0.f; }
   __syncthreads();
 
@@ -72,132 +207,127 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
     const float pexp = pStart * expf(lnPr * frac);
     const float lr = lrStart * expf(lnLr * frac);
 
-    prime(C, true);
-    if (!(copy_ready ? conv_tc_prebuilt(C, S.sa, status) : conv_tc(C, S.sa, status))) break;
-    const float M = block_max(gather_conv(C, ln, S.cb), S.red);   // b in cb
-    if (!(M > 0.f)) break;
-    // c_k = (1+d)^(p-1), R = sum c_k (1+d), d = (b_k - M)/M, written straight
-    // into the correlation's B copy: thread q takes chunks (row x, K group h)
-    // = the 8 weights from 64 x + 8 h on (8 independent k per chunk), rows
-    // beyond the 2m weight blocks are zero
-    float rloc = 0.f;
-    const float invM = 1.f / M, q = pexp - 1.f;
-    {
-      const int rows = C.rcc, nch8 = rows * 8;
-      for (int cq = threadIdx.x; cq < nch8; cq += NTHREADS) {
-        const int h = cq / rows, x = cq - h * rows;
-        const int k0 = 64 * x + 8 * h;
-        float v[8];
-        if (k0 < nb) {
-          const float4 u0 = *reinterpret_cast<const float4*>(S.cb + pidx(k0));
-          const float4 u1 = *reinterpret_cast<const float4*>(S.cb + pidx(k0) + 4);
-          const float bv[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const float d = (bv[j] - M) * invM;
-            const float cw = (k0 + j < nb && d > -1.f) ? pow_from_d_fast(d, q) : 0.f;
-            rloc += cw * (1.f + d);
-            v[j] = cw;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 8; ++j) v[j] = 0.f;
-        }
-        corr_copy_chunk(C, x, h, v);
-      }
-      fence_async_smem();
-    }
-    const float R = block_sum(rloc, S.red);      // barrier: weights complete
     b1t *= beta1;
     b2t *= beta2;
-    const float bc1 = 1.f / (1.f - b1t), bc2 = 1.f / (1.f - b2t);
-    const float lrn = lr / (float)n;
-
-    // the Adam moments of this thread's cells, loaded now so that the
-    // correlation phase hides their L2 / HBM latency
-    float pm[kCellsPerThread], pv[kCellsPerThread];
-    if (mode == 0) {
-#pragma unroll
-      for (int u = 0; u < kCellsPerThread; ++u) {
-        const int i = threadIdx.x + u * NTHREADS;
-        if (i < n) {
-          pm[u] = mg[i];
-          pv[u] = vg[i];
-        }
-      }
-    }
-    fence_before();
-    __syncthreads();
-    if (!corr_tc_prebuilt(C, S.sa, status)) break;
-    gather_corr(C, ln, S.cb);                     // G in cb
-
-    // Adam / mirror step (cells i = thread + u * NTHREADS)
-    float sloc = 0.f;
-    const float invR = 1.f / R;
-#pragma unroll
-    for (int u = 0; u < kCellsPerThread; ++u) {
-      const int i = threadIdx.x + u * NTHREADS;
-      if (i >= n) continue;
-      const float gi = S.cb[pidx(i)] * invR - M;
-      const float x0 = S.sa[pidx(i)];
-      float x;
-      if (mode == 0) {
-        const float mm = __fmaf_rn(beta1, pm[u], (1.f - beta1) * gi);
-        const float vv = __fmaf_rn(beta2, pv[u], (1.f - beta2) * gi * gi);
-        mg[i] = mm;
-        vg[i] = vv;
-        const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
-        x = x0 - step;
-        if (x < 0.f) x = 0.f;
-      } else {
-        float e = -lr * (gi * invM);
-        if (e > 4.f) e = 4.f;
-        if (e < -4.f) e = -4.f;
-        x = x0 * __expf(e);
-      }
-      S.sa[pidx(i)] = x;
-      sloc += x;
-    }
-    // renormalise (sum <= 0: the uniform 1/n), chunk by chunk of 8 cells,
-    // and write the next step's autoconvolution B copy from the same chunks
-    const float Ssum = block_sum(sloc, S.red);
-    const bool reset = !(Ssum > 0.f);
-    const float inv = 1.f / (reset ? 1.f : Ssum);
-    const float uniform = 1.f / (float)n;
-    {
-      const int rows = C.rc;
-      for (int cq = threadIdx.x; cq < rows * 8; cq += NTHREADS) {
-        const int h = cq / rows, x = cq - h * rows, J = x - ZP;
-        float v[8];
-        if (J >= 0 && J < C.m) {
-          const int c0 = 64 * J + 56 - 8 * h;
-          float* q = S.sa + pidx(c0);
-          float4 u0 = *reinterpret_cast<float4*>(q);
-          float4 u1 = *reinterpret_cast<float4*>(q + 4);
-          float w[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
-#pragma unroll
-          for (int j = 0; j < 8; ++j)
-            if (c0 + j < n) w[j] = (reset ? uniform : w[j]) * inv;
-          u0 = make_float4(w[0], w[1], w[2], w[3]);
-          u1 = make_float4(w[4], w[5], w[6], w[7]);
-          *reinterpret_cast<float4*>(q) = u0;
-          *reinterpret_cast<float4*>(q + 4) = u1;
-#pragma unroll
-          for (int t = 0; t < 8; ++t) v[t] = w[7 - t];
-        } else {
-#pragma unroll
-          for (int t = 0; t < 8; ++t) v[t] = 0.f;
-        }
-        conv_copy_chunk(C, x, h, v);
-      }
-      fence_async_smem();
-    }
-    copy_ready = true;
-    __syncthreads();
+    const int rs = lp_adam_step(S, ln, n, mode, pexp, lr, beta1, beta2, b1t, b2t, mg, vg,
+                                copy_ready, status);
+    if (rs) break;
   }
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = S.sa[pidx(i)];
   }  // candidates
+  teardown(S);
+}
+
+// ------------------- local search, balanced step segments -------------------
+// A uniform batch of P > G candidates (G = one resident CTA per SM) leaves SMs
+// idle in the last wave of the one-CTA-per-candidate kernel (256 candidates on
+// 148 SMs: 1.73 waves of work in 2 waves of time).  This kernel lays the P
+// chains of `iters` steps end to end and gives CTA c the steps
+// [c T / G, (c+1) T / G) of that sequence (T = P iters): at most three
+// pieces -- the head of the candidate that continues into the next CTA's
+// segment, whole candidates, the tail of the candidate begun by the previous
+// CTA.  It runs the head first and raises that candidate's flag, and the tail
+// last after waiting for its flag; as a segment holds at least `iters` steps
+// (P >= G), the head is finished long before the next CTA reaches the tail,
+// so the wait is a formality.  Heights and moments cross between CTAs through
+// L2 (ld.global.cg); each step is lp_adam_step, the fused kernel's arithmetic,
+// so every candidate's trajectory is the fused kernel's bit for bit.  The
+// flags are reset by the host before each launch; the wait gives up after
+// ~2^31 cycles (SIDON_ERR_TIMEOUT).
+constexpr int kMaxSegCandidates = 1 << 16;
+__device__ unsigned int g_seg_flags[kMaxSegCandidates];
+
+// steps [s0, s1) of candidate pid, its state read from and written to HBM
+__device__ __forceinline__ void run_piece(Shared& S, const Lane& ln, float* pop, float* mom,
+                                          float* vel, int pid, int n, int s0, int s1, int iters,
+                                          int mode, float pStart, float lnPr, float lrStart,
+                                          float lnLr, float beta1, float beta2,
+                                          unsigned int* status) {
+  float* a = pop + (size_t)pid * n;
+  float* mg = mom + (size_t)pid * n;
+  float* vg = vel + (size_t)pid * n;
+  begin(S, n, n);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    S.sa[pidx(i)] = __ldcg(a + i);
+    if (s0 == 0) { mg[i] = 0.f; vg[i] = 0.f; }
+  }
+  __syncthreads();
+  float b1t = 1.f, b2t = 1.f;
+  for (int it = 0; it < s0; ++it) {        // beta^s0, multiplied up as the fused kernel does
+    b1t *= beta1;
+    b2t *= beta2;
+  }
+  bool copy_ready = false;
+  int rs = 0;
+  for (int it = s0; it < s1; ++it) {
+    const float frac = iters > 1 ? (float)it / (float)(iters - 1) : 0.f;
+    const float pexp = pStart * expf(lnPr * frac);
+    const float lr = lrStart * expf(lnLr * frac);
+    b1t *= beta1;
+    b2t *= beta2;
+    rs = lp_adam_step(S, ln, n, mode, pexp, lr, beta1, beta2, b1t, b2t, mg, vg, copy_ready,
+                      status);
+    if (rs) break;          // M <= 0 stops the anneal; the heights are as they were
+  }
+  __syncthreads();
+  if (rs != 2)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = S.sa[pidx(i)];
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+k_local_search_tc_seg(float* pop, float* mom, float* vel, int P, int n,
+                      const int* __restrict__ skip, const int* __restrict__ mode_arr, int iters,
+                      float pStart, float pEnd, float lrStart, float lrEnd, float beta1,
+                      float beta2, int mode_default, int three, unsigned int* status,
+                      unsigned int* flags) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ int s_ok;
+  Shared S = setup(n, three != 0, smem_raw);
+  const Lane ln;
+  const float lnPr = (float)log((double)pEnd / (double)pStart);
+  const float lnLr = (float)log((double)lrEnd / (double)lrStart);
+  const long long T = (long long)P * iters, G = gridDim.x, c = blockIdx.x;
+  const long long seg0 = c * T / G, seg1 = (c + 1) * T / G;
+  if (seg1 > seg0) {
+    const int first = (int)(seg0 / iters), last = (int)((seg1 - 1) / iters);
+    const bool tail = (long long)first * iters < seg0;                 // begun by CTA c - 1
+    const bool head = (long long)(last + 1) * iters > seg1;            // continued by CTA c + 1
+    auto piece = [&](int pid) {
+      const long long b0 = (long long)pid * iters;
+      const int s0 = (int)((seg0 > b0 ? seg0 : b0) - b0);
+      const int s1 = (int)((seg1 < b0 + iters ? seg1 : b0 + iters) - b0);
+      if (!(skip && skip[pid]) && !*((volatile int*)S.C.abort))
+        run_piece(S, ln, pop, mom, vel, pid, n, s0, s1, iters,
+                  mode_arr ? mode_arr[pid] : mode_default, pStart, lnPr, lrStart, lnLr, beta1,
+                  beta2, status);
+    };
+    if (head) {
+      piece(last);
+      __threadfence();        // every thread's heights and moments reach L2 ...
+      __syncthreads();
+      if (threadIdx.x == 0) atomicExch(&flags[last], 1u);   // ... before the flag
+    }
+    for (int pid = tail ? first + 1 : first; pid <= (head ? last - 1 : last); ++pid) piece(pid);
+    if (tail && !(head && first == last)) {
+      if (threadIdx.x == 0) {
+        s_ok = 1;
+        volatile unsigned int* f = flags + first;
+        const long long t0 = clock64();
+        while (*f == 0u) {
+          if (clock64() - t0 > kWaitCycles) {
+            s_ok = 0;
+            atomicCAS(status, 0u, (unsigned int)SIDON_ERR_TIMEOUT);
+            break;
+          }
+          __nanosleep(200);
+        }
+        __threadfence();
+      }
+      __syncthreads();
+      if (s_ok) piece(first);
+    }
+  }
   teardown(S);
 }
 
@@ -500,6 +630,48 @@ int prepare_local_search_tc(int n_max) {
   return status_word() ? SIDON_OK : SIDON_ERR_CUDA;
 }
 
+// The balanced-segment kernel, or kNotHere when it does not apply (no
+// cooperative launch, fewer resident CTAs than SMs, more candidates than
+// flags, or the stream is being captured).
+constexpr int kNotHere = -1;
+static int launch_local_search_tc_seg(float* pop, float* mom, float* vel, int P, int n,
+                                      const int* skip, const int* mode_arr, int iters, double pS,
+                                      double pE, double lrS, double lrE, double b1, double b2,
+                                      int mode_default, int precision, size_t sm,
+                                      unsigned int* sw, cudaStream_t st) {
+  int dev = 0, coop = 0, per_sm = 0;
+  if (P > tc::kMaxSegCandidates) return kNotHere;
+  if (cudaGetDevice(&dev) != cudaSuccess) return kNotHere;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
+    return kNotHere;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return kNotHere;
+  int rc = set_dyn_smem((const void*)tc::k_local_search_tc_seg, sm);
+  if (rc) return rc;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_local_search_tc_seg,
+                                                    tc::NTHREADS, sm) != cudaSuccess ||
+      per_sm < 1)
+    return kNotHere;
+  const int G = sm_count();
+  if (P < G) return kNotHere;
+  void* addr = nullptr;                    // the per-candidate flags (looked up per call)
+  cudaError_t e = cudaGetSymbolAddress(&addr, tc::g_seg_flags);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  unsigned int* flags = (unsigned int*)addr;
+  e = cudaMemsetAsync(flags, 0, (size_t)P * sizeof(unsigned int), st);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  float fpS = (float)pS, fpE = (float)pE, flS = (float)lrS, flE = (float)lrE, fb1 = (float)b1,
+        fb2 = (float)b2;
+  int three = precision == SIDON_PREC_BF16X3 ? 1 : 0;
+  void* args[] = {&pop, &mom, &vel, &P, &n, &skip, &mode_arr, &iters, &fpS, &fpE, &flS, &flE,
+                  &fb1, &fb2, &mode_default, &three, &sw, &flags};
+  e = cudaLaunchCooperativeKernel((const void*)tc::k_local_search_tc_seg, dim3(G),
+                                  dim3(tc::NTHREADS), args, sm, st);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  return SIDON_OK;
+}
+
 int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* offsets,
                            const int* order, int P, int n_fixed, int n_max, const int* skip,
                            const int* mode_arr, int iters, double pS, double pE, double lrS,
@@ -512,6 +684,14 @@ int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* 
   if (rc) return rc;
   unsigned int* sw = status_word();
   if (!sw) return SIDON_ERR_CUDA;
+  // a uniform batch larger than one wave: balanced step segments over one
+  // resident CTA per SM (not inside a stream capture)
+  if (!offsets && P > sm_count()) {
+    const int r = launch_local_search_tc_seg(pop, mom, vel, P, n_fixed, skip, mode_arr, iters,
+                                             pS, pE, lrS, lrE, b1, b2, mode_default, precision,
+                                             sm, sw, st);
+    if (r != kNotHere) return r;              // else: the one-CTA-per-candidate kernel
+  }
   // one CTA per candidate for a uniform batch; persistent (one CTA per SM)
   // for a ragged batch
   const int grid = offsets ? (P < sm_count() ? P : sm_count()) : P;

@@ -197,3 +197,34 @@ def test_tc_largest_n(cuda):
     with pytest.raises(_lib.SidonError) as ei:
         K().run_local_search(big, 1, 2.0, 4.0, 1e-3, 1e-3, precision="bf16x3")
     assert ei.value.status == _lib.ERR_N
+
+
+@pytest.mark.parametrize("iters", [1, 7, 30])
+def test_balanced_segments_equal_one_wave(cuda, iters):
+    """A uniform batch larger than the SM count runs the balanced-segment
+    kernel (step chains split across CTAs); each candidate's result equals the
+    one-wave kernel's
+    (two halves of the batch, each within one wave) bit for bit, with skips,
+    mirror-mode candidates and an all-zero candidate (M <= 0) in the batch."""
+    from sidon_b200 import synth
+    sms = torch.cuda.get_device_properties(cuda).multi_processor_count
+    P = sms + 9
+    n = 700
+    pop = synth.population("lognormal", n, P, seed=iters)
+    pop[5] = 0.0
+    skip = torch.zeros(P, dtype=torch.int32, device=cuda)
+    skip[[3, P - 1]] = 1
+    mode = torch.zeros(P, dtype=torch.int32, device=cuda)
+    mode[[2, 100]] = 1
+    whole = T(pop, cuda)
+    K().run_local_search(whole, iters, 2.0, 256.0, 1e-3, 5e-4, precision="bf16x3", skip=skip,
+                         mode_arr=mode)
+    assert _status() == 0
+    h = P // 2
+    for lo, hi in ((0, h), (h, P)):
+        part = T(pop[lo:hi], cuda)
+        K().run_local_search(part, iters, 2.0, 256.0, 1e-3, 5e-4, precision="bf16x3",
+                             skip=skip[lo:hi].contiguous(), mode_arr=mode[lo:hi].contiguous())
+        assert torch.equal(part, whole[lo:hi]), (lo, hi)
+    np.testing.assert_array_equal(whole[5].cpu().numpy(), pop[5])
+    np.testing.assert_array_equal(whole[3].cpu().numpy(), pop[3])
