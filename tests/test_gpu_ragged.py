@@ -197,3 +197,25 @@ def test_torch_graph_capture_of_ragged_step(cuda):
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(b.flat, eager)
+
+
+def test_uniform_anneal_graph_beyond_one_wave(cuda):
+    """A uniform batch larger than the SM count: the eager anneal takes the
+    balanced-segment kernel, the captured graph the one-CTA-per-candidate
+    kernel (no cooperative launch inside a capture); results are equal."""
+    from sidon_b200 import synth
+    sms = torch.cuda.get_device_properties(cuda).multi_processor_count
+    P = 4 * ((sms + 12) // 4)                      # > SMs, divisible by 4 islands
+    pop = synth.population("structured", 256, P, seed=31)
+    x1 = torch.as_tensor(pop, device=cuda)
+    x2 = torch.as_tensor(pop, device=cuda)
+    cfg = K().anneal_config(steps=40, p_start=2.0, p_end=64.0, fw_every=20, pdhg_iters=5,
+                            fw_nT=3, n_islands=4, migrate_every=20, k_migrate=1)
+    fit1 = K().anneal(x1, cfg)
+    g = K().AnnealGraph(x2, cfg)
+    g.launch()
+    torch.cuda.synchronize()
+    assert torch.equal(x1, x2)
+    assert torch.equal(fit1, g.fit)
+    g.close()
+    assert _status() == 0
