@@ -66,9 +66,12 @@ enum sidon_op {
 SIDON_API const char* sidon_status_string(int status);
 /* The cudaError_t value behind the last SIDON_ERR_CUDA on this thread. */
 SIDON_API int sidon_last_cuda_error(void);
-/* Device-side status word of the tensor-core kernels: SIDON_ERR_TIMEOUT if a
- * bounded wait inside a kernel ran out since the last reset, else SIDON_OK.
- * Synchronous (copies one word from the current device); reset != 0 clears it. */
+/* Device-side status word of the tensor-core kernels since the last reset:
+ * SIDON_ERR_TIMEOUT if a bounded wait inside a kernel ran out,
+ * SIDON_ERR_NONFINITE if a candidate's heights held NaN, Inf or a negative
+ * value (computed anyway, as the reference would), else SIDON_OK; the first
+ * event is kept.  Synchronous (copies one word from the current device);
+ * reset != 0 clears it. */
 SIDON_API int sidon_device_status(int reset);
 /* ABI version of this library (bumped on any signature change). */
 SIDON_API int sidon_abi_version(void);

@@ -31,6 +31,14 @@ __device__ unsigned int g_status_word = 0u;   // SIDON_ERR_TIMEOUT after a timed
 constexpr int kCellsPerThread = 38;
 
 // ------------------------------ local search ------------------------------
+// Heights must be finite and non-negative; a candidate that is not is
+// computed anyway (as the reference would) and SIDON_ERR_NONFINITE is
+// recorded in the status word (sidon_device_status).  bad: this thread saw one.
+__device__ __forceinline__ bool bad_height(float x) { return !(x >= 0.f && x <= 3.402823466e38f); }
+__device__ __forceinline__ void note_bad(bool bad, unsigned int* status) {
+  if (bad) atomicCAS(status, 0u, (unsigned int)SIDON_ERR_NONFINITE);
+}
+
 // One L^p-Adam / mirror step of the candidate resident in S (n cells; its
 // Adam moments in the global rows mg, vg): convolution, max, weights written
 // into the correlation copy, correlation, update, renormalisation, and the
@@ -194,7 +202,15 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
   float* mg = mom + off;
   float* vg = vel + off;
   begin(S, n, n_max);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) { S.sa[pidx(i)] = a[i]; mg[i] = 0.f; vg[i] = 0.f; }
+  bool bad = false;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float x = a[i];
+    bad |= bad_height(x);
+    S.sa[pidx(i)] = x;
+    mg[i] = 0.f;
+    vg[i] = 0.f;
+  }
+  note_bad(bad, status);
   __syncthreads();
 
   const float lnPr = (float)log((double)pEnd / (double)pStart);
@@ -248,10 +264,13 @@ __device__ __forceinline__ void run_piece(Shared& S, const Lane& ln, float* pop,
   float* mg = mom + (size_t)pid * n;
   float* vg = vel + (size_t)pid * n;
   begin(S, n, n);
+  bool bad = false;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    S.sa[pidx(i)] = __ldcg(a + i);
-    if (s0 == 0) { mg[i] = 0.f; vg[i] = 0.f; }
+    const float x = __ldcg(a + i);
+    if (s0 == 0) { bad |= bad_height(x); mg[i] = 0.f; vg[i] = 0.f; }
+    S.sa[pidx(i)] = x;
   }
+  note_bad(bad, status);
   __syncthreads();
   float b1t = 1.f, b2t = 1.f;
   for (int it = 0; it < s0; ++it) {        // beta^s0, multiplied up as the fused kernel does
@@ -354,7 +373,14 @@ k_lp_forward_tc(const float* __restrict__ pop, int n, float p, float* __restrict
   const Lane ln;
   const float* a = pop + (size_t)pid * n;
   double sl = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; S.sa[pidx(i)] = x; sl += x; }
+  bool bad = false;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float x = a[i];
+    bad |= bad_height(x);
+    S.sa[pidx(i)] = x;
+    sl += x;
+  }
+  note_bad(bad, status);
   const double Ssum = block_sum(sl, s_red);
   prime(C, false);
   const bool ok = conv_tc(C, S.sa, status);
@@ -483,7 +509,14 @@ k_frank_wolfe_tc(float* pop, float* gbuf, float* gbbuf, const long long* __restr
     begin(S, n, n_max);
     const int nb = 2 * n - 1;
     float sl = 0.f;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) { const float x = a[i]; S.sa[pidx(i)] = x; sl += x; }
+    bool bad = false;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const float x = a[i];
+      bad |= bad_height(x);
+      S.sa[pidx(i)] = x;
+      sl += x;
+    }
+    note_bad(bad, status);
     const float s0 = block_sum(sl, S.red);
     if (!(s0 > 0.f)) continue;
     {

@@ -228,3 +228,21 @@ def test_balanced_segments_equal_one_wave(cuda, iters):
         assert torch.equal(part, whole[lo:hi]), (lo, hi)
     np.testing.assert_array_equal(whole[5].cpu().numpy(), pop[5])
     np.testing.assert_array_equal(whole[3].cpu().numpy(), pop[3])
+
+
+def test_nonfinite_heights_are_reported(cuda):
+    """NaN, Inf or negative heights do not stop the kernels (or hang them):
+    the device status word reports SIDON_ERR_NONFINITE; clean input leaves
+    it at SIDON_OK."""
+    from sidon_b200 import _lib
+    assert _status() == 0
+    base = np.full((2, 300), 1.0 / 300, dtype=np.float32)
+    for bad in (np.nan, np.inf, -1e-3):
+        x = base.copy()
+        x[1, 17] = bad
+        K().run_local_search(T(x, cuda), 2, 2.0, 4.0, 1e-3, 1e-3, precision="bf16x3")
+        assert _status() == _lib.ERR_NONFINITE, bad
+        K().lp_forward(T(x, cuda), 8.0, precision="bf16x3")
+        assert _status() == _lib.ERR_NONFINITE, bad
+    K().run_local_search(T(base, cuda), 2, 2.0, 4.0, 1e-3, 1e-3, precision="bf16x3")
+    assert _status() == 0
