@@ -398,6 +398,144 @@ SIDON_API int sidon_anneal_capture(float* pop, float* mom, float* vel, const lon
 SIDON_API int sidon_graph_launch(sidon_graph graph, void* stream);
 SIDON_API int sidon_graph_destroy(sidon_graph graph);
 
+/* --------------------------- memetic generations ---------------------------
+ * One generation of the reference driver's memetic island search
+ * (src/main.cu:586-785), with its selection policy on the device so that a
+ * generation -- and any number of them -- is a fixed sequence of launches on
+ * one stream that a CUDA graph can hold:
+ *   1. anneal tiers from the operator that produced each candidate: cold
+ *      (ops 9/11, at most max(1, 0.18 P) of them, in slot order) for
+ *      cold_iters steps, p 6 -> p_max, lr 0.085 -> 0.0015; medium (the
+ *      other 9/11 and ops 5, 7, 8, 10, 12, 13) for cold_iters/3 steps,
+ *      p 40 -> p_max, lr 0.04 -> 0.001; warm (the rest) for ls_iters steps,
+ *      p 400 -> 3 p_max, lr 0.012 -> 0.0003 (main.cu:607-629); mirror
+ *      descent on every fourth island (main.cu:569-572);
+ *   2. a Frank-Wolfe step on every candidate (skipped where the step does
+ *      not fit, main.cu:633-639); fp64 evaluation; support signatures;
+ *   3. the incumbent (improvement by more than 1e-13), the level best and
+ *      the generations since it improved; the tabu table over support
+ *      signatures (best F per signature, revisits without an improvement
+ *      of 1e-12); ranking inside each island (ties by slot); every 12th
+ *      generation the best of island i over the worst of island i+1
+ *      (main.cu:641-692);
+ *   4. the offspring plan: `elite` clones per island, the rest from two
+ *      binary tournaments inside the island and an operator drawn from the
+ *      bandit weights, replaced by a diversifying operator when the
+ *      parent's signature was revisited more than tabu_tenure times without
+ *      being within 2e-4 of the incumbent, and by a restart (op 9) with
+ *      probability 0.1 once stagnation passes 0.7; strength
+ *      (0.03 + 0.35 u)(0.5 + warm)(1 + 1.5 stagnation) (main.cu:694-730);
+ *   5. variation into the workspace, copied over the population; every 10th
+ *      generation the incumbent over the worst slot of island 0
+ *      (main.cu:737-754);
+ *   6. every 5th generation the bandit credit: an operator wins when its
+ *      child beats its first parent; weights 0.85 w + 0.15 (0.15 + 3 rate),
+ *      clamped to [0.05, 4]; use and win counts decay by 0.7
+ *      (main.cu:756-769).
+ * The draws (tournaments, operator, tabu and restart choices, strength)
+ * come from Philox4x32-10 streams keyed by the seed and counted by (slot,
+ * generation, level), not from the reference's host mt19937_64; the
+ * variation operators are those of sidon_variation.  Island ties rank by
+ * slot (std::sort leaves them unspecified).
+ *
+ * The workspace is caller-owned device memory of
+ * sidon_generation_workspace_bytes(n_max, P, tabu_capacity) bytes; the
+ * handle is a small host object (created once, never inside a hot call)
+ * holding its layout and the configuration. */
+typedef struct sidon_generation_config {
+  int n_islands;             /* islands of P / n_islands consecutive slots (<= 1024 each) */
+  int elite;                 /* clones kept per island (reference: 2) */
+  int ls_iters;              /* warm tier steps (reference: 4000) */
+  int cold_iters;            /* cold tier steps; the medium tier runs cold_iters / 3 (20000) */
+  float p_max;               /* top of the exponent anneal (20000) */
+  int precision;             /* local search: FP32_SIMT, BF16X1 or BF16X3 */
+  int fw_rounds;             /* Frank-Wolfe rounds per generation, 0 = off (6) */
+  int fw_iters;              /* Chambolle-Pock iterations per round (500) */
+  int fw_nT;                 /* line-search points (12) */
+  float fw_t_max;            /* line-search range (0.30) */
+  int fw_precision;          /* FP32_SIMT (the reference step), BF16X1 or BF16X3 */
+  int tabu_tenure;           /* revisits before a support cell is escaped (6) */
+  int tabu_capacity;         /* signature table entries, a power of two */
+  unsigned long long seed;   /* Philox key of the plan draws and of the variation */
+} sidon_generation_config;
+
+/* The search state on the device, readable with sidon_generation_read_state. */
+typedef struct sidon_generation_state {
+  double best_F;             /* incumbent F (1e30: none) */
+  double level_best_F;       /* best F seen at this level */
+  double op_weight[14], op_use[14], op_win[14];   /* bandit over the 14 operators */
+  double flop;               /* algorithmic flop of the search so far (main.cu:625, 637, 642) */
+  long long ls_steps;        /* candidate-steps of local search */
+  long long evals;           /* fp64 evaluations */
+  long long fw_steps;        /* candidate Frank-Wolfe rounds */
+  int gen;                   /* generations done at this level */
+  int level;
+  int n;                     /* cells of this level */
+  int since_improve;         /* generations since level_best_F improved */
+  int best_n;                /* cells of the incumbent (0: none) */
+  int best_slot;             /* slot of the last generation's best candidate */
+  int improved;              /* the last generation improved the incumbent */
+  int best_nactive, best_nnz;/* near-maximal k and support size of that candidate */
+  int n_cold, n_med;         /* tier sizes of the last generation */
+  int cells;                 /* distinct support signatures seen */
+  int status;                /* SIDON_OK, or SIDON_ERR_CAPACITY once the tabu table filled */
+  int pad_;
+} sidon_generation_state;
+
+/* Device arrays inside the workspace, for callers that read them. */
+typedef struct sidon_generation_views {
+  double* fit;               /* [P] fp64 F after the Frank-Wolfe step */
+  double* parent_fit;        /* [P] fit after the migration (the plan's parent fitness) */
+  double* child_fit;         /* [P] fp64 F of the offspring */
+  int* nactive;              /* [P] */
+  unsigned long long* sig;   /* [P] support signatures */
+  int* nnz;                  /* [P] */
+  int* p1;                   /* [P] plan: first parent */
+  int* p2;                   /* [P] plan: second parent */
+  int* op;                   /* [P] plan: operator (20 = elite clone) */
+  float* strength;           /* [P] plan: strength */
+  int* cur_op;               /* [P] operator that produced the current slot */
+  int* mode;                 /* [P] descent mode per slot */
+  int* rank;                 /* [P] slots of island i in rank order at [i*PI, (i+1)*PI) */
+  int* tier_skip;            /* [3][P] skip masks of the cold, medium and warm tiers */
+  float* best_row;           /* [n_max] incumbent heights */
+  sidon_generation_state* state;
+  unsigned long long* tabu_key;   /* [tabu_capacity + 1]; the last entry holds key 0 */
+  double* tabu_best;              /* [tabu_capacity + 1] */
+  int* tabu_hits;                 /* [tabu_capacity + 1] */
+  int* tabu_used;                 /* [tabu_capacity + 1] */
+} sidon_generation_views;
+
+typedef struct sidon_generation_s* sidon_generation;
+
+SIDON_API size_t sidon_generation_workspace_bytes(int n_max, int P, int tabu_capacity);
+/* Lays the handle over the workspace and initialises the state on the
+ * stream (bandit weights 1, 2.5 / 1.8 / 1.8 for operators 11-13 as at
+ * main.cu:466-467; empty tabu table; no incumbent). */
+SIDON_API int sidon_generation_create(void* workspace, size_t bytes, int n_max, int P,
+                                      const sidon_generation_config* cfg,
+                                      sidon_generation* out, void* stream);
+SIDON_API int sidon_generation_destroy(sidon_generation h);
+SIDON_API int sidon_generation_views_of(sidon_generation h, sidon_generation_views* out);
+/* Starts a ladder level of n cells: generation 0, no level best, seed_op
+ * (device [P], or NULL for all 9) as the operator of each slot, mirror
+ * descent on islands 3, 7, 11, ... (main.cu:566-585). */
+SIDON_API int sidon_generation_begin_level(sidon_generation h, int n, int level,
+                                           const int* seed_op, void* stream);
+/* Adopts row (device fp32 [n]) with F as the incumbent (the resumed vector
+ * of main.cu:414-425). */
+SIDON_API int sidon_generation_set_best(sidon_generation h, const float* row, int n, double F,
+                                        void* stream);
+/* Enqueues one generation on pop (device fp32 [P][n], updated in place). */
+SIDON_API int sidon_generation_step(sidon_generation h, float* pop, void* stream);
+/* Records `generations` generations on pop as a CUDA graph (nothing runs). */
+SIDON_API int sidon_generation_capture(sidon_generation h, float* pop, int generations,
+                                       sidon_graph* graph);
+/* Copies the state to *out after the stream's work so far (synchronises
+ * the stream; not for use inside a capture). */
+SIDON_API int sidon_generation_read_state(sidon_generation h, sidon_generation_state* out,
+                                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,14 @@ _SIG = {
     "so_certify_exact": (_d, [_vp, _i, _vp, _vp, _vp]),
     "so_exact_bk": (_d, [_vp, _i, _i]),
     "so_num_threads": (_i, []),
+    "so_gen_init": (None, [_vp]),
+    "so_gen_begin": (None, [_vp, _vp, _vp, _i, _i, _i, _i, _vp]),
+    "so_gen_tiers": (None, [_vp, _vp, _i, _i, _i, _i, _i, _vp]),
+    "so_gen_select": (None, [_vp, _vp, _i, _i, _i, _i, _i, C.c_ulonglong, _i, _i, _i, _vp, _vp,
+                             _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                             _i, _vp]),
+    "so_gen_post": (None, [_vp, _vp, _i, _i, _i, _vp, _vp, _vp, _vp]),
+    "so_gen_credit": (None, [_vp, _i, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None
@@ -315,3 +323,110 @@ def certify_exact(a):
 def exact_bk(a, k) -> float:
     a = _c(a, np.float64)
     return lib().so_exact_bk(a.ctypes.data, a.size, int(k))
+
+
+# ----------------------- memetic generation policy -------------------------
+class GenState(C.Structure):
+    """struct sidon_generation_state (include/sidon_b200.h), for the oracle."""
+
+    _fields_ = [
+        ("best_F", _d), ("level_best_F", _d),
+        ("op_weight", _d * 14), ("op_use", _d * 14), ("op_win", _d * 14),
+        ("flop", _d),
+        ("ls_steps", C.c_longlong), ("evals", C.c_longlong), ("fw_steps", C.c_longlong),
+        ("gen", _i), ("level", _i), ("n", _i), ("since_improve", _i),
+        ("best_n", _i), ("best_slot", _i), ("improved", _i),
+        ("best_nactive", _i), ("best_nnz", _i),
+        ("n_cold", _i), ("n_med", _i),
+        ("cells", _i), ("status", _i), ("pad_", _i),
+    ]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for k, _ in self._fields_:
+            if k == "pad_":
+                continue
+            x = getattr(self, k)
+            out[k] = list(x) if k.startswith("op_") else x
+        return out
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class GenerationPolicy:
+    """The generation loop's selection policy on the host (so_gen_*): the
+    state, the operator record, the descent modes and the tabu list."""
+
+    def __init__(self, P: int, n_islands: int, elite: int, tabu_tenure: int, seed: int,
+                 n_max: int, tabu_list: int = 1 << 16):
+        self.P, self.NI, self.PI = P, n_islands, P // n_islands
+        self.elite, self.tenure, self.seed = elite, tabu_tenure, seed
+        self.s = GenState()
+        lib().so_gen_init(C.byref(self.s))
+        self.cur_op = np.zeros(P, np.int32)
+        self.mode = np.zeros(P, np.int32)
+        self.best_row = np.zeros(n_max, np.float32)
+        self.tcap = tabu_list
+        self.tkey = np.zeros(tabu_list, np.uint64)
+        self.tbest = np.zeros(tabu_list, np.float64)
+        self.thits = np.zeros(tabu_list, np.int32)
+        self.tcount = np.zeros(1, np.int32)
+        self.var_gen = np.zeros(1, np.uint64)
+        self.n = 0
+
+    def begin_level(self, n: int, level: int, seed_op=None) -> None:
+        keep = None if seed_op is None else _c(seed_op, np.int32)
+        so = None if keep is None else _p(keep)
+        lib().so_gen_begin(C.byref(self.s), _p(self.cur_op), _p(self.mode), self.P, self.PI, n,
+                           level, so)
+        self.n = n
+
+    def set_best(self, row, F: float) -> None:
+        row = _c(row, np.float32)
+        self.best_row[:row.size] = row
+        self.s.best_F = F
+        self.s.best_n = row.size
+
+    def tiers(self, cold: int, med: int, warm: int) -> np.ndarray:
+        skip = np.zeros((3, self.P), np.int32)
+        lib().so_gen_tiers(C.byref(self.s), _p(self.cur_op), self.P, self.n, cold, med, warm,
+                           _p(skip))
+        return skip
+
+    def select(self, pop: np.ndarray, fit, nact, sig, nnz, fw_ran: int, fw_rounds: int,
+               fw_iters: int) -> dict:
+        """pop: host fp32 [P][n], updated in place (migration); sig updated."""
+        P = self.P
+        fit = _c(fit, np.float64)
+        nact = _c(nact, np.int32)
+        nnz = _c(nnz, np.int32)
+        out = {k: np.zeros(P, t) for k, t in (("parent_fit", np.float64), ("rank", np.int32),
+                                               ("p1", np.int32), ("p2", np.int32),
+                                               ("op", np.int32), ("strength", np.float32))}
+        lib().so_gen_select(C.byref(self.s), _p(pop), self.n, P, self.NI, self.elite,
+                            self.tenure, self.seed & 0xFFFFFFFFFFFFFFFF, int(fw_ran),
+                            int(fw_rounds), int(fw_iters), _p(fit), _p(nact), _p(sig), _p(nnz),
+                            _p(out["parent_fit"]), _p(out["rank"]), _p(out["p1"]),
+                            _p(out["p2"]), _p(out["op"]), _p(out["strength"]),
+                            _p(self.best_row), _p(self.tkey), _p(self.tbest), _p(self.thits),
+                            _p(self.tcount), self.tcap, _p(self.var_gen))
+        self.plan = out
+        return out
+
+    def post(self, pop: np.ndarray) -> None:
+        pl = self.plan
+        lib().so_gen_post(C.byref(self.s), _p(pop), self.n, self.P, self.PI, _p(pl["op"]),
+                          _p(self.cur_op), _p(pl["rank"]), _p(self.best_row))
+
+    def credit(self, child_fit) -> None:
+        pl = self.plan
+        child_fit = _c(child_fit, np.float64)
+        lib().so_gen_credit(C.byref(self.s), self.P, _p(pl["op"]), _p(pl["p1"]), _p(child_fit),
+                            _p(pl["parent_fit"]))
+
+    def tabu(self) -> dict:
+        """signature -> (best F, revisits)."""
+        k = int(self.tcount[0])
+        return {int(self.tkey[i]): (float(self.tbest[i]), int(self.thits[i])) for i in range(k)}

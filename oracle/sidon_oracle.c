@@ -914,3 +914,216 @@ SO_EXPORT void so_support_sig_f32(const float* pop, int n, int P, float tol,
     nnz[p] = c;
   }
 }
+
+
+/* ========================= memetic generation policy ===================== */
+/* Test oracle for csrc/generation.cu: the selection policy of the reference
+ * driver's generation loop (src/main.cu:586-785) restated sequentially, in
+ * the reference's loop order and fp64 expressions, with the generation
+ * kernels' Philox draws in place of the driver's mt19937_64.  The tabu map
+ * is a plain list (key, best F, revisits); state is struct
+ * sidon_generation_state of include/sidon_b200.h. */
+#include "../include/sidon_b200.h"
+
+#define GEN_NOPS 14
+
+/* main.cu:466-467 */
+SO_EXPORT void so_gen_init(sidon_generation_state* s) {
+  memset(s, 0, sizeof *s);
+  s->best_F = 1e30;
+  s->level_best_F = 1e30;
+  for (int o = 0; o < GEN_NOPS; ++o) s->op_weight[o] = 1.0;
+  s->op_weight[11] = 2.5; s->op_weight[12] = 1.8; s->op_weight[13] = 1.8;
+}
+
+/* main.cu:566-585: operator record of the seeds, mirror descent on every
+ * fourth island, per-level counters */
+SO_EXPORT void so_gen_begin(sidon_generation_state* s, int* cur_op, int* mode, int P, int PI,
+                            int n, int level, const int* seed_op) {
+  for (int p = 0; p < P; ++p) {
+    cur_op[p] = seed_op ? seed_op[p] : 9;
+    mode[p] = ((p / PI) % 4 == 3) ? 1 : 0;
+  }
+  s->gen = 0; s->level = level; s->n = n; s->since_improve = 0;
+  s->level_best_F = 1e30; s->improved = 0;
+}
+
+/* main.cu:606-629: tiers and their effort counters; skip is [3][P] */
+SO_EXPORT void so_gen_tiers(sidon_generation_state* s, const int* cur_op, int P, int n,
+                            int cold_iters, int med_iters, int warm_iters, int* skip) {
+  const double n2 = (double)n * (double)n;
+  int cold_cap = (int)(0.18 * P); if (cold_cap < 1) cold_cap = 1;
+  int nc = 0, cnt[3] = {0, 0, 0};
+  for (int p = 0; p < P; ++p) {
+    const int o = cur_op[p];
+    int t = 2;
+    if ((o == 9 || o == 11) && nc < cold_cap) { t = 0; ++nc; }
+    else if (o == 9 || o == 11 || o == 10 || o == 5 || o == 7 || o == 8 || o == 12 || o == 13)
+      t = 1;
+    for (int k = 0; k < 3; ++k) skip[k * P + p] = t == k ? 0 : 1;
+    ++cnt[t];
+  }
+  const int iters[3] = {cold_iters, med_iters, warm_iters};
+  s->n_cold = cnt[0]; s->n_med = cnt[1];
+  for (int t = 0; t < 3; ++t)
+    if (cnt[t] > 0) {
+      s->ls_steps += (long long)cnt[t] * iters[t];
+      s->flop += 4.0 * n2 * (double)cnt[t] * (double)iters[t];
+    }
+}
+
+static int gen_before(double fa, int a, double fb, int b) {
+  const int na = fa != fa, nb = fb != fb;
+  if (na != nb) return nb;
+  if (!na && fa != fb) return fa < fb;
+  return a < b;
+}
+static int gen_pos(double u, int m) { const int k = (int)(u * (double)m); return k < m - 1 ? k : m - 1; }
+static double gen_u53(uint32_t hi, uint32_t lo) {
+  return ((double)(hi >> 5) * 67108864.0 + (double)(lo >> 6)) * (1.0 / 9007199254740992.0);
+}
+static int gen_find(const unsigned long long* key, int cnt, unsigned long long k) {
+  for (int i = 0; i < cnt; ++i) if (key[i] == k) return i;
+  return -1;
+}
+
+/* main.cu:641-730: incumbent, level best, tabu list, island ranking,
+ * migration every 12 generations, offspring plan.  fit / nact / nnz are the
+ * evaluation's, sig is updated by the migration, parent_fit receives the
+ * migrated fitness.  The tabu list has room for tcap entries (*tcount
+ * used); a full list sets status SIDON_ERR_CAPACITY. */
+SO_EXPORT void so_gen_select(sidon_generation_state* s, float* pop, int n, int P, int NI,
+                             int elite, int tenure, unsigned long long seed, int fw_ran,
+                             int fw_rounds, int fw_iters, const double* fit, const int* nact,
+                             unsigned long long* sig, const int* nnz, double* parent_fit,
+                             int* rank, int* p1, int* p2, int* op, float* strength,
+                             float* best_row, unsigned long long* tkey, double* tbest,
+                             int* thits, int* tcount, int tcap, unsigned long long* var_gen) {
+  const int PI = P / NI, gen = s->gen;
+  const double n2 = (double)n * (double)n;
+  int bi = 0;
+  for (int p = 1; p < P; ++p) if (fit[p] < fit[bi]) bi = p;
+  const int impr = fit[bi] < s->best_F - 1e-13;
+  if (impr) {
+    s->best_F = fit[bi]; s->best_n = n;
+    memcpy(best_row, pop + (size_t)bi * n, sizeof(float) * (size_t)n);
+  }
+  if (fit[bi] < s->level_best_F - 1e-13) { s->level_best_F = fit[bi]; s->since_improve = 0; }
+  else s->since_improve += 1;
+  s->best_slot = bi; s->improved = impr;
+  s->best_nactive = nact[bi]; s->best_nnz = nnz[bi];
+  if (fw_ran) {
+    s->fw_steps += (long long)fw_rounds * P;
+    s->flop += (double)P * (double)fw_rounds * (4.0 * n2 * (double)fw_iters + 2.0 * n2 * 13.0);
+  }
+  s->evals += P;
+  s->flop += 2.0 * n2 * (double)P;
+  *var_gen = (unsigned long long)(gen + 1000 * s->level);
+
+  /* tabu (main.cu:653-661) */
+  for (int p = 0; p < P; ++p) {
+    int e = gen_find(tkey, *tcount, sig[p]);
+    if (e < 0) {
+      if (*tcount >= tcap) { if (s->status == 0) s->status = SIDON_ERR_CAPACITY; continue; }
+      e = (*tcount)++;
+      tkey[e] = sig[p]; tbest[e] = fit[p]; thits[e] = 0;
+      s->cells += 1;
+    } else if (fit[p] < tbest[e] - 1e-12) {
+      tbest[e] = fit[p]; thits[e] = 0;
+    } else {
+      thits[e] += 1;
+    }
+  }
+
+  /* rank inside each island: insertion sort, ascending F, NaN last, ties by slot */
+  for (int i = 0; i < NI; ++i) {
+    int* L = rank + i * PI;
+    for (int r = 0; r < PI; ++r) {
+      const int p = i * PI + r;
+      int k = r;
+      while (k > 0 && gen_before(fit[p], p, fit[L[k - 1]], L[k - 1])) { L[k] = L[k - 1]; --k; }
+      L[k] = p;
+    }
+  }
+  for (int p = 0; p < P; ++p) parent_fit[p] = fit[p];
+
+  /* migration (main.cu:672-680) */
+  if (gen > 0 && gen % 12 == 0)
+    for (int i = 0; i < NI; ++i) {
+      const int src = rank[i * PI], dst = rank[((i + 1) % NI) * PI + PI - 1];
+      memmove(pop + (size_t)dst * n, pop + (size_t)src * n, sizeof(float) * (size_t)n);
+      parent_fit[dst] = parent_fit[src];
+      sig[dst] = sig[src];
+    }
+
+  /* offspring plan (main.cu:682-730) */
+  double warm = (double)gen / 40.0; if (warm > 1.0) warm = 1.0;
+  double stagn = (double)s->since_improve / 25.0; if (stagn > 1.0) stagn = 1.0;
+  double cum[GEN_NOPS], tot = 0.0, c = 0.0;
+  for (int o = 0; o < GEN_NOPS; ++o) tot += s->op_weight[o];
+  for (int o = 0; o < GEN_NOPS; ++o) { c += s->op_weight[o] / tot; cum[o] = c; }
+  cum[GEN_NOPS - 1] = 1.0;
+  const uint32_t key[2] = {(uint32_t)seed ^ 0x243F6A88u, (uint32_t)(seed >> 32) ^ 0x85A308D3u};
+  static const int divers[7] = {5, 7, 9, 10, 8, 11, 12};
+  for (int slot = 0; slot < P; ++slot) {
+    const int i = slot / PI, r = slot - i * PI;
+    const int* isl = rank + i * PI;
+    if (r < elite) {
+      p1[slot] = p2[slot] = isl[r]; op[slot] = 20; strength[slot] = 0.f;
+      continue;
+    }
+    double u[8];
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t ctr[4] = {(uint32_t)slot, (uint32_t)gen, (uint32_t)s->level, (uint32_t)q};
+      uint32_t x[4];
+      so_philox4x32(ctr, key, x);
+      u[2 * q] = gen_u53(x[0], x[1]);
+      u[2 * q + 1] = gen_u53(x[2], x[3]);
+    }
+    int a = isl[gen_pos(u[0], PI)], b = isl[gen_pos(u[1], PI)];
+    const int pa = parent_fit[a] < parent_fit[b] ? a : b;
+    a = isl[gen_pos(u[2], PI)]; b = isl[gen_pos(u[3], PI)];
+    const int pb = parent_fit[a] < parent_fit[b] ? a : b;
+    int o = 0;
+    while (o < GEN_NOPS - 1 && cum[o] < u[4]) ++o;
+    const int e = gen_find(tkey, *tcount, sig[pa]);
+    const int hits = e >= 0 ? thits[e] : 0;
+    const double cb = e >= 0 ? tbest[e] : 1e30;
+    if (hits > tenure && cb > s->best_F * (1.0 + 2e-4)) o = divers[gen_pos(u[5], 7)];
+    if (stagn > 0.7 && u[6] < 0.10) o = 9;
+    p1[slot] = pa; p2[slot] = pb; op[slot] = o;
+    strength[slot] = (float)((0.03 + 0.35 * u[7]) * (0.5 + warm) * (1.0 + 1.5 * stagn));
+    s->op_use[o] += 1.0;
+  }
+}
+
+/* main.cu:743-754: operator record, reinjection of the incumbent every 10th
+ * generation over the worst slot of island 0 */
+SO_EXPORT void so_gen_post(const sidon_generation_state* s, float* pop, int n, int P, int PI,
+                           const int* op, int* cur_op, const int* rank, const float* best_row) {
+  for (int p = 0; p < P; ++p) cur_op[p] = op[p];
+  if (s->gen % 10 == 9 && s->best_n == n) {
+    const int slot = rank[PI - 1];
+    memcpy(pop + (size_t)slot * n, best_row, sizeof(float) * (size_t)n);
+    cur_op[slot] = 20;
+  }
+}
+
+/* main.cu:756-769: bandit credit every 5th generation; the counter */
+SO_EXPORT void so_gen_credit(sidon_generation_state* s, int P, const int* op, const int* p1,
+                             const double* child_fit, const double* parent_fit) {
+  const int gen = s->gen;
+  if (gen > 0 && gen % 5 == 0) {
+    for (int p = 0; p < P; ++p)
+      if (op[p] >= 0 && op[p] < GEN_NOPS && child_fit[p] < parent_fit[p1[p]]) s->op_win[op[p]] += 1.0;
+    for (int o = 0; o < GEN_NOPS; ++o) {
+      const double rate = s->op_use[o] > 20 ? s->op_win[o] / s->op_use[o] : 0.25;
+      double x = 0.85 * s->op_weight[o] + 0.15 * (0.15 + 3.0 * rate);
+      x = x < 4.0 ? x : 4.0;
+      x = x > 0.05 ? x : 0.05;
+      s->op_weight[o] = x;
+    }
+    for (int o = 0; o < GEN_NOPS; ++o) { s->op_use[o] *= 0.7; s->op_win[o] *= 0.7; }
+  }
+  s->gen = gen + 1;
+}

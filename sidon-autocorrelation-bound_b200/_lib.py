@@ -67,6 +67,15 @@ SIGNATURES = {
     "sidon_anneal_capture": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
     "sidon_graph_launch": (_i, [_vp, _vp]),
     "sidon_graph_destroy": (_i, [_vp]),
+    "sidon_generation_workspace_bytes": (_sz, [_i, _i, _i]),
+    "sidon_generation_create": (_i, [_vp, _sz, _i, _i, _vp, _vp, _vp]),
+    "sidon_generation_destroy": (_i, [_vp]),
+    "sidon_generation_views_of": (_i, [_vp, _vp]),
+    "sidon_generation_begin_level": (_i, [_vp, _i, _i, _vp, _vp]),
+    "sidon_generation_set_best": (_i, [_vp, _vp, _i, _d, _vp]),
+    "sidon_generation_step": (_i, [_vp, _vp, _vp]),
+    "sidon_generation_capture": (_i, [_vp, _vp, _i, _vp]),
+    "sidon_generation_read_state": (_i, [_vp, _vp, _vp]),
 }
 
 
@@ -87,6 +96,51 @@ class AnnealConfig(C.Structure):
         ("migrate_every", _i),
         ("k_migrate", _i),
     ]
+
+
+class GenerationConfig(C.Structure):
+    """struct sidon_generation_config."""
+
+    _fields_ = [
+        ("n_islands", _i), ("elite", _i),
+        ("ls_iters", _i), ("cold_iters", _i),
+        ("p_max", _f),
+        ("precision", _i),
+        ("fw_rounds", _i), ("fw_iters", _i), ("fw_nT", _i),
+        ("fw_t_max", _f),
+        ("fw_precision", _i),
+        ("tabu_tenure", _i), ("tabu_capacity", _i),
+        ("seed", C.c_ulonglong),
+    ]
+
+
+NOPS = 14
+
+
+class GenerationState(C.Structure):
+    """struct sidon_generation_state."""
+
+    _fields_ = [
+        ("best_F", _d), ("level_best_F", _d),
+        ("op_weight", _d * NOPS), ("op_use", _d * NOPS), ("op_win", _d * NOPS),
+        ("flop", _d),
+        ("ls_steps", C.c_longlong), ("evals", C.c_longlong), ("fw_steps", C.c_longlong),
+        ("gen", _i), ("level", _i), ("n", _i), ("since_improve", _i),
+        ("best_n", _i), ("best_slot", _i), ("improved", _i),
+        ("best_nactive", _i), ("best_nnz", _i),
+        ("n_cold", _i), ("n_med", _i),
+        ("cells", _i), ("status", _i), ("pad_", _i),
+    ]
+
+
+class GenerationViews(C.Structure):
+    """struct sidon_generation_views (device pointers into the workspace)."""
+
+    _fields_ = [(k, _vp) for k in (
+        "fit", "parent_fit", "child_fit", "nactive", "sig", "nnz", "p1", "p2", "op", "strength",
+        "cur_op", "mode", "rank", "tier_skip", "best_row", "state", "tabu_key", "tabu_best",
+        "tabu_hits", "tabu_used")]
+
 
 _lock = threading.Lock()
 _lib: C.CDLL | None = None

@@ -30,7 +30,7 @@ NVCC_FLAGS = [
 
 # the variation operators keep each product and sum rounded on its own (no
 # fused multiply-add), so a host restatement reproduces them bit for bit
-PER_FILE_FLAGS = {"variation.cu": ["--fmad=false"]}
+PER_FILE_FLAGS = {"variation.cu": ["--fmad=false"], "generation.cu": ["--fmad=false"]}
 
 
 def nvcc() -> str:

@@ -43,11 +43,6 @@ int prepare_simt(int n_max, bool local_search);
 
 using namespace sidon_host;
 
-struct sidon_graph_s {
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-};
-
 namespace {
 
 struct Args {

@@ -73,7 +73,8 @@ int launch_island_migrate_ragged(float* pop, const long long* offsets, double* f
 int launch_ragged_order(const long long* offsets, int P, int* order, cudaStream_t st);
 int launch_variation(const void* pop, void* out, int dtype, int n, int n_off, const int* p1,
                      const int* p2, const int* op, const float* strength,
-                     unsigned long long seed, unsigned long long gen, cudaStream_t st);
+                     unsigned long long seed, unsigned long long gen, cudaStream_t st,
+                     const unsigned long long* gen_dev = nullptr);
 int launch_support_sig(const void* pop, int dtype, int n, int P, float tol,
                        unsigned long long* sig, int* nnz, cudaStream_t st);
 

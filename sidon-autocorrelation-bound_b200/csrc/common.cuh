@@ -151,3 +151,10 @@ int device_ok();                                     // SIDON_OK if current devi
 // run eagerly.
 int set_dyn_smem(const void* fn, size_t smem);
 }  // namespace sidon_host
+
+// a captured CUDA graph and its executable (sidon_anneal_capture,
+// sidon_generation_capture; replayed by sidon_graph_launch)
+struct sidon_graph_s {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};

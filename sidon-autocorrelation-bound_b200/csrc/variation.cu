@@ -22,36 +22,16 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "philox.cuh"
 
 namespace sidon {
 namespace var {
 
 constexpr int BD = 256;
 
-struct U4 {
-  uint32_t x, y, z, w;
-};
-
-// Philox4x32-10: ten rounds of two 32x32 -> 64 multiplications on the
-// counter, key bumped by the Weyl constants between rounds.
-__host__ __device__ inline U4 philox(U4 c, uint32_t k0, uint32_t k1) {
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
-    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
-    const U4 n = {(uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1,
-                  (uint32_t)p0};
-    c = n;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
-  }
-  return c;
-}
-
-// uniform in (0, 1): the top 24 bits plus one half, exactly representable
-__host__ __device__ inline float u01(uint32_t w) {
-  return ((float)(w >> 8) + 0.5f) * (1.0f / 16777216.0f);
-}
+using rng::U4;
+using rng::philox;
+using rng::u01;
 
 // the offspring's 64 parameters: counters (q, j, gen_lo, gen_hi ^ 0), q < 16
 __host__ __device__ inline void params(unsigned long long seed, unsigned long long gen, int j,
@@ -93,8 +73,10 @@ template <typename T>
 __global__ void __launch_bounds__(BD)
 k_variation(const T* __restrict__ pop, T* __restrict__ out, int n, int n_off,
             const int* __restrict__ p1, const int* __restrict__ p2, const int* __restrict__ opv,
-            const float* __restrict__ strength, unsigned long long seed, unsigned long long gen) {
+            const float* __restrict__ strength, unsigned long long seed, unsigned long long gen,
+            const unsigned long long* __restrict__ gen_dev) {
   __shared__ float u[64];
+  if (gen_dev) gen = *gen_dev;   // the generation counter of a captured loop
   __shared__ double red[32];
   const int j = blockIdx.x;
   if (j >= n_off) return;
@@ -336,13 +318,15 @@ using namespace sidon;
 
 int launch_variation(const void* pop, void* out, int dtype, int n, int n_off, const int* p1,
                      const int* p2, const int* op, const float* strength,
-                     unsigned long long seed, unsigned long long gen, cudaStream_t st) {
+                     unsigned long long seed, unsigned long long gen, cudaStream_t st,
+                     const unsigned long long* gen_dev) {
   if (dtype == SIDON_F32)
     var::k_variation<float><<<n_off, var::BD, 0, st>>>((const float*)pop, (float*)out, n, n_off,
-                                                        p1, p2, op, strength, seed, gen);
+                                                        p1, p2, op, strength, seed, gen, gen_dev);
   else
     var::k_variation<double><<<n_off, var::BD, 0, st>>>((const double*)pop, (double*)out, n,
-                                                         n_off, p1, p2, op, strength, seed, gen);
+                                                         n_off, p1, p2, op, strength, seed, gen,
+                                                         gen_dev);
   return check_launch();
 }
 

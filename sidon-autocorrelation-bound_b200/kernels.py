@@ -607,3 +607,165 @@ class AnnealGraph:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# memetic generations (sidon_generation_*)
+# ---------------------------------------------------------------------------
+def generation_config(n_islands: int = 8, elite: int = 2, ls_iters: int = 4000,
+                      cold_iters: int = 20000, p_max: float = 20000.0,
+                      precision: str = "bf16x3", fw_rounds: int = 6, fw_iters: int = 500,
+                      fw_nT: int = 12, fw_t_max: float = 0.30, fw_precision: str = "fp32",
+                      tabu_tenure: int = 6, tabu_capacity: int = 1 << 16,
+                      seed: int = 20260905) -> _lib.GenerationConfig:
+    """struct sidon_generation_config; the defaults are the reference driver's
+    (src/main.cu:41-58, 472: 8 islands, 2 elites, warm 4000 / cold 20000
+    steps, p up to 20000, 6 Frank-Wolfe rounds of 500 iterations, tabu
+    tenure 6)."""
+    return _lib.GenerationConfig(int(n_islands), int(elite), int(ls_iters), int(cold_iters),
+                                 float(p_max), PRECISIONS[precision], int(fw_rounds),
+                                 int(fw_iters), int(fw_nT), float(fw_t_max),
+                                 PRECISIONS[fw_precision], int(tabu_tenure), int(tabu_capacity),
+                                 int(seed) & 0xFFFFFFFFFFFFFFFF)
+
+
+class GenerationGraph:
+    """Generations recorded once as a CUDA graph (sidon_generation_capture);
+    ``launch`` replays them."""
+
+    def __init__(self, handle, pop: torch.Tensor, generations: int):
+        h = C.c_void_p()
+        _lib.call("sidon_generation_capture", handle, _dev(pop, "pop", torch.float32),
+                  int(generations), C.byref(h))
+        self._h = h
+        self._pop = pop
+        self.generations = int(generations)
+
+    def launch(self, stream=None) -> None:
+        if not self._h:
+            raise RuntimeError("graph destroyed")
+        _lib.call("sidon_graph_launch", self._h, _stream(stream))
+
+    def close(self) -> None:
+        if self._h:
+            _lib.load().sidon_graph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Generation:
+    """The memetic island search, one generation at a time on the device
+    (src/main.cu:586-785): anneal tiers, Frank-Wolfe, fp64 evaluation,
+    support signatures, incumbent, tabu table, island ranking and
+    migration, offspring plan, variation, reinjection and bandit credit.
+
+    The workspace is one device byte tensor owned by this object; the state
+    (incumbent, bandit, tabu table, counters) lives in it across levels.
+    """
+
+    def __init__(self, n_max: int, P: int, cfg: _lib.GenerationConfig | None = None,
+                 device="cuda", stream=None):
+        self.cfg = cfg if cfg is not None else generation_config()
+        self.n_max, self.P = int(n_max), int(P)
+        lib = _lib.load()
+        nbytes = lib.sidon_generation_workspace_bytes(self.n_max, self.P,
+                                                      int(self.cfg.tabu_capacity))
+        if nbytes == 0:
+            raise SidonError("sidon_generation_workspace_bytes", _lib.ERR_ARG)
+        self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        h = C.c_void_p()
+        _lib.call("sidon_generation_create", self.workspace.data_ptr(), nbytes, self.n_max,
+                  self.P, C.byref(self.cfg), C.byref(h), _stream(stream))
+        self._h = h
+        v = _lib.GenerationViews()
+        _lib.call("sidon_generation_views_of", self._h, C.byref(v))
+        self._views = v
+        self.n = 0
+
+    def _view(self, name: str, count: int, dtype) -> torch.Tensor:
+        off = getattr(self._views, name) - self.workspace.data_ptr()
+        size = torch.tensor([], dtype=dtype).element_size() * count
+        return self.workspace[off:off + size].view(dtype)
+
+    def views(self) -> dict:
+        """Device tensors over the workspace arrays (current level's P)."""
+        P, cap1 = self.P, int(self.cfg.tabu_capacity) + 1
+        return {
+            "fit": self._view("fit", P, torch.float64),
+            "parent_fit": self._view("parent_fit", P, torch.float64),
+            "child_fit": self._view("child_fit", P, torch.float64),
+            "nactive": self._view("nactive", P, torch.int32),
+            "sig": self._view("sig", P, torch.int64),
+            "nnz": self._view("nnz", P, torch.int32),
+            "p1": self._view("p1", P, torch.int32),
+            "p2": self._view("p2", P, torch.int32),
+            "op": self._view("op", P, torch.int32),
+            "strength": self._view("strength", P, torch.float32),
+            "cur_op": self._view("cur_op", P, torch.int32),
+            "mode": self._view("mode", P, torch.int32),
+            "rank": self._view("rank", P, torch.int32),
+            "tier_skip": self._view("tier_skip", 3 * P, torch.int32).view(3, P),
+            "best_row": self._view("best_row", self.n_max, torch.float32),
+            "tabu_key": self._view("tabu_key", cap1, torch.int64),
+            "tabu_best": self._view("tabu_best", cap1, torch.float64),
+            "tabu_hits": self._view("tabu_hits", cap1, torch.int32),
+            "tabu_used": self._view("tabu_used", cap1, torch.int32),
+        }
+
+    def begin_level(self, n: int, level: int, seed_op: torch.Tensor | None = None,
+                    stream=None) -> None:
+        """Start a ladder level of n cells; seed_op: int32 [P] operator per slot
+        (None: all 9, fresh restarts)."""
+        _lib.call("sidon_generation_begin_level", self._h, int(n), int(level),
+                  _opt(seed_op, "seed_op", torch.int32), _stream(stream))
+        self.n = int(n)
+
+    def set_best(self, row: torch.Tensor, F: float, stream=None) -> None:
+        """Adopt row (fp32 device [n]) with fp64 F as the incumbent."""
+        _lib.call("sidon_generation_set_best", self._h, _dev(row, "row", torch.float32),
+                  int(row.numel()), float(F), _stream(stream))
+
+    def step(self, pop: torch.Tensor, stream=None) -> None:
+        """Enqueue one generation on pop (fp32 [P][n], in place)."""
+        if tuple(pop.shape) != (self.P, self.n):
+            raise ValueError(f"pop must be [{self.P}][{self.n}]")
+        _lib.call("sidon_generation_step", self._h, _dev(pop, "pop", torch.float32),
+                  _stream(stream))
+
+    def capture(self, pop: torch.Tensor, generations: int) -> GenerationGraph:
+        if tuple(pop.shape) != (self.P, self.n):
+            raise ValueError(f"pop must be [{self.P}][{self.n}]")
+        return GenerationGraph(self._h, pop, generations)
+
+    def state(self, stream=None) -> dict:
+        """The device state after the stream's work so far (synchronises it)."""
+        s = _lib.GenerationState()
+        _lib.call("sidon_generation_read_state", self._h, C.byref(s), _stream(stream))
+        out = {}
+        for k, _ in _lib.GenerationState._fields_:
+            if k == "pad_":
+                continue
+            x = getattr(s, k)
+            out[k] = list(x) if k.startswith("op_") else x
+        return out
+
+    def best(self) -> np.ndarray:
+        """The incumbent heights (host fp32, its own n cells)."""
+        n = self.state()["best_n"]
+        return self.views()["best_row"][:n].cpu().numpy()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().sidon_generation_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

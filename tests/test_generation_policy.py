@@ -1,0 +1,205 @@
+"""The generation loop's selection policy on the CPU: the oracle's restatement
+(so_gen_*) of src/main.cu:586-785 checked against the driver's rules one by
+one, and the C ABI's argument checks of sidon_generation_* (no GPU needed).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+
+def policy(orc, P=64, NI=4, elite=2, tenure=6, seed=7, n=16):
+    pol = orc.GenerationPolicy(P, NI, elite, tenure, seed, n)
+    pol.begin_level(n, 0)
+    return pol
+
+
+def test_initial_bandit_weights_and_modes(orc):
+    pol = policy(orc, P=64, NI=8)
+    s = pol.s.as_dict()
+    assert s["op_weight"] == [1.0] * 11 + [2.5, 1.8, 1.8]          # main.cu:466-467
+    assert s["best_F"] == 1e30 and s["level_best_F"] == 1e30
+    assert list(pol.cur_op) == [9] * 64
+    # one island in four uses mirror descent (main.cu:569-572)
+    assert [int(pol.mode[i * 8]) for i in range(8)] == [0, 0, 0, 1, 0, 0, 0, 1]
+
+
+def test_tiers_cold_cap_and_classes(orc):
+    P = 64
+    pol = policy(orc, P=P)
+    ops = np.full(P, 20, np.int32)
+    ops[:20] = 9                     # 20 restarts: only max(1, 0.18 P) = 11 go cold
+    ops[20:24] = 11
+    ops[24:30] = [10, 5, 7, 8, 12, 13]
+    ops[30:34] = [0, 1, 2, 3]
+    pol.cur_op[:] = ops
+    skip = pol.tiers(30, 10, 7)
+    tier = np.argmin(skip, axis=0)
+    assert (tier[:11] == 0).all() and (tier[11:30] == 1).all() and (tier[30:] == 2).all()
+    assert (skip.sum(axis=0) == 2).all()
+    s = pol.s.as_dict()
+    assert (s["n_cold"], s["n_med"]) == (11, 19)
+    assert s["ls_steps"] == 11 * 30 + 19 * 10 + 34 * 7
+    n2 = 16.0 * 16.0
+    assert s["flop"] == ((0.0 + 4.0 * n2 * 11 * 30) + 4.0 * n2 * 19 * 10) + 4.0 * n2 * 34 * 7
+
+
+def run_select(pol, fit, sig, n=16, fw_ran=1):
+    P = pol.P
+    rng = np.random.default_rng(0)
+    pop = rng.uniform(size=(P, n)).astype(np.float32)
+    pop0 = pop.copy()
+    sig = np.asarray(sig, np.uint64).copy()
+    plan = pol.select(pop, fit, np.zeros(P, np.int32), sig, np.full(P, n, np.int32), fw_ran, 6,
+                      500)
+    return plan, pop, pop0, sig
+
+
+def test_select_incumbent_ranking_elites_and_tournaments(orc):
+    P, NI, PI, elite = 64, 4, 16, 2
+    pol = policy(orc, P=P, NI=NI, elite=elite)
+    rng = np.random.default_rng(1)
+    fit = rng.uniform(1.5, 2.0, P)
+    fit[37] = 1.49
+    fit[5] = fit[6]                  # a tie ranks by slot
+    plan, pop, pop0, _ = run_select(pol, fit, rng.integers(0, 2**63, P))
+    s = pol.s.as_dict()
+    assert s["best_slot"] == 37 and s["best_F"] == 1.49 and s["improved"] == 1
+    assert np.array_equal(pol.best_row[:16], pop0[37])
+    for i in range(NI):
+        isl = plan["rank"][i * PI:(i + 1) * PI]
+        assert sorted(isl) == list(range(i * PI, (i + 1) * PI))
+        keys = [(fit[p], p) for p in isl]
+        assert keys == sorted(keys)
+        for r in range(PI):
+            slot = i * PI + r
+            if r < elite:
+                assert plan["op"][slot] == 20 and plan["p1"][slot] == isl[r] == plan["p2"][slot]
+                assert plan["strength"][slot] == 0.0
+            else:
+                assert i * PI <= plan["p1"][slot] < (i + 1) * PI
+                assert i * PI <= plan["p2"][slot] < (i + 1) * PI
+                assert 0 <= plan["op"][slot] < 14
+                # gen 0, no stagnation: (0.03 + 0.35 u) * 0.5 * 1
+                assert 0.015 - 1e-7 <= plan["strength"][slot] <= 0.19 + 1e-7
+    assert np.array_equal(plan["parent_fit"], fit)    # no migration at generation 0
+    assert np.array_equal(pop, pop0)
+    assert sum(s["op_use"]) == P - NI * elite          # elites are not counted
+    assert int(pol.var_gen[0]) == 0                    # gen + 1000 level
+
+
+def test_select_migration_every_12th_generation(orc):
+    P, NI, PI = 32, 4, 8
+    pol = policy(orc, P=P, NI=NI)
+    pol.s.gen = 12
+    pol.s.level = 3
+    rng = np.random.default_rng(2)
+    fit = rng.uniform(1.5, 2.0, P)
+    sig = rng.integers(0, 2**63, P)
+    plan, pop, pop0, sig_after = run_select(pol, fit, sig)
+    for i in range(NI):
+        src = plan["rank"][i * PI]
+        dst = plan["rank"][((i + 1) % NI) * PI + PI - 1]
+        assert np.array_equal(pop[dst], pop0[src])
+        assert plan["parent_fit"][dst] == fit[src]
+        assert sig_after[dst] == np.uint64(sig[src])
+    assert int(pol.var_gen[0]) == 12 + 3000
+
+
+def test_tabu_list_revisits_and_diversification(orc):
+    P, NI = 16, 1
+    pol = policy(orc, P=P, NI=NI, elite=0, tenure=1)
+    fit = np.linspace(1.6, 1.7, P)
+    sig = np.full(P, 42, np.uint64)          # one support cell for everybody
+    run_select(pol, fit, sig)
+    # first slot sets the cell's best, the 15 others revisit it without improving
+    assert pol.tabu() == {42: (1.6, 15)}
+    assert pol.s.cells == 1
+    # the cell is not within 2e-4 of the incumbent once a better F exists
+    pol.s.best_F = 1.0
+    plan, *_ = run_select(pol, fit, sig)
+    assert set(plan["op"]) <= {5, 7, 9, 10, 8, 11, 12}
+    # an improvement of more than 1e-12 resets the revisits
+    fit2 = fit.copy()
+    fit2[3] = 1.0
+    run_select(pol, fit2, sig)
+    assert pol.tabu()[42] == (1.0, 12)
+
+
+def test_stagnation_turns_a_tenth_into_restarts(orc):
+    P = 1024
+    pol = policy(orc, P=P, NI=1, elite=0, n=8)
+    pol.s.since_improve = 30
+    pol.s.level_best_F = 0.0
+    fit = np.linspace(1.6, 1.7, P)
+    plan, *_ = run_select(pol, fit, np.arange(P), n=8)
+    share = float((plan["op"] == 9).mean())
+    assert 0.1 < share < 0.25                   # 0.1 forced + the bandit's own draws of 9
+    stagn = 1.0                                 # min(1, 31 / 25)
+    assert plan["strength"].max() <= (0.03 + 0.35) * 0.5 * (1 + 1.5 * stagn) + 1e-6
+
+
+def test_post_reinjects_the_incumbent_every_10th_generation(orc):
+    P, NI, PI, n = 16, 2, 8, 8
+    pol = policy(orc, P=P, NI=NI, n=n)
+    fit = np.linspace(1.6, 1.7, P)[::-1].copy()
+    plan, pop, pop0, _ = run_select(pol, fit, np.arange(P), n=n)
+    best = pol.best_row[:n].copy()
+    pol.s.gen = 9
+    pop2 = np.zeros((P, n), np.float32)
+    pol.post(pop2)
+    worst0 = plan["rank"][PI - 1]
+    assert np.array_equal(pop2[worst0], best)
+    assert pol.cur_op[worst0] == 20
+    others = [p for p in range(P) if p != worst0]
+    assert np.array_equal(pol.cur_op[others], plan["op"][others])
+
+
+def test_credit_updates_the_bandit(orc):
+    P = 40
+    pol = policy(orc, P=P, NI=1, elite=0)
+    fit = np.linspace(1.6, 1.7, P)
+    plan, *_ = run_select(pol, fit, np.arange(P))
+    use = np.array(pol.s.as_dict()["op_use"])
+    w0 = np.array(pol.s.as_dict()["op_weight"])
+    child = plan["parent_fit"][plan["p1"]] - 0.01 * (np.arange(P) % 2)   # odd slots win
+    pol.s.gen = 5
+    pol.credit(child)
+    win = np.zeros(14)
+    for p in range(P):
+        if child[p] < plan["parent_fit"][plan["p1"][p]]:
+            win[plan["op"][p]] += 1.0
+    s = pol.s.as_dict()
+    for o in range(14):
+        rate = win[o] / use[o] if use[o] > 20 else 0.25
+        w = min(4.0, max(0.05, 0.85 * w0[o] + 0.15 * (0.15 + 3.0 * rate)))
+        assert s["op_weight"][o] == w
+        assert s["op_use"][o] == use[o] * 0.7 and s["op_win"][o] == win[o] * 0.7
+    assert s["gen"] == 6
+
+
+def test_capi_generation_argument_checks(lib):
+    from sidon_b200 import _lib, kernels
+    assert lib.sidon_generation_workspace_bytes(0, 64, 1024) == 0
+    a = lib.sidon_generation_workspace_bytes(128, 64, 1024)
+    b = lib.sidon_generation_workspace_bytes(256, 64, 1024)
+    assert 0 < a < b and a % 256 == 0
+    h = C.c_void_p()
+    fake = C.c_void_p(1 << 20)          # never dereferenced: the checks come first
+
+    def create(**kw):
+        cfg = kernels.generation_config(**kw)
+        return lib.sidon_generation_create(fake, a, 128, 64, C.byref(cfg), C.byref(h), None)
+
+    assert create(n_islands=3) == _lib.ERR_ARG              # 64 slots in 3 islands
+    assert create(tabu_capacity=1000) == _lib.ERR_ARG       # not a power of two
+    assert create(elite=-1) == _lib.ERR_ARG
+    assert create(precision="fp64") == _lib.ERR_DTYPE
+    assert create(fw_t_max=1.5) == _lib.ERR_ARG
+    cfg = kernels.generation_config()
+    assert lib.sidon_generation_create(fake, a - 256, 128, 64, C.byref(cfg), C.byref(h),
+                                       None) == _lib.ERR_ARG  # workspace too small
+    assert lib.sidon_generation_create(C.c_void_p((1 << 20) + 16), a, 128, 64, C.byref(cfg),
+                                       C.byref(h), None) == _lib.ERR_ARG  # misaligned
+    assert lib.sidon_generation_step(None, None, None) == _lib.ERR_ARG
+    assert lib.sidon_generation_destroy(None) == _lib.OK
