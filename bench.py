@@ -2,7 +2,7 @@
 adjoint correlation + update) at n = 8400 cells, B = 256 candidates per GPU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|bf16x1|fp32]
-                    [--impl ours|reference] [--workload lp_adam|islands]
+                    [--impl ours|reference] [--workload lp_adam|islands|ladder|memetic]
 
 One *step* = every candidate of the batch advances one Adam step.  The timed
 region is ONE launch of the fused local-search kernel running K steps (the
@@ -474,6 +474,72 @@ def islands_arm(args) -> None:
         print(json.dumps(line))
 
 
+# ----------------------------- memetic generations ---------------------------
+def memetic_arm(args) -> None:
+    """The reference driver's generation (src/main.cu:586-785) at its default
+    settings -- 256 candidates in 8 islands, 2 elites, warm / medium / cold
+    tiers of 4000 / 6666 / 20000 steps with p up to 20000, 6 Frank-Wolfe
+    rounds of 500 iterations, tabu tenure 6 -- at one ladder level of n
+    cells, on the device with the policy included.  One warm-up generation,
+    then --steps generations replayed from one CUDA graph.  Prints one JSON
+    line (its own metric; not the headline line)."""
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import sidon_b200
+    sidon_b200.load(build=not (ROOT / "sidon-autocorrelation-bound_b200" / "libsidon_b200.so").exists())
+    from sidon_b200 import kernels, synth
+
+    n, P, G = args.memetic_n, 256, max(1, args.steps)
+    cfg = kernels.generation_config(precision=args.precision, fw_precision=args.fw_precision,
+                                    seed=20260905 + rank)
+    pop = torch.as_tensor(synth.population("lognormal", n, P, seed=2048 + rank), device=dev)
+    gen = kernels.Generation(n, P, cfg, device=dev)
+    seed_op = torch.full((P,), 9, dtype=torch.int32, device=dev)   # fresh level: restarts
+    gen.begin_level(n, 0, seed_op)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    gen.step(pop)                                    # warm-up: generation 0 (eager)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    first_ms = e0.elapsed_time(e1)
+    s0 = gen.state()
+    graph = gen.capture(pop, G)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0.record(stream)
+        graph.launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = e0.elapsed_time(e1)
+    s1 = gen.state()
+    graph.close()
+    ck = clk.summary()
+    if rank == 0:
+        steps = s1["ls_steps"] - s0["ls_steps"]
+        flop = s1["flop"] - s0["flop"]
+        line = {
+            "metric": "memetic_generations_per_s", "value": G / (total_ms / 1e3),
+            "unit": "generations/s", "n_gpus": 1, "higher_is_better": True,
+            "data": "synthetic", "steps": G, "ms_per_generation": total_ms / G,
+            "first_generation_ms": first_ms,
+            "config": {"workload": f"memetic generation n={n} P={P} 8 islands, tiers "
+                                   f"4000/6666/20000 steps p<=20000, FW 6x500, one CUDA graph "
+                                   f"of {G} generations",
+                       "precision": args.precision, "fw_precision": args.fw_precision},
+            "local_search": {"candidate_steps_per_s": steps / (total_ms / 1e3),
+                             "tflops_algorithmic_overall": flop / (total_ms / 1e3) / 1e12},
+            "search": {"best_F": s1["best_F"], "level_best_F": s1["level_best_F"],
+                       "cells": s1["cells"], "n_cold_last": s1["n_cold"],
+                       "n_med_last": s1["n_med"], "status": s1["status"]},
+            "clocks": {"sm_mhz": ck["sm_mhz"], "sm_max_mhz": ck["sm_max_mhz"],
+                       "reasons": ck["reasons"]},
+        }
+        print(json.dumps(line))
+
+
 # --------------------------------- large ladder -----------------------------
 LADDER = (8192, 16384, 32768, 65536)
 
@@ -615,7 +681,9 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=os.environ.get("SIDON_BENCH_PRECISION", "bf16x3"),
                     choices=["fp32", "bf16x3", "bf16x1"])
-    ap.add_argument("--workload", default="lp_adam", choices=["lp_adam", "islands", "ladder"])
+    ap.add_argument("--workload", default="lp_adam",
+                    choices=["lp_adam", "islands", "ladder", "memetic"])
+    ap.add_argument("--memetic-n", type=int, default=2048)
     ap.add_argument("--ladder-B", type=int, default=32)
     ap.add_argument("--ladder-steps", type=int, default=200)
     ap.add_argument("--ladder-pdhg", type=int, default=100)
@@ -637,6 +705,8 @@ def main() -> None:
         islands_arm(args)
     elif args.workload == "ladder":
         ladder_arm(args)
+    elif args.workload == "memetic":
+        memetic_arm(args)
     else:
         our_arm(args)
 

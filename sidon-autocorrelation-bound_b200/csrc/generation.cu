@@ -43,6 +43,16 @@ int prepare_frank_wolfe_tc(int n_max);
 int prepare_simt(int n_max, bool local_search);
 int tc_n_ok_public(int n);
 size_t smem_local_search_tc(int n);
+int launch_local_search(void* pop, void* mom, void* vel, const long long* offsets,
+                        const int* order, int P, int n_fixed, int n_max, const int* skip,
+                        const int* mode_arr, int iters, double pS, double pE, double lrS,
+                        double lrE, double b1, double b2, int mode_default, int dtype,
+                        cudaStream_t st);
+int launch_local_search_tc_plain(float* pop, float* mom, float* vel, const long long* offsets,
+                                 const int* order, int P, int n_fixed, int n_max, const int* skip,
+                                 const int* mode_arr, int iters, double pS, double pE,
+                                 double lrS, double lrE, double b1, double b2, int mode_default,
+                                 int precision, cudaStream_t st);
 }  // namespace sidon_host
 
 namespace sidon {
@@ -502,6 +512,17 @@ struct sidon_generation_s {
   int n = 0;                   // cells of the current level (0: no level begun)
   G::W w{};
   sidon_generation_views v{};
+  // the three tiers run side by side (disjoint candidates) on streams of
+  // falling priority: cold, medium, warm
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
+  ~sidon_generation_s() {
+    for (int k = 0; k < 3; ++k) {
+      if (side[k]) cudaStreamDestroy(side[k]);
+      if (join[k]) cudaEventDestroy(join[k]);
+    }
+    if (fork) cudaEventDestroy(fork);
+  }
 };
 
 namespace {
@@ -604,13 +625,34 @@ int enqueue(sidon_generation_s* h, float* pop, cudaStream_t st) {
   const int iters[3] = {q.cold_iters, q.med_iters, q.warm_iters};
   const float pa[3] = {6.f, 40.f, 400.f}, pb[3] = {pTop, pTop, pTop * 3.f};
   const float la[3] = {0.085f, 0.040f, 0.012f}, lb[3] = {0.0015f, 0.0010f, 0.0003f};
+  // The tiers touch disjoint candidates (rows of pop, mom, vel), so they run
+  // concurrently, forked from and joined back into the launching stream:
+  // the cold tier's long chains on the highest-priority stream, so that its
+  // CTAs take SMs first, the medium and warm tiers on streams of lower
+  // priority whose CTAs fill the SMs the cold tier leaves idle.  One CTA per
+  // candidate; a skipped candidate's CTA exits at once.  (The reference runs
+  // them one after another, main.cu:627-629; the results are the same.)
+  cudaError_t e = cudaEventRecord(h->fork, st);
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(h->side[k], h->fork, 0);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  const cudaStream_t* tier_st = h->side;
   for (int t = 0; t < 3; ++t) {
     if (iters[t] <= 0) continue;
-    rc = sidon_local_search(pop, w.mom, w.vel, w.skip + (size_t)t * P, w.mode, n, P, iters[t],
-                            pa[t], pb[t], la[t], lb[t], 0.9f, 0.999f, 0, SIDON_F32, c.precision,
-                            st);
+    rc = c.precision == SIDON_PREC_FP32_SIMT
+             ? launch_local_search(pop, w.mom, w.vel, nullptr, nullptr, P, n, n,
+                                   w.skip + (size_t)t * P, w.mode, iters[t], pa[t], pb[t], la[t],
+                                   lb[t], 0.9f, 0.999f, 0, SIDON_F32, tier_st[t])
+             : launch_local_search_tc_plain(pop, w.mom, w.vel, nullptr, nullptr, P, n, n,
+                                            w.skip + (size_t)t * P, w.mode, iters[t], pa[t],
+                                            pb[t], la[t], lb[t], 0.9f, 0.999f, 0, c.precision,
+                                            tier_st[t]);
     if (rc) return rc;
   }
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+    e = cudaEventRecord(h->join[k], h->side[k]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h->join[k], 0);
+  }
+  if (e != cudaSuccess) return set_cuda_error(e);
   int fw_ran = 0;
   if (c.fw_rounds > 0) {
     rc = c.fw_precision == SIDON_PREC_FP32_SIMT
@@ -631,8 +673,7 @@ int enqueue(sidon_generation_s* h, float* pop, cudaStream_t st) {
   rc = launch_variation(pop, w.nxt, SIDON_F32, n, P, w.p1, w.p2, w.op, w.strength, c.seed, 0, st,
                         w.var_gen);
   if (rc) return rc;
-  cudaError_t e = cudaMemcpyAsync(pop, w.nxt, (size_t)P * n * sizeof(float),
-                                  cudaMemcpyDeviceToDevice, st);
+  e = cudaMemcpyAsync(pop, w.nxt, (size_t)P * n * sizeof(float), cudaMemcpyDeviceToDevice, st);
   if (e != cudaSuccess) return set_cuda_error(e);
   G::k_post<<<1, G::BD, 0, st>>>(pop, w, q);
   rc = check_launch();
@@ -721,7 +762,15 @@ int sidon_generation_create(void* workspace, size_t bytes, int n_max, int P,
   v.tabu_hits = w.thits;
   v.tabu_used = w.tused;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  cudaError_t e = cudaMemsetAsync(workspace, 0, L.total, st);
+  int lo = 0, hi = 0;                      // least and greatest stream priority
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+    const int prio = k == 0 ? hi : (k == 1 ? (hi + lo) / 2 : lo);
+    e = cudaStreamCreateWithPriority(&h->side[k], cudaStreamNonBlocking, prio);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join[k], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(workspace, 0, L.total, st);
   if (e != cudaSuccess) {
     delete h;
     return set_cuda_error(e);
@@ -806,7 +855,9 @@ int sidon_generation_capture(sidon_generation h, float* pop, int generations,
     rc = set_cuda_error(e);
   }
   if (rc == SIDON_OK) {
-    e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    // the kernel nodes keep the priorities of the streams they were
+    // captured from
+    e = cudaGraphInstantiate(&g->exec, g->graph, cudaGraphInstantiateFlagUseNodePriority);
     if (e != cudaSuccess) rc = set_cuda_error(e);
   }
   cudaStreamDestroy(st);

@@ -705,6 +705,12 @@ static int launch_local_search_tc_seg(float* pop, float* mom, float* vel, int P,
   return SIDON_OK;
 }
 
+int launch_local_search_tc_plain(float* pop, float* mom, float* vel, const long long* offsets,
+                                 const int* order, int P, int n_fixed, int n_max, const int* skip,
+                                 const int* mode_arr, int iters, double pS, double pE,
+                                 double lrS, double lrE, double b1, double b2, int mode_default,
+                                 int precision, cudaStream_t st);
+
 int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* offsets,
                            const int* order, int P, int n_fixed, int n_max, const int* skip,
                            const int* mode_arr, int iters, double pS, double pE, double lrS,
@@ -725,8 +731,27 @@ int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* 
                                              sm, sw, st);
     if (r != kNotHere) return r;              // else: the one-CTA-per-candidate kernel
   }
-  // one CTA per candidate for a uniform batch; persistent (one CTA per SM)
-  // for a ragged batch
+  return launch_local_search_tc_plain(pop, mom, vel, offsets, order, P, n_fixed, n_max, skip,
+                                      mode_arr, iters, pS, pE, lrS, lrE, b1, b2, mode_default,
+                                      precision, st);
+}
+
+// The fused kernel alone: one CTA per candidate for a uniform batch (CTAs of
+// skipped candidates exit at once, so launches on disjoint candidate sets can
+// share the SMs from concurrent streams); persistent (one CTA per SM) for a
+// ragged batch.
+int launch_local_search_tc_plain(float* pop, float* mom, float* vel, const long long* offsets,
+                                 const int* order, int P, int n_fixed, int n_max, const int* skip,
+                                 const int* mode_arr, int iters, double pS, double pE,
+                                 double lrS, double lrE, double b1, double b2, int mode_default,
+                                 int precision, cudaStream_t st) {
+  int rc = tc_n_ok(n_max);
+  if (rc) return rc;
+  const size_t sm = smem_local_search_tc(n_max);
+  rc = prep_tc((const void*)tc::k_local_search_tc, sm);
+  if (rc) return rc;
+  unsigned int* sw = status_word();
+  if (!sw) return SIDON_ERR_CUDA;
   const int grid = offsets ? (P < sm_count() ? P : sm_count()) : P;
   tc::k_local_search_tc<<<grid, tc::NTHREADS, sm, st>>>(
       pop, mom, vel, offsets, order, P, n_fixed, n_max, skip, mode_arr, iters, (float)pS,
