@@ -540,6 +540,89 @@ def memetic_arm(args) -> None:
         print(json.dumps(line))
 
 
+def reference_memetic_arm(args) -> None:
+    """The same generations with the reference's own implementation: its
+    kernels (kLocalSearch<float> per non-empty tier, kFrankWolfe<float>,
+    kEval, kSupportSig, kVariation<float>) launched through its own helpers
+    (src/main.cu:152-184, 606-741, compiled from its sources into
+    oracle/_ref), one after another with the driver's synchronous copies; the
+    host policy between them is the oracle's restatement of the driver's
+    rules.  Wall clock per generation (the driver is synchronous)."""
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref not built (reference sources absent here)"}))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from sidon_b200 import synth
+    ref = oracle.ref_main()
+    n, P, NI, seed = args.memetic_n, 256, 8, 20260905
+    cold, warm, p_top, fw_rounds, fw_iters = 20000, 4000, 20000.0, 6, 500
+    pol = oracle.GenerationPolicy(P, NI, 2, 6, seed, n)
+    pol.begin_level(n, 0)
+    pop = torch.as_tensor(synth.population("lognormal", n, P, seed=2048), device=dev)
+    nxt, mom, vel = torch.empty_like(pop), torch.empty_like(pop), torch.empty_like(pop)
+    i32 = dict(dtype=torch.int32, device=dev)
+    skip_d, p1_d, p2_d, op_d = (torch.zeros(P, **i32) for _ in range(4))
+    mode_d = torch.as_tensor(pol.mode, device=dev)
+    str_d = torch.zeros(P, dtype=torch.float32, device=dev)
+    fit_d = torch.zeros(P, dtype=torch.float64, device=dev)
+    nact_d, nnz_d = torch.zeros(P, **i32), torch.zeros(P, **i32)
+    sig_d = torch.zeros(P, dtype=torch.int64, device=dev)
+    fit_h, nact_h = np.zeros(P), np.zeros(P, np.int32)
+    sig_h, nnz_h = np.zeros(P, np.uint64), np.zeros(P, np.int32)
+    times = []
+    for g in range(1 + max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tier = np.ascontiguousarray(np.argmin(pol.tiers(cold, cold // 3, warm), axis=0),
+                                    dtype=np.int32)
+        fw = ref.ref_gpu_generation_search(
+            pop.data_ptr(), mom.data_ptr(), vel.data_ptr(), skip_d.data_ptr(), mode_d.data_ptr(),
+            tier.ctypes.data, n, P, cold, warm, p_top, fw_rounds, fw_iters, fit_d.data_ptr(),
+            nact_d.data_ptr(), sig_d.data_ptr(), nnz_d.data_ptr(), fit_h.ctypes.data,
+            nact_h.ctypes.data, sig_h.ctypes.data, nnz_h.ctypes.data)
+        assert fw >= 0, f"reference generation failed ({fw})"
+        host = pop.cpu().numpy()
+        plan = pol.select(host, fit_h, nact_h, sig_h, nnz_h, fw, fw_rounds, fw_iters)
+        pop.copy_(torch.from_numpy(host))
+        rc = ref.ref_gpu_generation_vary(
+            pop.data_ptr(), nxt.data_ptr(), n, P, p1_d.data_ptr(), p2_d.data_ptr(),
+            op_d.data_ptr(), str_d.data_ptr(), plan["p1"].ctypes.data, plan["p2"].ctypes.data,
+            plan["op"].ctypes.data, plan["strength"].ctypes.data, seed, int(pol.var_gen[0]))
+        assert rc == 0, f"reference variation failed ({rc})"
+        pop, nxt = nxt, pop
+        host = pop.cpu().numpy()
+        pol.post(host)
+        pop.copy_(torch.from_numpy(host))
+        child = np.zeros(P)
+        if pol.s.gen > 0 and pol.s.gen % 5 == 0:
+            assert ref.ref_gpu_eval(pop.data_ptr(), n, P, fit_d.data_ptr(), nact_d.data_ptr(),
+                                    1e-4, None) == 0
+            child = fit_d.cpu().numpy()
+        pol.credit(child)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    timed = times[1:]
+    sec = sum(timed) / len(timed)
+    print(json.dumps({
+        "impl": "reference", "metric": "memetic_generations_per_s", "value": 1.0 / sec,
+        "unit": "generations/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+        "steps": len(timed), "ms_per_generation": 1e3 * sec, "first_generation_ms": 1e3 * times[0],
+        "config": {"workload": f"memetic generation n={n} P={P} 8 islands, tiers "
+                               f"4000/6666/20000 steps p<=20000, FW 6x500",
+                   "kernels": "reference kLocalSearch/kFrankWolfe/kEval/kSupportSig/"
+                              "kVariation<float>, sm_100a build of its sources, sequential"},
+        "search": {"best_F": pol.s.best_F, "cells": pol.s.cells},
+    }))
+
+
 # --------------------------------- large ladder -----------------------------
 LADDER = (8192, 16384, 32768, 65536)
 
@@ -700,7 +783,10 @@ def main() -> None:
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
-        reference_arm(args)
+        if args.workload == "memetic":
+            reference_memetic_arm(args)
+        else:
+            reference_arm(args)
     elif args.workload == "islands":
         islands_arm(args)
     elif args.workload == "ladder":

@@ -49,4 +49,63 @@ int ref_gpu_eval(const float* pop, int n, int P, double* fit, int* nact, double 
   return (int)cudaGetLastError();
 }
 
+// The numeric device steps of one generation of the reference driver
+// (src/main.cu:606-651), launched through its own helpers on a Gpu view of
+// the caller's buffers: the non-empty anneal tiers in order (skip masks
+// copied host -> device as launchTier does), the Frank-Wolfe step, kEval,
+// kSupportSig, and the synchronous copies of fit / nact / sig / nnz to the
+// host.  tier[P] (host) holds 0 cold, 1 medium, 2 warm; mode (device) is
+// modeArr.  Returns 1 when the Frank-Wolfe step ran, 0 when it did not fit,
+// -cudaError on failure.
+int ref_gpu_generation_search(float* pop, float* mom, float* vel, int* skip_dev, int* mode_dev,
+                              const int* tier, int n, int P, int cold_iters, int lsIters,
+                              float pTop, int fwRounds, int fwIters, double* fit_dev,
+                              int* nact_dev, unsigned long long* sig_dev, int* nnz_dev,
+                              double* fit_h, int* nact_h, unsigned long long* sig_h,
+                              int* nnz_h) {
+  Gpu g;
+  g.n = n; g.P = P; g.pop = pop; g.mom = mom; g.vel = vel; g.fit = fit_dev; g.nact = nact_dev;
+  g.modeArr = mode_dev; g.skip = skip_dev; g.sig = sig_dev; g.nnz = nnz_dev;
+  int cnt[3] = {0, 0, 0};
+  for (int p = 0; p < P; ++p) ++cnt[tier[p]];
+  std::vector<int> sk(P);
+  auto launchTier = [&](int t, int iters, float pa, float pb, float la, float lb) {
+    for (int p = 0; p < P; ++p) sk[p] = tier[p] == t ? 0 : 1;
+    cudaMemcpy(g.skip, sk.data(), P * sizeof(int), cudaMemcpyHostToDevice);
+    runLocalSearch(g, iters, pa, pb, la, lb, g.modeArr, g.skip);
+  };
+  if (cnt[0]) launchTier(0, cold_iters, 6.f, pTop, 0.085f, 0.0015f);
+  if (cnt[1]) launchTier(1, cold_iters / 3, 40.f, pTop, 0.040f, 0.0010f);
+  if (cnt[2]) launchTier(2, lsIters, 400.f, pTop * 3.f, 0.012f, 0.0003f);
+  int optin = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const bool fwOk = fwRounds > 0 && runFrankWolfe(g, fwRounds, fwIters, 12, 0.30f, optin);
+  runEval(g);
+  runSig(g);
+  cudaMemcpy(fit_h, g.fit, P * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaMemcpy(nact_h, g.nact, P * sizeof(int), cudaMemcpyDeviceToHost);
+  cudaMemcpy(sig_h, g.sig, P * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+  cudaMemcpy(nnz_h, g.nnz, P * sizeof(int), cudaMemcpyDeviceToHost);
+  const cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return -(int)e;
+  return fwOk ? 1 : 0;
+}
+
+// The variation launch of the generation (src/main.cu:732-741): plan copied
+// host -> device, kVariation<float> from pop into nxt.
+int ref_gpu_generation_vary(const float* pop, float* nxt, int n, int P, int* p1_dev, int* p2_dev,
+                            int* op_dev, float* str_dev, const int* p1, const int* p2,
+                            const int* op, const float* str, unsigned long long seed,
+                            unsigned long long gen) {
+  cudaMemcpy(p1_dev, p1, P * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(p2_dev, p2, P * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(op_dev, op, P * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(str_dev, str, P * sizeof(float), cudaMemcpyHostToDevice);
+  const size_t smv = sizeof(float) * ((size_t)2 * n + 64 + 128);
+  setSmemLimit((const void*)kVariation<float>, smv);
+  kVariation<float><<<P, BD, smv>>>(pop, nxt, n, P, p1_dev, p2_dev, op_dev, str_dev, seed, gen);
+  return (int)cudaGetLastError();
+}
+
 }  // extern "C"
