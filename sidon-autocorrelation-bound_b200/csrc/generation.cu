@@ -625,44 +625,51 @@ int enqueue(sidon_generation_s* h, float* pop, cudaStream_t st) {
   const int iters[3] = {q.cold_iters, q.med_iters, q.warm_iters};
   const float pa[3] = {6.f, 40.f, 400.f}, pb[3] = {pTop, pTop, pTop * 3.f};
   const float la[3] = {0.085f, 0.040f, 0.012f}, lb[3] = {0.0015f, 0.0010f, 0.0003f};
-  // The tiers touch disjoint candidates (rows of pop, mom, vel), so they run
-  // concurrently, forked from and joined back into the launching stream:
-  // the cold tier's long chains on the highest-priority stream, so that its
-  // CTAs take SMs first, the medium and warm tiers on streams of lower
-  // priority whose CTAs fill the SMs the cold tier leaves idle.  One CTA per
-  // candidate; a skipped candidate's CTA exits at once.  (The reference runs
-  // them one after another, main.cu:627-629; the results are the same.)
+  // Every step up to the evaluation acts on each candidate alone, and the
+  // tiers are disjoint sets of candidates (rows of pop, mom, vel), so each
+  // tier runs its local search and then its Frank-Wolfe step on its own
+  // stream, forked from and joined back into the launching stream: the cold
+  // tier's long chains on the highest-priority stream, so that its CTAs take
+  // SMs first, the medium and warm tiers (and their Frank-Wolfe steps) on
+  // streams of lower priority whose CTAs fill the SMs the cold chains leave
+  // idle.  One CTA per candidate; a skipped candidate's CTA exits at once.
+  // (The reference runs the tiers one after another and then the
+  // Frank-Wolfe step on everybody, main.cu:627-639; the results are the
+  // same.)
   cudaError_t e = cudaEventRecord(h->fork, st);
   for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(h->side[k], h->fork, 0);
   if (e != cudaSuccess) return set_cuda_error(e);
-  const cudaStream_t* tier_st = h->side;
+  int fw_ran = 0;
   for (int t = 0; t < 3; ++t) {
-    if (iters[t] <= 0) continue;
-    rc = c.precision == SIDON_PREC_FP32_SIMT
-             ? launch_local_search(pop, w.mom, w.vel, nullptr, nullptr, P, n, n,
-                                   w.skip + (size_t)t * P, w.mode, iters[t], pa[t], pb[t], la[t],
-                                   lb[t], 0.9f, 0.999f, 0, SIDON_F32, tier_st[t])
-             : launch_local_search_tc_plain(pop, w.mom, w.vel, nullptr, nullptr, P, n, n,
-                                            w.skip + (size_t)t * P, w.mode, iters[t], pa[t],
-                                            pb[t], la[t], lb[t], 0.9f, 0.999f, 0, c.precision,
-                                            tier_st[t]);
-    if (rc) return rc;
+    const cudaStream_t ts = h->side[t];
+    const int* skip = w.skip + (size_t)t * P;
+    if (iters[t] > 0) {
+      rc = c.precision == SIDON_PREC_FP32_SIMT
+               ? launch_local_search(pop, w.mom, w.vel, nullptr, nullptr, P, n, n, skip, w.mode,
+                                     iters[t], pa[t], pb[t], la[t], lb[t], 0.9f, 0.999f, 0,
+                                     SIDON_F32, ts)
+               : launch_local_search_tc_plain(pop, w.mom, w.vel, nullptr, nullptr, P, n, n, skip,
+                                              w.mode, iters[t], pa[t], pb[t], la[t], lb[t], 0.9f,
+                                              0.999f, 0, c.precision, ts);
+      if (rc) return rc;
+    }
+    if (c.fw_rounds > 0 && (t == 0 || fw_ran)) {
+      // the dead Adam moments of the tier's rows are the tensor-core step's
+      // g / gbar rows
+      rc = c.fw_precision == SIDON_PREC_FP32_SIMT
+               ? sidon_frank_wolfe(pop, skip, n, P, c.fw_rounds, c.fw_iters, c.fw_nT,
+                                   c.fw_t_max, 0.f, 0.f, ts)
+               : sidon_frank_wolfe_tc(pop, w.mom, w.vel, skip, n, P, c.fw_rounds, c.fw_iters,
+                                      c.fw_nT, c.fw_t_max, 0.f, 0.f, c.fw_precision, ts);
+      if (rc == SIDON_OK) fw_ran = 1;
+      else if (rc != SIDON_ERR_SMEM && rc != SIDON_ERR_N) return rc;   // main.cu:173: skipped
+    }
   }
   for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
     e = cudaEventRecord(h->join[k], h->side[k]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h->join[k], 0);
   }
   if (e != cudaSuccess) return set_cuda_error(e);
-  int fw_ran = 0;
-  if (c.fw_rounds > 0) {
-    rc = c.fw_precision == SIDON_PREC_FP32_SIMT
-             ? sidon_frank_wolfe(pop, nullptr, n, P, c.fw_rounds, c.fw_iters, c.fw_nT,
-                                 c.fw_t_max, 0.f, 0.f, st)
-             : sidon_frank_wolfe_tc(pop, w.mom, w.vel, nullptr, n, P, c.fw_rounds, c.fw_iters,
-                                    c.fw_nT, c.fw_t_max, 0.f, 0.f, c.fw_precision, st);
-    if (rc == SIDON_OK) fw_ran = 1;
-    else if (rc != SIDON_ERR_SMEM && rc != SIDON_ERR_N) return rc;   // main.cu:173: skipped
-  }
   rc = sidon_eval(pop, SIDON_F32, n, P, w.fit, w.nact, 1e-4, st);
   if (rc) return rc;
   rc = sidon_support_sig(pop, SIDON_F32, n, P, 0.02f, w.sig, w.nnz, st);
