@@ -536,6 +536,63 @@ SIDON_API int sidon_generation_capture(sidon_generation h, float* pop, int gener
 SIDON_API int sidon_generation_read_state(sidon_generation h, sidon_generation_state* out,
                                           void* stream);
 
+/* ------------------------------ search driver ------------------------------
+ * Host seeding of a ladder level (src/main.cu:483-553), on host buffers:
+ * pop [P][n] fp32 and seed_op [P] (the operator record that picks each
+ * slot's first anneal tier: 20 carried over, 9 fresh).  Row p refines row p
+ * of prev ([P][n_prev], NULL at the first level; duplicate when n = 2 n_prev,
+ * else nearest-neighbour resample), the last 20 % of the rows start afresh;
+ * an empty row gets the structured prior with probability 0.6, else a smooth
+ * random profile; rows are normalised to sum 1.  Draws: std::mt19937_64
+ * seeded with seed + level in the reference's call order. */
+SIDON_API int sidon_seed_level(float* pop, int* seed_op, int n, int P, int level,
+                               const float* prev, int n_prev, unsigned long long seed);
+
+typedef struct sidon_search_progress {
+  double seconds;            /* wall clock since sidon_search began */
+  int level, n, gen;         /* ladder level, its cells, generations done at it */
+  int improved;              /* the incumbent improved since the previous report */
+  double best_F;             /* incumbent F */
+  double level_best_F;
+  long long evals, ls_steps, fw_steps;
+  double pflop;              /* algorithmic PFLOP so far */
+  int cells;                 /* distinct support signatures seen */
+  int best_nactive, best_nnz;
+  int n_cold, n_med;
+} sidon_search_progress;
+
+/* Called after every replay of gens_per_graph generations with the progress
+ * and the incumbent's heights (host fp64, best_n cells). */
+typedef void (*sidon_search_callback)(const sidon_search_progress* progress, const double* best,
+                                      int best_n, void* user);
+
+typedef struct sidon_search_config {
+  const int* ladder;         /* host [n_levels]: cells per level (reference: 64 ... 2048) */
+  int n_levels;
+  int P;                     /* population (256) */
+  double seconds;            /* wall-clock budget; 82 % split over the levels by 1.85^l */
+  int gens_per_level;        /* 0: each level runs until its time share is spent */
+  int gens_per_graph;        /* generations per CUDA-graph replay between budget checks */
+  int polish_iters;          /* fp64 polish steps over 6 passes (40000) */
+  int polish_top;            /* polish candidates (8) */
+  sidon_generation_config gen;
+} sidon_search_config;
+
+/* The reference driver's whole search (src/main.cu:400-874): resume
+ * adoption (the resumed vector is the incumbent at once, coarser levels are
+ * dropped), the ladder levels with their time shares, per level the host
+ * seeding, the incumbent injected into slot 0 and the resumed vector into
+ * slot 1, sidon_generation_* generations replayed from a CUDA graph until
+ * the level's share is spent, the population carried to the next level;
+ * then the fp64 polish of the incumbent (sidon_polish, 6 passes, K =
+ * polish_top basin-hopping starts from mt19937_64(seed ^ 0xABCDEF)).
+ * Writes the incumbent (up to best_cap cells of best, host fp64), its cell
+ * count and F = max(search F, hostF recheck) (main.cu:865-873).  Allocates
+ * and frees its own device buffers; returns a status. */
+SIDON_API int sidon_search(const sidon_search_config* cfg, const double* resume, int n_resume,
+                           double* best, int best_cap, int* best_n, double* best_F,
+                           sidon_search_callback cb, void* user);
+
 #ifdef __cplusplus
 }
 #endif

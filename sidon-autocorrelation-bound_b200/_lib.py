@@ -76,6 +76,8 @@ SIGNATURES = {
     "sidon_generation_step": (_i, [_vp, _vp, _vp]),
     "sidon_generation_capture": (_i, [_vp, _vp, _i, _vp]),
     "sidon_generation_read_state": (_i, [_vp, _vp, _vp]),
+    "sidon_seed_level": (_i, [_vp, _vp, _i, _i, _i, _vp, _i, C.c_ulonglong]),
+    "sidon_search": (_i, [_vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp]),
 }
 
 
@@ -140,6 +142,31 @@ class GenerationViews(C.Structure):
         "fit", "parent_fit", "child_fit", "nactive", "sig", "nnz", "p1", "p2", "op", "strength",
         "cur_op", "mode", "rank", "tier_skip", "best_row", "state", "tabu_key", "tabu_best",
         "tabu_hits", "tabu_used")]
+
+
+class SearchProgress(C.Structure):
+    """struct sidon_search_progress."""
+
+    _fields_ = [
+        ("seconds", _d), ("level", _i), ("n", _i), ("gen", _i), ("improved", _i),
+        ("best_F", _d), ("level_best_F", _d),
+        ("evals", C.c_longlong), ("ls_steps", C.c_longlong), ("fw_steps", C.c_longlong),
+        ("pflop", _d), ("cells", _i), ("best_nactive", _i), ("best_nnz", _i),
+        ("n_cold", _i), ("n_med", _i),
+    ]
+
+
+SEARCH_CALLBACK = C.CFUNCTYPE(None, C.POINTER(SearchProgress), C.POINTER(_d), _i, _vp)
+
+
+class SearchConfig(C.Structure):
+    """struct sidon_search_config."""
+
+    _fields_ = [
+        ("ladder", C.POINTER(_i)), ("n_levels", _i), ("P", _i), ("seconds", _d),
+        ("gens_per_level", _i), ("gens_per_graph", _i), ("polish_iters", _i),
+        ("polish_top", _i), ("gen", GenerationConfig),
+    ]
 
 
 _lock = threading.Lock()

@@ -769,3 +769,48 @@ class Generation:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# search driver (sidon_seed_level, sidon_search)
+# ---------------------------------------------------------------------------
+def seed_level(n: int, P: int, level: int, prev: np.ndarray | None = None,
+               seed: int = 20260905) -> tuple[np.ndarray, np.ndarray]:
+    """Host seeding of a ladder level (src/main.cu:483-553): (pop float32
+    [P][n], seed_op int32 [P]); prev is the previous level's population."""
+    pop = np.zeros((P, n), np.float32)
+    op = np.zeros(P, np.int32)
+    pv = None if prev is None else np.ascontiguousarray(prev, dtype=np.float32)
+    _lib.call("sidon_seed_level", pop.ctypes.data, op.ctypes.data, int(n), int(P), int(level),
+              None if pv is None else pv.ctypes.data, 0 if pv is None else pv.shape[1],
+              int(seed) & 0xFFFFFFFFFFFFFFFF)
+    return pop, op
+
+
+def search(ladder=(64, 128, 256, 512, 1024, 2048), P: int = 256, seconds: float = 600.0,
+           gens_per_level: int = 0, gens_per_graph: int = 5, polish_iters: int = 40000,
+           polish_top: int = 8, gen: _lib.GenerationConfig | None = None, resume=None,
+           progress=None) -> tuple[np.ndarray, float]:
+    """The reference driver's whole search (src/main.cu:400-874) in one call:
+    returns (incumbent heights fp64, F).  progress(dict, best ndarray) is
+    called after every replay of gens_per_graph generations."""
+    lad = (C.c_int * len(ladder))(*[int(x) for x in ladder])
+    cfg = _lib.SearchConfig(C.cast(lad, C.POINTER(C.c_int)), len(ladder), int(P), float(seconds),
+                            int(gens_per_level), int(gens_per_graph), int(polish_iters),
+                            int(polish_top), gen if gen is not None else generation_config())
+    res = None if resume is None else np.ascontiguousarray(resume, dtype=np.float64)
+    cap = max(max(ladder), 0 if res is None else res.size)
+    out = np.zeros(cap, np.float64)
+    nb, fb = C.c_int(0), C.c_double(0.0)
+
+    def _cb(pr, best, best_n, _user):
+        if progress is not None:
+            p = pr.contents
+            d = {k: getattr(p, k) for k, _ in _lib.SearchProgress._fields_}
+            progress(d, np.ctypeslib.as_array(best, shape=(best_n,)).copy() if best_n else None)
+
+    cb = _lib.SEARCH_CALLBACK(_cb)
+    _lib.call("sidon_search", C.byref(cfg), None if res is None else res.ctypes.data,
+              0 if res is None else res.size, out.ctypes.data, cap, C.byref(nb), C.byref(fb),
+              cb, None)
+    return out[:nb.value].copy(), fb.value

@@ -203,3 +203,40 @@ def test_capi_generation_argument_checks(lib):
                                        C.byref(h), None) == _lib.ERR_ARG  # misaligned
     assert lib.sidon_generation_step(None, None, None) == _lib.ERR_ARG
     assert lib.sidon_generation_destroy(None) == _lib.OK
+
+
+def test_seed_level_first_level_and_carry_over():
+    from sidon_b200 import kernels
+    P, n = 20, 64
+    pop, op = kernels.seed_level(n, P, 0, seed=11)
+    assert (op == 9).all()                                   # every slot a fresh start
+    assert (pop >= 0).all() and np.allclose(pop.sum(axis=1), 1.0, atol=1e-5)
+    again, _ = kernels.seed_level(n, P, 0, seed=11)
+    assert np.array_equal(pop, again)                        # deterministic in the seed
+    other, _ = kernels.seed_level(n, P, 0, seed=12)
+    assert not np.array_equal(pop, other)
+    # n -> 2n: rows below 0.8 P are the refined carry-over, the rest fresh
+    up, op2 = kernels.seed_level(2 * n, P, 1, prev=pop, seed=11)
+    keep = int(0.8 * P)
+    assert (op2[:keep] == 20).all() and (op2[keep:] == 9).all()
+    for p in range(keep):
+        want = (pop[p].astype(np.float64) / pop[p].astype(np.float64).sum()).astype(np.float32)
+        assert np.array_equal(up[p, 0::2], up[p, 1::2])
+        np.testing.assert_allclose(up[p, 0::2] * 2, want, rtol=1e-6)
+    # arbitrary ratio: nearest-neighbour resample of the previous row
+    rs, _ = kernels.seed_level(96, P, 1, prev=pop, seed=11)
+    src = pop[3, [min(n - 1, i * n // 96) for i in range(96)]].astype(np.float64)
+    np.testing.assert_allclose(rs[3], src / src.sum(), rtol=1e-6)
+
+
+def test_seed_level_fresh_rows_follow_the_reference_families():
+    """Fresh rows are either the structured prior (a dominant endpoint atom
+    and a hard zero gap) or a smooth random profile (no exact gap needed)."""
+    from sidon_b200 import kernels
+    pop, _ = kernels.seed_level(512, 64, 0, seed=3)
+    structured = 0
+    for row in pop:
+        end = max(row[0], row[-1])
+        if end > 10 * np.median(row[row > 0]) and (row == 0).sum() >= 0.04 * row.size:
+            structured += 1
+    assert 20 <= structured <= 58          # about 60 % of 64
