@@ -97,10 +97,9 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
 #pragma unroll
     for (int u = 0; u < kCellsPerThread; ++u) {
       const int i = threadIdx.x + u * NTHREADS;
-      if (i < n) {
-        pm[u] = __ldcg(mg + i);
-        pv[u] = __ldcg(vg + i);
-      }
+      if (i >= n) break;        // the cells of a thread ascend: none further
+      pm[u] = __ldcg(mg + i);
+      pv[u] = __ldcg(vg + i);
     }
   }
   fence_before();
@@ -114,7 +113,7 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
 #pragma unroll
   for (int u = 0; u < kCellsPerThread; ++u) {
     const int i = threadIdx.x + u * NTHREADS;
-    if (i >= n) continue;
+    if (i >= n) break;          // (a predicated tail would cost all 38 bodies at small n)
     const float gi = S.cb[pidx(i)] * invR - M;
     const float x0 = S.sa[pidx(i)];
     float x;
