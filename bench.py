@@ -2,7 +2,7 @@
 adjoint correlation + update) at n = 8400 cells, B = 256 candidates per GPU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|bf16x1|fp32]
-                    [--impl ours|reference] [--workload lp_adam|islands|ladder|memetic]
+                    [--impl ours|reference] [--workload lp_adam|islands|ladder|memetic|micro]
 
 One *step* = every candidate of the batch advances one Adam step.  The timed
 region is ONE launch of the fused local-search kernel running K steps (the
@@ -474,6 +474,123 @@ def islands_arm(args) -> None:
         print(json.dumps(line))
 
 
+# ------------------------- the reference's own micro-benchmark ---------------
+MICRO_N = (128, 256, 512, 1024, 2048, 4096)
+
+
+def _micro_setup(n: int, seed: int = 1):
+    """The settings of src/main.cu:294-320: P = max(32, min(512, 4M / n)),
+    heights uniform in [0.2, 1) (seeded PCG64 standing in for its
+    mt19937(1)), a 10-iteration warm-up at p = 8, then 100 iterations with p
+    8 -> 200 and lr 0.05 -> 0.005; TFLOP/s = 4 n^2 P iters / time."""
+    P = max(32, min(512, 4 * 1024 * 1024 // n))
+    h = np.random.default_rng(seed).uniform(0.2, 1.0, (P, n)).astype(np.float32)
+    return P, h
+
+
+def _micro_line(impl: str, rows: list, extra: dict) -> dict:
+    return {"metric": "micro_lp_adam_tflops", "impl": impl, "unit": "TFLOP/s",
+            "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": "src/main.cu:294-320 benchmark: n = 128 .. 4096, "
+                                   "P = max(32, min(512, 4M/n)), 100 local-search iterations "
+                                   "p 8->200, lr 0.05->0.005, then one fp64 evaluation",
+                       **extra},
+            "rows": rows}
+
+
+def micro_arm(args) -> None:
+    """Our kernels on the reference's own benchmark (--bench of src/main.cu):
+    the tensor-core step (BF16x3) and the FP32 SIMT step per n, and the fp64
+    evaluation; CUDA events on the launching stream."""
+    import torch
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import sidon_b200
+    sidon_b200.load(build=not (ROOT / "sidon-autocorrelation-bound_b200" / "libsidon_b200.so").exists())
+    from sidon_b200 import kernels
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1e3
+
+    rows = []
+    for n in MICRO_N:
+        P, h = _micro_setup(n)
+        row = {"n": n, "P": P}
+        flop = 4.0 * n * n * P * 100
+        for prec in ("bf16x3", "fp32"):
+            x = torch.as_tensor(h, device=dev)
+            mom, vel = torch.empty_like(x), torch.empty_like(x)
+            kernels.run_local_search(x, 10, 8.0, 8.0, 0.01, 0.01, mom=mom, vel=vel, precision=prec)
+            dt = timed(lambda: kernels.run_local_search(x, 100, 8.0, 200.0, 0.05, 0.005, mom=mom,
+                                                        vel=vel, precision=prec))
+            row[f"ls_ms_{prec}"] = dt * 1e3
+            row[f"tflops_{prec}"] = flop / dt / 1e12
+        F = torch.empty(P, dtype=torch.float64, device=dev)
+        nact = torch.empty(P, dtype=torch.int32, device=dev)
+        kernels.run_eval(x, out_F=F, out_nactive=nact)
+        row["eval_ms"] = timed(lambda: kernels.run_eval(x, out_F=F, out_nactive=nact)) * 1e3
+        rows.append(row)
+    print(json.dumps(_micro_line("ours", rows, {"precision": "bf16x3 and fp32 SIMT"})))
+
+
+def reference_micro_arm(args) -> None:
+    """The reference's kernels on its own benchmark: kLocalSearch<float> and
+    kEval<float,double> built for sm_100a from its sources (oracle/_ref),
+    launched as runLocalSearch / runEval do."""
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref not built (reference sources absent here)"}))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ref = oracle.ref_main()
+    stream = torch.cuda.current_stream()
+    rows = []
+    for n in MICRO_N:
+        P, h = _micro_setup(n)
+        x = torch.as_tensor(h, device=dev)
+        mom, vel = torch.empty_like(x), torch.empty_like(x)
+        F = torch.empty(P, dtype=torch.float64, device=dev)
+        nact = torch.empty(P, dtype=torch.int32, device=dev)
+        assert ref.ref_gpu_local_search(x.data_ptr(), mom.data_ptr(), vel.data_ptr(), n, P, 10,
+                                        8.0, 8.0, 0.01, 0.01, None) == 0
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        rc = ref.ref_gpu_local_search(x.data_ptr(), mom.data_ptr(), vel.data_ptr(), n, P, 100,
+                                      8.0, 200.0, 0.05, 0.005, None)
+        b.record(stream)
+        torch.cuda.synchronize()
+        assert rc == 0
+        dt = a.elapsed_time(b) / 1e3
+        a.record(stream)
+        rc = ref.ref_gpu_eval(x.data_ptr(), n, P, F.data_ptr(), nact.data_ptr(), 1e-4, None)
+        b.record(stream)
+        torch.cuda.synchronize()
+        assert rc == 0
+        rows.append({"n": n, "P": P, "ls_ms": dt * 1e3,
+                     "tflops": 4.0 * n * n * P * 100 / dt / 1e12,
+                     "eval_ms": a.elapsed_time(b)})
+    print(json.dumps(_micro_line("reference", rows, {"kernels": "reference kLocalSearch<float>, "
+                                                     "kEval<float,double>, sm_100a build"})))
+
+
 # ----------------------------- memetic generations ---------------------------
 def memetic_arm(args) -> None:
     """The reference driver's generation (src/main.cu:586-785) at its default
@@ -765,7 +882,7 @@ def main() -> None:
     ap.add_argument("--precision", default=os.environ.get("SIDON_BENCH_PRECISION", "bf16x3"),
                     choices=["fp32", "bf16x3", "bf16x1"])
     ap.add_argument("--workload", default="lp_adam",
-                    choices=["lp_adam", "islands", "ladder", "memetic"])
+                    choices=["lp_adam", "islands", "ladder", "memetic", "micro"])
     ap.add_argument("--memetic-n", type=int, default=2048)
     ap.add_argument("--ladder-B", type=int, default=32)
     ap.add_argument("--ladder-steps", type=int, default=200)
@@ -785,6 +902,8 @@ def main() -> None:
     if args.impl == "reference":
         if args.workload == "memetic":
             reference_memetic_arm(args)
+        elif args.workload == "micro":
+            reference_micro_arm(args)
         else:
             reference_arm(args)
     elif args.workload == "islands":
@@ -793,6 +912,8 @@ def main() -> None:
         ladder_arm(args)
     elif args.workload == "memetic":
         memetic_arm(args)
+    elif args.workload == "micro":
+        micro_arm(args)
     else:
         our_arm(args)
 

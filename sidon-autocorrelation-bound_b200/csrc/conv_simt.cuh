@@ -66,18 +66,16 @@ struct Team {
   __device__ bool active() const { return t0 < nt; }
 };
 
-// b_k = sum_i x_i y_{k-i}, k in [0, 2n-1).  epi(k, value) is called once per
-// output k < 2n-1 by the lane that owns it.
+// b_k = sum_i x_i y_{k-i}, k in [0, 2n-1), by NW warps of which this lane's
+// warp is number wid.  epi(k, value) is called once per output k < 2n-1 by
+// the lane that owns it.
 template <int TK, bool FUSED, typename T, typename Epi>
-__device__ __forceinline__ void conv_warp_tiles(const T* __restrict__ x, const T* __restrict__ y,
-                                                int n, const Team& tm, Epi&& epi) {
+__device__ __forceinline__ void conv_tiles(const T* __restrict__ x, const T* __restrict__ y, int n,
+                                           int wid, int NW, int lane, Epi&& epi) {
   constexpr int W = 32 * TK;
-  if (!tm.active()) return;
   const int nb = 2 * n - 1;
   const int Q = (nb + W - 1) / W;
   const int c = (n - 1) / W;
-  const int NW = tm.nt >> 5;
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int r = 0;; ++r) {
     const int p = r * NW + ((r & 1) ? (NW - 1 - wid) : wid);
     if (p >= Q) break;
@@ -109,16 +107,23 @@ __device__ __forceinline__ void conv_warp_tiles(const T* __restrict__ x, const T
   }
 }
 
-// G_i = sum_j c_{i+j} a_j, i in [0, n).  epi(i, value) once per i < n.
-// c must be valid (zero) up to index 2n - 2 + margin.
-template <int TI, typename T, typename Epi>
-__device__ __forceinline__ void corr_warp_tiles(const T* __restrict__ a, const T* __restrict__ cc,
+// conv_tiles over the warps of a team
+template <int TK, bool FUSED, typename T, typename Epi>
+__device__ __forceinline__ void conv_warp_tiles(const T* __restrict__ x, const T* __restrict__ y,
                                                 int n, const Team& tm, Epi&& epi) {
-  constexpr int W = 32 * TI;
   if (!tm.active()) return;
+  conv_tiles<TK, FUSED>(x, y, n, (int)(threadIdx.x >> 5), tm.nt >> 5, (int)(threadIdx.x & 31),
+                        epi);
+}
+
+// G_i = sum_j c_{i+j} a_j, i in [0, n), by NW warps (this lane's is wid).
+// epi(i, value) once per i < n.  c must be valid (zero) up to index
+// 2n - 2 + margin.
+template <int TI, typename T, typename Epi>
+__device__ __forceinline__ void corr_tiles(const T* __restrict__ a, const T* __restrict__ cc, int n,
+                                           int wid, int NW, int lane, Epi&& epi) {
+  constexpr int W = 32 * TI;
   const int Q = (n + W - 1) / W;
-  const int NW = tm.nt >> 5;
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int trips = (n + TI - 1) / TI;
   for (int q = wid; q < Q; q += NW) {
     const int i0 = q * W + lane * TI;
@@ -142,6 +147,14 @@ __device__ __forceinline__ void corr_warp_tiles(const T* __restrict__ a, const T
     for (int s = 0; s < TI; ++s)
       if (i0 + s < n) epi(i0 + s, acc[s]);
   }
+}
+
+// corr_tiles over the warps of a team
+template <int TI, typename T, typename Epi>
+__device__ __forceinline__ void corr_warp_tiles(const T* __restrict__ a, const T* __restrict__ cc,
+                                                int n, const Team& tm, Epi&& epi) {
+  if (!tm.active()) return;
+  corr_tiles<TI>(a, cc, n, (int)(threadIdx.x >> 5), tm.nt >> 5, (int)(threadIdx.x & 31), epi);
 }
 
 // warps a CTA should have so one round of correlation tiles covers n

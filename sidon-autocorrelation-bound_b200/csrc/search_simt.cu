@@ -32,6 +32,41 @@ __device__ __forceinline__ void zero_fill(T* p, int count) {
 }
 
 // ------------------------------ local search ------------------------------
+// The step's elementwise pieces, shared by the CTA and the warp kernels so
+// that both compile them to the same arithmetic.
+// weight c_k = (1+d)^(p-1) with d = (b_k - M)/M (0 for d = -1); adds
+// c_k (1+d) to *r
+template <typename T>
+__device__ __forceinline__ T ls_weight(T b, T M, T pexp, T* r) {
+  const T d = (b - M) / M;
+  const T cw = d > T(-1) ? pow_from_d(d, pexp - T(1)) : T(0);
+  *r += cw * (T(1) + d);
+  return cw;
+}
+// Adam (mode 0, moments m / v updated in place) or mirror (mode 1) step of
+// height x0 with gradient term g_i = G/R - M, then the projection
+template <typename T>
+__device__ __forceinline__ T ls_update(T x0, T G, T R, T M, int mode, T lr, T lrn, T beta1, T beta2,
+                                       T bc1, T bc2, T* m, T* v) {
+  const T gi = G / R - M;
+  T x;
+  if (mode == 0) {
+    const T mm = dev_fma(beta1, *m, (T(1) - beta1) * gi);
+    const T vv = dev_fma(beta2, *v, (T(1) - beta2) * gi * gi);
+    *m = mm;
+    *v = vv;
+    const T step = lrn * (mm * bc1) / (dev_sqrt(vv * bc2) + T(1e-30));
+    x = x0 - step;
+    if (x < T(0)) x = T(0);
+  } else {
+    T e = -lr * (gi / M);
+    if (e > T(4)) e = T(4);
+    if (e < T(-4)) e = T(-4);
+    x = x0 * dev_exp(e);
+  }
+  return x;
+}
+
 template <typename T, int TK>
 __global__ void __launch_bounds__(1024, 1)
 k_local_search(T* pop, T* mom, T* vel, const long long* __restrict__ offsets,
@@ -80,12 +115,7 @@ k_local_search(T* pop, T* mom, T* vel, const long long* __restrict__ offsets,
 
     // c_k = (1+d)^(p-1), R = sum c_k (1+d), d = (b_k - M)/M
     T rloc = T(0);
-    for (int k = tm.t0; k < nb; k += tm.nt) {
-      const T d = (sC[k] - M) / M;
-      const T cw = d > T(-1) ? pow_from_d(d, pexp - T(1)) : T(0);
-      rloc += cw * (T(1) + d);
-      sC[k] = cw;
-    }
+    for (int k = tm.t0; k < nb; k += tm.nt) sC[k] = ls_weight(sC[k], M, pexp, &rloc);
     const T R = block_sum(rloc, sRed);      // (barrier inside: c complete)
 
     b1t *= beta1;
@@ -96,23 +126,7 @@ k_local_search(T* pop, T* mom, T* vel, const long long* __restrict__ offsets,
     // G = corr(c, a); update fused into the epilogue; the new heights are
     // staged in the candidate's own row of pop (sA is still being read).
     corr_warp_tiles<TK>(sA, sC, n, tm, [&](int i, T G) {
-      const T gi = G / R - M;
-      T x;
-      if (mode == 0) {
-        const T mm = dev_fma(beta1, m[i], (T(1) - beta1) * gi);
-        const T vv = dev_fma(beta2, v[i], (T(1) - beta2) * gi * gi);
-        m[i] = mm;
-        v[i] = vv;
-        const T step = lrn * (mm * bc1) / (dev_sqrt(vv * bc2) + T(1e-30));
-        x = sA[i] - step;
-        if (x < T(0)) x = T(0);
-      } else {
-        T e = -lr * (gi / M);
-        if (e > T(4)) e = T(4);
-        if (e < T(-4)) e = T(-4);
-        x = sA[i] * dev_exp(e);
-      }
-      a[i] = x;
+      a[i] = ls_update(sA[i], G, R, M, mode, lr, lrn, beta1, beta2, bc1, bc2, m + i, v + i);
     });
     __syncthreads();
 
@@ -132,6 +146,117 @@ k_local_search(T* pop, T* mom, T* vel, const long long* __restrict__ offsets,
     __syncthreads();
   }
   for (int i = tm.t0; i < n; i += tm.nt) a[i] = sA[i];
+}
+
+// ------------------ local search, one warp per candidate -------------------
+// For small n the CTA kernel's latency is barriers and reductions, and its
+// tiles leave most lanes idle.  Here one warp carries a candidate (no block
+// barriers: warp shuffles and __syncwarp), kWarpCands candidates per CTA.
+// Results are bit for bit those of the CTA kernel: every convolution /
+// correlation output is the same fma chain (whatever the tiling), the
+// elementwise pieces are shared, the maximum is order free, and the two sums
+// (R and S) are formed in the CTA kernel's order -- the partial sums of the
+// team's virtual threads t = 32 w + lane (i = t, t + nt, ...), each virtual
+// warp w reduced by the xor butterfly and read at lane 0, the warps added in
+// order -- with nt the CTA kernel's team size at this n.
+constexpr int kWarpTK = 7;          // outputs per lane of the warp kernel's tiles
+constexpr int kWarpCands = 4;       // candidates (warps) per CTA
+constexpr int kWarpMaxN = 512;      // largest n the warp kernel takes (the CTA kernel is faster beyond)
+
+__host__ __device__ constexpr size_t warp_ls_elems(int n) {
+  return (size_t)(n + 2 * margin<kWarpTK>()) + (size_t)(2 * n - 1 + 2 * margin<kWarpTK>()) + 1;
+}
+
+// sum over virtual thread partials part[w] (w < NWV) in block_sum's order
+template <int NWV>
+__device__ __forceinline__ float team_sum(const float (&part)[NWV]) {
+  float r = 0.f;
+#pragma unroll
+  for (int w = 0; w < NWV; ++w) r += __shfl_sync(0xffffffffu, warp_sum(part[w]), 0);
+  return r;
+}
+
+template <int NWV>
+__global__ void __launch_bounds__(32 * kWarpCands)
+k_local_search_warp(float* pop, float* mom, float* vel, int P, int n, const int* __restrict__ skip,
+                    const int* __restrict__ mode_arr, int iters, float pStart, float pEnd,
+                    float lrStart, float lrEnd, float beta1, float beta2, int mode_default) {
+  constexpr int MG = margin<kWarpTK>();
+  constexpr int NT = 32 * NWV;          // the CTA kernel's team size at this n
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int pid = blockIdx.x * kWarpCands + wl;
+  if (pid >= P) return;
+  if (skip && skip[pid]) return;
+  const int mode = mode_arr ? mode_arr[pid] : mode_default;
+  float* a = pop + (size_t)pid * n;
+  float* m = mom + (size_t)pid * n;
+  float* v = vel + (size_t)pid * n;
+  const int nb = 2 * n - 1;
+  float* base = reinterpret_cast<float*>(smem_raw) + (size_t)wl * warp_ls_elems(n);
+  float* sA = base + MG;
+  float* sC = base + (n + 2 * MG) + MG;
+  for (int i = lane; i < (int)warp_ls_elems(n); i += 32) base[i] = 0.f;
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) { sA[i] = a[i]; m[i] = 0.f; v[i] = 0.f; }
+  __syncwarp();
+
+  const float lnPr = float(log(double(pEnd) / double(pStart)));
+  const float lnLr = float(log(double(lrEnd) / double(lrStart)));
+  float b1t = 1.f, b2t = 1.f;
+  for (int it = 0; it < iters; ++it) {
+    const float frac = iters > 1 ? float(it) / float(iters - 1) : 0.f;
+    const float pexp = pStart * dev_exp(lnPr * frac);
+    const float lr = lrStart * dev_exp(lnLr * frac);
+
+    float mloc = 0.f;
+    conv_tiles<kWarpTK, true>(sA, sA, n, 0, 1, lane, [&](int k, float val) {
+      sC[k] = val;
+      mloc = val > mloc ? val : mloc;
+    });
+    const float M = warp_max(mloc);
+    __syncwarp();
+    if (!(M > 0.f)) break;
+
+    float rpart[NWV];
+#pragma unroll
+    for (int w = 0; w < NWV; ++w) {
+      rpart[w] = 0.f;
+      for (int k = 32 * w + lane; k < nb; k += NT) sC[k] = ls_weight(sC[k], M, pexp, &rpart[w]);
+    }
+    const float R = team_sum(rpart);
+    __syncwarp();
+
+    b1t *= beta1;
+    b2t *= beta2;
+    const float bc1 = 1.f / (1.f - b1t), bc2 = 1.f / (1.f - b2t);
+    const float lrn = lr / float(n);
+    corr_tiles<kWarpTK>(sA, sC, n, 0, 1, lane, [&](int i, float G) {
+      a[i] = ls_update(sA[i], G, R, M, mode, lr, lrn, beta1, beta2, bc1, bc2, m + i, v + i);
+    });
+    __syncwarp();
+
+    float spart[NWV];
+#pragma unroll
+    for (int w = 0; w < NWV; ++w) {
+      spart[w] = 0.f;
+      for (int i = 32 * w + lane; i < n; i += NT) {
+        const float x = a[i];
+        sA[i] = x;
+        spart[w] += x;
+      }
+    }
+    float S = team_sum(spart);
+    __syncwarp();
+    if (!(S > 0.f)) {
+      for (int i = lane; i < n; i += 32) sA[i] = 1.f / float(n);
+      S = 1.f;
+    }
+    const float inv = 1.f / S;
+    for (int i = lane; i < n; i += 32) sA[i] *= inv;
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32) a[i] = sA[i];
 }
 
 // ----------------------------- G_p forward --------------------------------
@@ -406,6 +531,18 @@ int launch_local_search(void* pop, void* mom, void* vel, const long long* offset
                         const int* mode_arr, int iters, double pS, double pE, double lrS,
                         double lrE, double b1, double b2, int mode_default, int dtype,
                         cudaStream_t st) {
+  if (dtype == SIDON_F32 && !offsets && n_max <= kWarpMaxN && P >= 2 * sm_count() &&
+      warps_for<kTK32>(n_max) == 4) {
+    // many small candidates: one warp each (bitwise the CTA kernel's results)
+    const size_t sm = sizeof(float) * warp_ls_elems(n_max) * kWarpCands;
+    const void* fn = (const void*)k_local_search_warp<4>;
+    int rc = prep(fn, sm);
+    if (rc) return rc;
+    k_local_search_warp<4><<<(P + kWarpCands - 1) / kWarpCands, 32 * kWarpCands, sm, st>>>(
+        (float*)pop, (float*)mom, (float*)vel, P, n_max, skip, mode_arr, iters, (float)pS,
+        (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default);
+    return check_launch();
+  }
   if (dtype == SIDON_F32) {
     const size_t sm = smem_local_search(n_max, dtype);
     const void* fn = (const void*)k_local_search<float, kTK32>;
