@@ -2,6 +2,7 @@
 //  search_simt.cu -- CUDA-core kernels of the hot path:
 //    k_local_search   L^p-annealed projected Adam / mirror descent
 //                     (src/kernels.cuh:177-289), fp32 and fp64
+//    k_local_search_warp  the same, fp32, one warp per small candidate
 //    k_lp_forward     G_p(a) = 2n ||a*a||_p / S^2 and the saved {M, S, R}
 //    k_lp_backward    dG_p/da with b recomputed (or read back)
 //    k_eval           certifying fp64 F + active-peak count
