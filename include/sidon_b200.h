@@ -201,6 +201,15 @@ SIDON_API int sidon_refine(const void* src, int n, int P, void* dst, int dtype, 
 /* Pairwise average 2n -> n.  Replaces kCoarsen<T> (src/kernels.cuh:550-557). */
 SIDON_API int sidon_coarsen(const void* src, int n2, int P, void* dst, int dtype, void* stream);
 
+/* Nearest-neighbour resample of every row of src (fp32 [P][m]) to n cells:
+ * dst[p][t] = src[p][min(m-1, floor(t m / n))]; with normalise != 0 each row
+ * is then scaled to sum 1 (fp64 sum in t order, dst = fl(dst / S); rows
+ * summing to 0 stay as they are).  dst (fp32 [P][n]) must not overlap src.
+ * Replaces the arbitrary-ratio host resample of src/main.cu:496-497 and the
+ * injection of main.cu:555-562. */
+SIDON_API int sidon_resample(const float* src, int m, int P, float* dst, int n, int normalise,
+                             void* stream);
+
 /* Island selection + migration on the device: islands are n_islands
  * groups of P/n_islands consecutive slots (at most 1024 per island); each is
  * ranked by fit ascending (ties by slot index, NaN last) into order_out

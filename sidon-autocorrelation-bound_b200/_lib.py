@@ -42,6 +42,7 @@ SIGNATURES = {
     "sidon_frank_wolfe_tc": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _i, _vp]),
     "sidon_refine": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "sidon_coarsen": (_i, [_vp, _i, _i, _vp, _i, _vp]),
+    "sidon_resample": (_i, [_vp, _i, _i, _vp, _i, _i, _vp]),
     "sidon_island_migrate": (_i, [_vp, _i, _vp, _i, _i, _i, _vp, _vp]),
     "sidon_variation": (_i, [_vp, _vp, _i, _i, _i, _vp, _vp, _vp, _vp, C.c_ulonglong,
                              C.c_ulonglong, _vp]),

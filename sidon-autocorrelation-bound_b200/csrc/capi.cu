@@ -66,6 +66,8 @@ int launch_frank_wolfe_big(float* pop, const int* skip, int n, int P, int rounds
                            int nT, float tMax, float tau, float sig, int precision, int Q,
                            void* ws, size_t ws_bytes, cudaStream_t st);
 int launch_coarsen(const void* src, int n2, int P, void* dst, int dtype, cudaStream_t st);
+int launch_resample(const float* src, int m, int P, float* dst, int n, int normalise,
+                    cudaStream_t st);
 int launch_island_migrate(float* pop, int n, double* fit, int P, int NI, int k, int* order,
                           cudaStream_t st);
 int launch_island_migrate_ragged(float* pop, const long long* offsets, double* fit, int P, int NI,
@@ -342,6 +344,20 @@ int sidon_coarsen(const void* src, int n2, int P, void* dst, int dtype, void* st
   if (!src || !dst || src == dst) return SIDON_ERR_ARG;
   if (dtype != SIDON_F32 && dtype != SIDON_F64) return SIDON_ERR_DTYPE;
   return launch_coarsen(src, n2, P, dst, dtype, S(stream));
+}
+
+int sidon_resample(const float* src, int m, int P, float* dst, int n, int normalise,
+                   void* stream) {
+  int rc = pre(m, P);
+  if (rc) return rc;
+  if (n < 1) return SIDON_ERR_N;
+  if (P == 0) return SIDON_OK;
+  if (!src || !dst) return SIDON_ERR_ARG;
+  const char* s0 = (const char*)src;
+  const char* d0 = (const char*)dst;
+  if (d0 < s0 + (size_t)P * m * sizeof(float) && s0 < d0 + (size_t)P * n * sizeof(float))
+    return SIDON_ERR_ARG;                               // the rows must not overlap
+  return launch_resample(src, m, P, dst, n, normalise ? 1 : 0, S(stream));
 }
 
 int sidon_island_migrate(float* pop, int n, double* fit, int P, int n_islands, int k_migrate,

@@ -158,6 +158,33 @@ __global__ void k_island_migrate_ragged(float* __restrict__ pop,
     for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = (float)__ddiv_rn((double)d[t], S);
 }
 
+// Resample every row of a [P][m] batch to n cells by nearest neighbour,
+// dst[t] = src[min(m-1, floor(t m / n))] (the host resample of
+// src/main.cu:496-497 and the injection of main.cu:555-562), optionally
+// normalised to sum 1 as the migration above does (fp64 sum in t order,
+// dst[t] = fl(dst[t] / S)).  One CTA per row.
+__global__ void k_resample(const float* __restrict__ src, int m, float* __restrict__ dst, int n,
+                           int normalise) {
+  __shared__ double sS;
+  const float* s = src + (size_t)blockIdx.x * m;
+  float* d = dst + (size_t)blockIdx.x * n;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const long long q = (long long)t * m / n;
+    d[t] = s[q < m - 1 ? q : m - 1];
+  }
+  if (!normalise) return;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double S = 0.0;
+    for (int t = 0; t < n; ++t) S = __dadd_rn(S, (double)d[t]);
+    sS = S;
+  }
+  __syncthreads();
+  const double S = sS;
+  if (S > 0.0)
+    for (int t = threadIdx.x; t < n; t += blockDim.x) d[t] = (float)__ddiv_rn((double)d[t], S);
+}
+
 // order[r] = candidate of rank r when sorted by size descending, ties by
 // index: the longest-first processing order of a ragged batch.  One thread
 // per candidate counts the candidates ranked before it.
@@ -207,6 +234,12 @@ int launch_coarsen(const void* src, int n2, int P, void* dst, int dtype, cudaStr
     if (((uintptr_t)src & 15) != 0) return SIDON_ERR_ARG;
     k_coarsen_f64<<<grid_for(total, 256), 256, 0, st>>>((const double*)src, (double*)dst, total);
   }
+  return check_launch();
+}
+
+int launch_resample(const float* src, int m, int P, float* dst, int n, int normalise,
+                    cudaStream_t st) {
+  k_resample<<<P, 256, 0, st>>>(src, m, dst, n, normalise);
   return check_launch();
 }
 

@@ -228,6 +228,18 @@ def coarsen(pop: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> 
     return out
 
 
+def resample(pop: torch.Tensor, n: int, normalise: bool = True,
+             out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """Nearest-neighbour resample of every row to n cells, optionally
+    normalised to sum 1 (src/main.cu:496-497, 555-562)."""
+    m, P = _pop_shape(pop)
+    if out is None:
+        out = torch.empty((P, int(n)), dtype=torch.float32, device=pop.device)
+    _lib.call("sidon_resample", _dev(pop, "pop", torch.float32), m, P,
+              _dev(out, "out", torch.float32), int(n), int(bool(normalise)), _stream(stream))
+    return out
+
+
 def lp_forward(a: torch.Tensor, p: float, store_b: bool = False, precision: str = "fp32",
                stream=None):
     """G_p(a) = 2n ||a*a||_p / (sum a)^2 per row.  Returns (value, saved, b|None)."""

@@ -249,6 +249,23 @@ def test_refine_coarsen_exact(cuda, dtype):
     assert torch.equal(K().coarsen(r), x)
 
 
+@pytest.mark.parametrize("m,n", [(64, 128), (1000, 1500), (1500, 1000), (7, 3), (5, 5)])
+def test_resample_matches_oracle(cuda, orc, m, n):
+    """Nearest-neighbour resample + fp64 renormalisation (main.cu:496-497,
+    555-562) = the oracle bit for bit; without normalisation a 2x resample
+    is the cell split."""
+    rng = np.random.default_rng(m + n)
+    pop = rng.uniform(0, 1, (6, m)).astype(np.float32)
+    pop[2] = 0.0                                        # a zero row stays zero
+    got = K().resample(T(pop, cuda), n).cpu().numpy()
+    for p in range(6):
+        want = orc.resample(pop[p], n)
+        assert np.array_equal(got[p], want) or (p == 2 and not got[p].any())
+    if n == 2 * m:
+        raw = K().resample(T(pop, cuda), n, normalise=False)
+        assert torch.equal(raw, K().refine(T(pop, cuda)))
+
+
 def test_island_migrate_matches_oracle(cuda, orc):
     rng = np.random.default_rng(12)
     P, NI, n, k = 64, 8, 333, 2
