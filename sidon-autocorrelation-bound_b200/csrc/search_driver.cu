@@ -242,12 +242,14 @@ int sidon_search(const sidon_search_config* cfg, const double* resume, int n_res
     if (e != cudaSuccess) return set_cuda_error(e);
     rc = sidon_generation_begin_level(B.gen, n, (int)lvl, B.seed_op, nullptr);
     if (rc) return rc;
-    rc = sidon_generation_capture(B.gen, B.pop, cfg->gens_per_graph, &B.graph);
-    if (rc) return rc;
+    if (cfg->gens_per_level == 0 || cfg->gens_per_level >= cfg->gens_per_graph) {
+      rc = sidon_generation_capture(B.gen, B.pop, cfg->gens_per_graph, &B.graph);
+      if (rc) return rc;
+    }
     int gen = 0;
     while (seconds_since(t0) < t_end && (cfg->gens_per_level == 0 || gen < cfg->gens_per_level)) {
       const int left = cfg->gens_per_level ? cfg->gens_per_level - gen : cfg->gens_per_graph;
-      if (left >= cfg->gens_per_graph) {
+      if (left >= cfg->gens_per_graph && B.graph) {
         rc = sidon_graph_launch(B.graph, nullptr);
       } else {
         for (int k = 0; k < left && rc == SIDON_OK; ++k) rc = sidon_generation_step(B.gen, B.pop, nullptr);
@@ -292,7 +294,7 @@ int sidon_search(const sidon_search_config* cfg, const double* resume, int n_res
         cb(&pr, best.data(), (int)best.size(), user);
       }
     }
-    sidon_graph_destroy(B.graph);
+    if (B.graph) sidon_graph_destroy(B.graph);
     B.graph = nullptr;
     // carry the population to the next level (main.cu:786-790)
     prev.assign((size_t)P * n, 0.f);
