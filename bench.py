@@ -276,20 +276,23 @@ def our_arm(args) -> None:
     # end-to-end through the public call with host buffers: every step copies
     # its population in from pinned host memory, runs one step and copies the
     # result out.  Three streams overlap step s's compute with the copy-in of
-    # step s+1 and the copy-out of step s-1 (device buffers double-buffered).
+    # step s+1 and the copy-out of step s-1; three device buffers, so that a
+    # copy-in waits only for the copy-out of step s-3 (with two, the chain
+    # copy-out -> copy-in -> compute of alternate steps bounds the rate).
+    NBUF = 3
     hpin = torch.as_tensor(host).pin_memory()
-    houts = [torch.empty_like(hpin).pin_memory() for _ in range(2)]
-    xs = [torch.empty_like(pop) for _ in range(2)]
+    houts = [torch.empty_like(hpin).pin_memory() for _ in range(NBUF)]
+    xs = [torch.empty_like(pop) for _ in range(NBUF)]
     s_in, s_cp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
 
     def e2e_loop(nsteps, start_ev):
-        ev_cp, ev_out = [None, None], [None, None]
+        ev_cp, ev_out = [None] * NBUF, [None] * NBUF
         for sidx in (s_in, s_cp, s_out):
             sidx.wait_event(start_ev)
         for step in range(nsteps):
-            b = step % 2
+            b = step % NBUF
             if ev_out[b] is not None:
-                s_in.wait_event(ev_out[b])        # x[b] of step-2 fully read back
+                s_in.wait_event(ev_out[b])        # x[b] of step - NBUF fully read back
             with torch.cuda.stream(s_in):
                 xs[b].copy_(hpin, non_blocking=True)
             ev_in = torch.cuda.Event()
