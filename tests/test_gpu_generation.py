@@ -251,3 +251,31 @@ def test_generation_tabu_capacity_reported(cuda, orc):
     assert st["status"] == L().ERR_CAPACITY
     assert st["cells"] <= 9
     assert np.isfinite(pop.cpu().numpy()).all()
+
+
+@pytest.mark.parametrize("P,NI,elite", [(8, 1, 2), (4, 4, 0), (12, 3, 5)])
+def test_generation_edge_islands(cuda, orc, P, NI, elite):
+    """One island (migration onto itself), single-slot islands (migration
+    chained through every island in order) and more elites than slots."""
+    rng = np.random.default_rng(P * 10 + NI)
+    n = 48
+    G, pop, hc = make(cuda, orc, n, P, NI, rng, elite=elite, ls_iters=3, cold_iters=6)
+    for g in range(14):                        # a migration at generation 12
+        G.step(pop)
+        hc.step()
+        check_same(G, pop, hc, f"generation {g}")
+    if elite >= P // NI:
+        assert (hc.pol.plan["op"] == 20).all()
+
+
+def test_search_driver_eager_remainder(cuda, orc):
+    """gens_per_level not a multiple of gens_per_graph: one graph replay, then
+    single eager generations."""
+    gen = K().generation_config(n_islands=2, elite=1, ls_iters=4, cold_iters=6, p_max=200.0,
+                                precision="fp32", fw_rounds=0, tabu_capacity=1 << 10, seed=9)
+    seen = []
+    best, F = K().search(ladder=(40,), P=8, seconds=1e9, gens_per_level=3, gens_per_graph=2,
+                         polish_iters=0, polish_top=0, gen=gen,
+                         progress=lambda d, b: seen.append(d["gen"]))
+    assert seen == [2, 3]
+    assert best.size == 40 and F == orc.host_f(best)
