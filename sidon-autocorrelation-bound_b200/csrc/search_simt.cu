@@ -2,7 +2,6 @@
 //  search_simt.cu -- CUDA-core kernels of the hot path:
 //    k_local_search   L^p-annealed projected Adam / mirror descent
 //                     (src/kernels.cuh:177-289), fp32 and fp64
-//    k_local_search_warp  the same, fp32, one warp per small candidate
 //    k_lp_forward     G_p(a) = 2n ||a*a||_p / S^2 and the saved {M, S, R}
 //    k_lp_backward    dG_p/da with b recomputed (or read back)
 //    k_eval           certifying fp64 F + active-peak count
@@ -149,116 +148,15 @@ k_local_search(T* pop, T* mom, T* vel, const long long* __restrict__ offsets,
   for (int i = tm.t0; i < n; i += tm.nt) a[i] = sA[i];
 }
 
-// ------------------ local search, one warp per candidate -------------------
-// For small n the CTA kernel's latency is barriers and reductions, and its
-// tiles leave most lanes idle.  Here one warp carries a candidate (no block
-// barriers: warp shuffles and __syncwarp), kWarpCands candidates per CTA.
-// Results are bit for bit those of the CTA kernel: every convolution /
-// correlation output is the same fma chain (whatever the tiling), the
-// elementwise pieces are shared, the maximum is order free, and the two sums
-// (R and S) are formed in the CTA kernel's order -- the partial sums of the
-// team's virtual threads t = 32 w + lane (i = t, t + nt, ...), each virtual
-// warp w reduced by the xor butterfly and read at lane 0, the warps added in
-// order -- with nt the CTA kernel's team size at this n.
-constexpr int kWarpTK = 7;          // outputs per lane of the warp kernel's tiles
-constexpr int kWarpCands = 4;       // candidates (warps) per CTA
-constexpr int kWarpMaxN = 512;      // largest n the warp kernel takes (the CTA kernel is faster beyond)
-
-__host__ __device__ constexpr size_t warp_ls_elems(int n) {
-  return (size_t)(n + 2 * margin<kWarpTK>()) + (size_t)(2 * n - 1 + 2 * margin<kWarpTK>()) + 1;
-}
-
-// sum over virtual thread partials part[w] (w < NWV) in block_sum's order
-template <int NWV>
-__device__ __forceinline__ float team_sum(const float (&part)[NWV]) {
-  float r = 0.f;
-#pragma unroll
-  for (int w = 0; w < NWV; ++w) r += __shfl_sync(0xffffffffu, warp_sum(part[w]), 0);
-  return r;
-}
-
-template <int NWV>
-__global__ void __launch_bounds__(32 * kWarpCands)
-k_local_search_warp(float* pop, float* mom, float* vel, int P, int n, const int* __restrict__ skip,
-                    const int* __restrict__ mode_arr, int iters, float pStart, float pEnd,
-                    float lrStart, float lrEnd, float beta1, float beta2, int mode_default) {
-  constexpr int MG = margin<kWarpTK>();
-  constexpr int NT = 32 * NWV;          // the CTA kernel's team size at this n
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-  const int pid = blockIdx.x * kWarpCands + wl;
-  if (pid >= P) return;
-  if (skip && skip[pid]) return;
-  const int mode = mode_arr ? mode_arr[pid] : mode_default;
-  float* a = pop + (size_t)pid * n;
-  float* m = mom + (size_t)pid * n;
-  float* v = vel + (size_t)pid * n;
-  const int nb = 2 * n - 1;
-  float* base = reinterpret_cast<float*>(smem_raw) + (size_t)wl * warp_ls_elems(n);
-  float* sA = base + MG;
-  float* sC = base + (n + 2 * MG) + MG;
-  for (int i = lane; i < (int)warp_ls_elems(n); i += 32) base[i] = 0.f;
-  __syncwarp();
-  for (int i = lane; i < n; i += 32) { sA[i] = a[i]; m[i] = 0.f; v[i] = 0.f; }
-  __syncwarp();
-
-  const float lnPr = float(log(double(pEnd) / double(pStart)));
-  const float lnLr = float(log(double(lrEnd) / double(lrStart)));
-  float b1t = 1.f, b2t = 1.f;
-  for (int it = 0; it < iters; ++it) {
-    const float frac = iters > 1 ? float(it) / float(iters - 1) : 0.f;
-    const float pexp = pStart * dev_exp(lnPr * frac);
-    const float lr = lrStart * dev_exp(lnLr * frac);
-
-    float mloc = 0.f;
-    conv_tiles<kWarpTK, true>(sA, sA, n, 0, 1, lane, [&](int k, float val) {
-      sC[k] = val;
-      mloc = val > mloc ? val : mloc;
-    });
-    const float M = warp_max(mloc);
-    __syncwarp();
-    if (!(M > 0.f)) break;
-
-    float rpart[NWV];
-#pragma unroll
-    for (int w = 0; w < NWV; ++w) {
-      rpart[w] = 0.f;
-      for (int k = 32 * w + lane; k < nb; k += NT) sC[k] = ls_weight(sC[k], M, pexp, &rpart[w]);
-    }
-    const float R = team_sum(rpart);
-    __syncwarp();
-
-    b1t *= beta1;
-    b2t *= beta2;
-    const float bc1 = 1.f / (1.f - b1t), bc2 = 1.f / (1.f - b2t);
-    const float lrn = lr / float(n);
-    corr_tiles<kWarpTK>(sA, sC, n, 0, 1, lane, [&](int i, float G) {
-      a[i] = ls_update(sA[i], G, R, M, mode, lr, lrn, beta1, beta2, bc1, bc2, m + i, v + i);
-    });
-    __syncwarp();
-
-    float spart[NWV];
-#pragma unroll
-    for (int w = 0; w < NWV; ++w) {
-      spart[w] = 0.f;
-      for (int i = 32 * w + lane; i < n; i += NT) {
-        const float x = a[i];
-        sA[i] = x;
-        spart[w] += x;
-      }
-    }
-    float S = team_sum(spart);
-    __syncwarp();
-    if (!(S > 0.f)) {
-      for (int i = lane; i < n; i += 32) sA[i] = 1.f / float(n);
-      S = 1.f;
-    }
-    const float inv = 1.f / S;
-    for (int i = lane; i < n; i += 32) sA[i] *= inv;
-    __syncwarp();
-  }
-  for (int i = lane; i < n; i += 32) a[i] = sA[i];
-}
+// Small candidates: the local search kernel above with kSmallTK-output lane
+// tiles (for n <= kSmallTKMaxN the team is still 4 warps): at n <= 896 the
+// 15-output tiles leave most of the team's warps without a tile (one
+// correlation tile of 480 outputs for n <= 480), 7-output tiles spread the
+// convolution and the correlation over all four.  Results are bit for bit
+// those of the 15-output kernel: every output is the same fma chain whatever
+// the tiling, and the team, its per-thread sums and their order are the same.
+constexpr int kSmallTK = 7;
+constexpr int kSmallTKMaxN = 896;   // largest n with a 4-warp team at kSmallTK (32 * 7 * 4 = 896)
 
 // ----------------------------- G_p forward --------------------------------
 // value = 2n M R^(1/p) / S^2 with M = max b, R = sum (b/M)^p, S = sum a.  M is
@@ -520,8 +418,12 @@ static int prep(const void* fn, size_t smem) { return set_dyn_smem(fn, smem); }
 // capture.
 int prepare_simt(int n_max, bool local_search) {
   int rc = SIDON_OK;
-  if (local_search)
+  if (local_search) {
     rc = prep((const void*)k_local_search<float, kTK32>, smem_local_search(n_max, SIDON_F32));
+    if (!rc && n_max <= kSmallTKMaxN)
+      rc = prep((const void*)k_local_search<float, kSmallTK>,
+                sizeof(float) * ls_smem_elems<float, kSmallTK>(n_max));
+  }
   if (!rc) rc = prep((const void*)k_eval<float, kTK64>, smem_eval(n_max));
   if (!rc) rc = prep((const void*)k_frank_wolfe<kTK32>, smem_fw(n_max));
   return rc;
@@ -532,16 +434,16 @@ int launch_local_search(void* pop, void* mom, void* vel, const long long* offset
                         const int* mode_arr, int iters, double pS, double pE, double lrS,
                         double lrE, double b1, double b2, int mode_default, int dtype,
                         cudaStream_t st) {
-  if (dtype == SIDON_F32 && !offsets && n_max <= kWarpMaxN && P >= 2 * sm_count() &&
-      warps_for<kTK32>(n_max) == 4) {
-    // many small candidates: one warp each (bitwise the CTA kernel's results)
-    const size_t sm = sizeof(float) * warp_ls_elems(n_max) * kWarpCands;
-    const void* fn = (const void*)k_local_search_warp<4>;
+  if (dtype == SIDON_F32 && !offsets && n_max <= kSmallTKMaxN) {
+    // small uniform candidates: kSmallTK-output tiles over the same 4-warp
+    // team (bitwise the kTK32 kernel's results)
+    const size_t sm = sizeof(float) * ls_smem_elems<float, kSmallTK>(n_max);
+    const void* fn = (const void*)k_local_search<float, kSmallTK>;
     int rc = prep(fn, sm);
     if (rc) return rc;
-    k_local_search_warp<4><<<(P + kWarpCands - 1) / kWarpCands, 32 * kWarpCands, sm, st>>>(
-        (float*)pop, (float*)mom, (float*)vel, P, n_max, skip, mode_arr, iters, (float)pS,
-        (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default);
+    k_local_search<float, kSmallTK><<<P, 32 * warps_for<kTK32>(n_max), sm, st>>>(
+        (float*)pop, (float*)mom, (float*)vel, offsets, order, n_fixed, n_max, skip, mode_arr,
+        iters, (float)pS, (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default);
     return check_launch();
   }
   if (dtype == SIDON_F32) {
