@@ -426,6 +426,8 @@ int prepare_simt(int n_max, bool local_search) {
   }
   if (!rc) rc = prep((const void*)k_eval<float, kTK64>, smem_eval(n_max));
   if (!rc) rc = prep((const void*)k_frank_wolfe<kTK32>, smem_fw(n_max));
+  if (!rc && n_max <= kSmallTKMaxN)
+    rc = prep((const void*)k_frank_wolfe<kSmallTK>, sizeof(float) * fw_smem_elems<kSmallTK>(n_max));
   return rc;
 }
 
@@ -505,6 +507,16 @@ int launch_eval(const void* pop, int dtype, const long long* offsets, const int*
 int launch_frank_wolfe(float* pop, const long long* offsets, const int* order, int P, int n_fixed,
                        int n_max, const int* skip, int rounds, int pdhg, int nT, float tMax,
                        float tau, float sig, cudaStream_t st) {
+  if (!offsets && n_max <= kSmallTKMaxN) {
+    // small uniform candidates: kSmallTK-output tiles over the same 4-warp
+    // team (bitwise the kTK32 kernel's results)
+    const size_t sm = sizeof(float) * fw_smem_elems<kSmallTK>(n_max);
+    int rc = prep((const void*)k_frank_wolfe<kSmallTK>, sm);
+    if (rc) return rc;
+    k_frank_wolfe<kSmallTK><<<P, 32 * warps_for<kTK32>(n_max), sm, st>>>(
+        pop, offsets, order, n_fixed, n_max, skip, rounds, pdhg, nT, tMax, tau, sig);
+    return check_launch();
+  }
   const size_t sm = smem_fw(n_max);
   int rc = prep((const void*)k_frank_wolfe<kTK32>, sm);
   if (rc) return rc;

@@ -1,8 +1,9 @@
-"""The fp32 local search of small uniform candidates (n <= 896: the CTA kernel
-with 7-output lane tiles) against the 15-output kernel that a ragged batch of
-the same rows runs: bit-identical heights (every output is the same fma
-chain, the team and its sums are the same), with skip[] and mirror-descent
-candidates; and against the oracle within the fp32 bars.  Needs a B200.
+"""The fp32 local search and Frank-Wolfe step of small uniform candidates
+(n <= 896: the CTA kernels with 7-output lane tiles) against the 15-output
+kernels that a ragged batch of the same rows runs: bit-identical heights
+(every output is the same fma chain, the team and its sums are the same),
+with skip[] and mirror-descent candidates; and against the oracle within the
+fp32 bars.  Needs a B200.
 """
 import numpy as np
 import pytest
@@ -51,3 +52,19 @@ def test_small_tiles_against_the_oracle(cuda, orc):
     for p in range(8):
         Fw = orc.host_f(ref[p].astype(np.float64))
         assert abs(got[p] - Fw) <= 1e-4 * Fw
+
+
+@pytest.mark.parametrize("n,P", [(33, 20), (300, 50), (896, 30)])
+def test_small_tile_frank_wolfe_is_bitwise_the_large_tiles(cuda, n, P):
+    """The fp32 Frank-Wolfe step with 7-output tiles (uniform, n <= 896) = the
+    15-output kernel of a ragged batch of the same rows, bit for bit."""
+    rng = np.random.default_rng(n + 1)
+    pop = rng.uniform(0.2, 1.0, (P, n)).astype(np.float32)
+    pop[:, rng.uniform(size=n) < 0.2] = 0.0
+    skip = torch.tensor((np.arange(P) % 6 == 5).astype(np.int32), device=cuda)
+    x = torch.tensor(pop, device=cuda)
+    assert K().run_frank_wolfe(x, 2, 30, skip=skip)
+    batch = K().RaggedBatch(list(pop), device=cuda)
+    K().run_frank_wolfe_ragged(batch, 2, 30, skip=skip)
+    torch.cuda.synchronize()
+    assert torch.equal(x.view(torch.int32), batch.flat.view(P, n).view(torch.int32))
