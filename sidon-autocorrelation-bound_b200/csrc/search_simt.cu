@@ -148,15 +148,17 @@ k_local_search(T* pop, T* mom, T* vel, const long long* __restrict__ offsets,
   for (int i = tm.t0; i < n; i += tm.nt) a[i] = sA[i];
 }
 
-// Small candidates: the local search kernel above with kSmallTK-output lane
-// tiles (for n <= kSmallTKMaxN the team is still 4 warps): at n <= 896 the
-// 15-output tiles leave most of the team's warps without a tile (one
-// correlation tile of 480 outputs for n <= 480), 7-output tiles spread the
-// convolution and the correlation over all four.  Results are bit for bit
-// those of the 15-output kernel: every output is the same fma chain whatever
-// the tiling, and the team, its per-thread sums and their order are the same.
-constexpr int kSmallTK = 7;
-constexpr int kSmallTKMaxN = 896;   // largest n with a 4-warp team at kSmallTK (32 * 7 * 4 = 896)
+// Small and middle candidates: the local search (and Frank-Wolfe) kernels
+// with narrower lane tiles.  With 15-output tiles a team of 4 warps leaves
+// most of its warps without a tile at small n (one correlation tile of 480
+// outputs for n <= 480); the narrowest odd TK whose 4-warp tiles still span
+// n (128 TK >= n) spreads the convolution and the correlation over all four.
+// Results are bit for bit those of the 15-output kernels: every output is the
+// same fma chain whatever the tiling, and the team (4 warps for n <= 1920),
+// its per-thread sums and their order are the same.
+__host__ __device__ constexpr int tile_for(int n) {
+  return n <= 128 * 7 ? 7 : n <= 128 * 9 ? 9 : n <= 128 * 11 ? 11 : n <= 128 * 13 ? 13 : 15;
+}
 
 // ----------------------------- G_p forward --------------------------------
 // value = 2n M R^(1/p) / S^2 with M = max b, R = sum (b/M)^p, S = sum a.  M is
@@ -413,6 +415,47 @@ size_t smem_fw(int n) { return sizeof(float) * fw_smem_elems<kTK32>(n); }
 
 static int prep(const void* fn, size_t smem) { return set_dyn_smem(fn, smem); }
 
+// uniform fp32 launches with TK-output lane tiles (TK < kTK32, 4-warp team)
+template <int TK>
+static int launch_ls_tiles(void* pop, void* mom, void* vel, int P, int n, const int* skip,
+                           const int* mode_arr, int iters, double pS, double pE, double lrS,
+                           double lrE, double b1, double b2, int mode_default, cudaStream_t st) {
+  const size_t sm = sizeof(float) * ls_smem_elems<float, TK>(n);
+  const int rc = prep((const void*)k_local_search<float, TK>, sm);
+  if (rc) return rc;
+  k_local_search<float, TK><<<P, 32 * warps_for<kTK32>(n), sm, st>>>(
+      (float*)pop, (float*)mom, (float*)vel, nullptr, nullptr, n, n, skip, mode_arr, iters,
+      (float)pS, (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default);
+  return check_launch();
+}
+template <int TK>
+static int launch_fw_tiles(float* pop, int P, int n, const int* skip, int rounds, int pdhg, int nT,
+                           float tMax, float tau, float sig, cudaStream_t st) {
+  const size_t sm = sizeof(float) * fw_smem_elems<TK>(n);
+  const int rc = prep((const void*)k_frank_wolfe<TK>, sm);
+  if (rc) return rc;
+  k_frank_wolfe<TK><<<P, 32 * warps_for<kTK32>(n), sm, st>>>(
+      pop, nullptr, nullptr, n, n, skip, rounds, pdhg, nT, tMax, tau, sig);
+  return check_launch();
+}
+// shared-memory attributes of the narrow-tile kernel at n (ahead of a capture)
+static int prep_tiles(int n, bool local_search) {
+  const int tk = tile_for(n);
+  if (tk >= kTK32) return SIDON_OK;
+#define SIDON_PREP_TILES(TK)                                                                 \
+  return local_search                                                                        \
+             ? prep((const void*)k_local_search<float, TK>,                                  \
+                    sizeof(float) * ls_smem_elems<float, TK>(n))                             \
+             : prep((const void*)k_frank_wolfe<TK>, sizeof(float) * fw_smem_elems<TK>(n))
+  switch (tk) {
+    case 7: SIDON_PREP_TILES(7);
+    case 9: SIDON_PREP_TILES(9);
+    case 11: SIDON_PREP_TILES(11);
+    default: SIDON_PREP_TILES(13);
+  }
+#undef SIDON_PREP_TILES
+}
+
 // The shared-memory attributes of the fp32 local search, the fp32-input
 // evaluation and the Frank-Wolfe kernels at n_max, set ahead of a stream
 // capture.
@@ -420,14 +463,11 @@ int prepare_simt(int n_max, bool local_search) {
   int rc = SIDON_OK;
   if (local_search) {
     rc = prep((const void*)k_local_search<float, kTK32>, smem_local_search(n_max, SIDON_F32));
-    if (!rc && n_max <= kSmallTKMaxN)
-      rc = prep((const void*)k_local_search<float, kSmallTK>,
-                sizeof(float) * ls_smem_elems<float, kSmallTK>(n_max));
+    if (!rc) rc = prep_tiles(n_max, true);
   }
   if (!rc) rc = prep((const void*)k_eval<float, kTK64>, smem_eval(n_max));
   if (!rc) rc = prep((const void*)k_frank_wolfe<kTK32>, smem_fw(n_max));
-  if (!rc && n_max <= kSmallTKMaxN)
-    rc = prep((const void*)k_frank_wolfe<kSmallTK>, sizeof(float) * fw_smem_elems<kSmallTK>(n_max));
+  if (!rc) rc = prep_tiles(n_max, false);
   return rc;
 }
 
@@ -436,17 +476,19 @@ int launch_local_search(void* pop, void* mom, void* vel, const long long* offset
                         const int* mode_arr, int iters, double pS, double pE, double lrS,
                         double lrE, double b1, double b2, int mode_default, int dtype,
                         cudaStream_t st) {
-  if (dtype == SIDON_F32 && !offsets && n_max <= kSmallTKMaxN) {
-    // small uniform candidates: kSmallTK-output tiles over the same 4-warp
-    // team (bitwise the kTK32 kernel's results)
-    const size_t sm = sizeof(float) * ls_smem_elems<float, kSmallTK>(n_max);
-    const void* fn = (const void*)k_local_search<float, kSmallTK>;
-    int rc = prep(fn, sm);
-    if (rc) return rc;
-    k_local_search<float, kSmallTK><<<P, 32 * warps_for<kTK32>(n_max), sm, st>>>(
-        (float*)pop, (float*)mom, (float*)vel, offsets, order, n_fixed, n_max, skip, mode_arr,
-        iters, (float)pS, (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default);
-    return check_launch();
+  if (dtype == SIDON_F32 && !offsets && tile_for(n_max) < kTK32) {
+    // uniform candidates of n <= 1664: narrower lane tiles over the same
+    // 4-warp team (bitwise the kTK32 kernel's results)
+    switch (tile_for(n_max)) {
+      case 7: return launch_ls_tiles<7>(pop, mom, vel, P, n_max, skip, mode_arr, iters, pS, pE,
+                                        lrS, lrE, b1, b2, mode_default, st);
+      case 9: return launch_ls_tiles<9>(pop, mom, vel, P, n_max, skip, mode_arr, iters, pS, pE,
+                                        lrS, lrE, b1, b2, mode_default, st);
+      case 11: return launch_ls_tiles<11>(pop, mom, vel, P, n_max, skip, mode_arr, iters, pS, pE,
+                                          lrS, lrE, b1, b2, mode_default, st);
+      default: return launch_ls_tiles<13>(pop, mom, vel, P, n_max, skip, mode_arr, iters, pS, pE,
+                                          lrS, lrE, b1, b2, mode_default, st);
+    }
   }
   if (dtype == SIDON_F32) {
     const size_t sm = smem_local_search(n_max, dtype);
@@ -507,15 +549,15 @@ int launch_eval(const void* pop, int dtype, const long long* offsets, const int*
 int launch_frank_wolfe(float* pop, const long long* offsets, const int* order, int P, int n_fixed,
                        int n_max, const int* skip, int rounds, int pdhg, int nT, float tMax,
                        float tau, float sig, cudaStream_t st) {
-  if (!offsets && n_max <= kSmallTKMaxN) {
-    // small uniform candidates: kSmallTK-output tiles over the same 4-warp
-    // team (bitwise the kTK32 kernel's results)
-    const size_t sm = sizeof(float) * fw_smem_elems<kSmallTK>(n_max);
-    int rc = prep((const void*)k_frank_wolfe<kSmallTK>, sm);
-    if (rc) return rc;
-    k_frank_wolfe<kSmallTK><<<P, 32 * warps_for<kTK32>(n_max), sm, st>>>(
-        pop, offsets, order, n_fixed, n_max, skip, rounds, pdhg, nT, tMax, tau, sig);
-    return check_launch();
+  if (!offsets && tile_for(n_max) < kTK32) {
+    // uniform candidates of n <= 1664: narrower lane tiles over the same
+    // 4-warp team (bitwise the kTK32 kernel's results)
+    switch (tile_for(n_max)) {
+      case 7: return launch_fw_tiles<7>(pop, P, n_max, skip, rounds, pdhg, nT, tMax, tau, sig, st);
+      case 9: return launch_fw_tiles<9>(pop, P, n_max, skip, rounds, pdhg, nT, tMax, tau, sig, st);
+      case 11: return launch_fw_tiles<11>(pop, P, n_max, skip, rounds, pdhg, nT, tMax, tau, sig, st);
+      default: return launch_fw_tiles<13>(pop, P, n_max, skip, rounds, pdhg, nT, tMax, tau, sig, st);
+    }
   }
   const size_t sm = smem_fw(n_max);
   int rc = prep((const void*)k_frank_wolfe<kTK32>, sm);

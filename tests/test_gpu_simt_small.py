@@ -1,6 +1,7 @@
-"""The fp32 local search and Frank-Wolfe step of small uniform candidates
-(n <= 896: the CTA kernels with 7-output lane tiles) against the 15-output
-kernels that a ragged batch of the same rows runs: bit-identical heights
+"""The fp32 local search and Frank-Wolfe step of small and middle uniform
+candidates (n <= 1664: the CTA kernels with 7-, 9-, 11- or 13-output lane
+tiles) against the 15-output kernels that a ragged batch of the same rows
+runs: bit-identical heights
 (every output is the same fma chain, the team and its sums are the same),
 with skip[] and mirror-descent candidates; and against the oracle within the
 fp32 bars.  Needs a B200.
@@ -17,7 +18,8 @@ def K():
     return kernels
 
 
-@pytest.mark.parametrize("n,P", [(1, 9), (33, 40), (128, 512), (300, 77), (512, 400), (896, 160)])
+@pytest.mark.parametrize("n,P", [(1, 9), (33, 40), (128, 512), (300, 77), (512, 400), (896, 160),
+                                 (1000, 60), (1300, 40), (1600, 40), (1700, 20)])
 def test_small_tiles_are_bitwise_the_large_tiles(cuda, n, P):
     rng = np.random.default_rng(n)
     pop = rng.uniform(0.2, 1.0, (P, n)).astype(np.float32)
@@ -54,9 +56,9 @@ def test_small_tiles_against_the_oracle(cuda, orc):
         assert abs(got[p] - Fw) <= 1e-4 * Fw
 
 
-@pytest.mark.parametrize("n,P", [(33, 20), (300, 50), (896, 30)])
+@pytest.mark.parametrize("n,P", [(33, 20), (300, 50), (896, 30), (1100, 20), (1500, 16)])
 def test_small_tile_frank_wolfe_is_bitwise_the_large_tiles(cuda, n, P):
-    """The fp32 Frank-Wolfe step with 7-output tiles (uniform, n <= 896) = the
+    """The fp32 Frank-Wolfe step with narrow tiles (uniform, n <= 1664) = the
     15-output kernel of a ragged batch of the same rows, bit for bit."""
     rng = np.random.default_rng(n + 1)
     pop = rng.uniform(0.2, 1.0, (P, n)).astype(np.float32)
