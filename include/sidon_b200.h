@@ -528,7 +528,10 @@ SIDON_API int sidon_generation_destroy(sidon_generation h);
 SIDON_API int sidon_generation_views_of(sidon_generation h, sidon_generation_views* out);
 /* Starts a ladder level of n cells: generation 0, no level best, seed_op
  * (device [P], or NULL for all 9) as the operator of each slot, mirror
- * descent on islands 3, 7, 11, ... (main.cu:566-585). */
+ * descent on islands 3, 7, 11, ... (main.cu:566-585).  n must fit the
+ * one-CTA local search of the configured precision (SIDON_ERR_N /
+ * SIDON_ERR_SMEM otherwise: up to 9728 cells on the tensor cores; the
+ * reference driver refuses n > 16384, main.cu:391-399). */
 SIDON_API int sidon_generation_begin_level(sidon_generation h, int n, int level,
                                            const int* seed_op, void* stream);
 /* Adopts row (device fp32 [n]) with F as the incumbent (the resumed vector
