@@ -27,6 +27,33 @@ def test_header_declares_the_boundary():
         assert must in names
 
 
+def test_header_is_plain_c_and_cxx(tmp_path):
+    """A C caller (cgo, ctypes stubs, a plain C driver) and a C++ caller can
+    both include the header: it compiles as C99 and as C++17, and a C file
+    can call an entry point and lay out the structs."""
+    import shutil
+    inc = str(ROOT / "include")
+    src = tmp_path / "use.c"
+    src.write_text(
+        "#include <sidon_b200.h>\n"
+        "int main(void) {\n"
+        "  sidon_generation_config g = {8, 2, 4000, 20000, 20000.f, SIDON_PREC_BF16X3, 6, 500,\n"
+        "                               12, 0.30f, SIDON_PREC_FP32_SIMT, 6, 1 << 16, 1ull};\n"
+        "  sidon_generation_state st; sidon_anneal_config a; sidon_search_config sc;\n"
+        "  (void)st; (void)a; (void)sc;\n"
+        "  double h[4] = {1, 2, 2, 1};\n"
+        "  return (int)(sidon_hostF(h, 4) > 0) + g.n_islands * 0;\n"
+        "}\n")
+    for cc, std in (("gcc", "-std=c99"), ("g++", "-std=c++17")):
+        exe = shutil.which(cc)
+        if exe is None:
+            continue
+        flags = [std] + (["-x", "c++"] if cc == "g++" else [])
+        r = subprocess.run([exe, *flags, "-Wall", "-Werror", "-fsyntax-only", "-I", inc, str(src)],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+
+
 def test_library_exports_every_declared_symbol(lib):
     import sidon_b200._lib as L
     so = pathlib.Path(L.LIB_PATH)
