@@ -191,12 +191,16 @@ def test_generation_tabu_and_stagnation_paths(cuda, orc):
     assert (ops == 9).any()
 
 
-def test_generation_graph_equals_eager(cuda, orc):
+@pytest.mark.parametrize("prec,n,P", [("bf16x3", 80, 32), ("fp32", 1000, 320)])
+def test_generation_graph_equals_eager(cuda, orc, prec, n, P):
+    """A captured graph of generations equals the eager ones bit for bit, on
+    the tensor cores and on the fp32 path (narrow-tile kernels, P over two
+    waves)."""
     rng = np.random.default_rng(11)
-    n, P, NI, gens = 80, 32, 4, 7
+    NI, gens = 4, 7
     cfg = K().generation_config(n_islands=NI, elite=2, ls_iters=6, cold_iters=9, p_max=300.0,
-                                precision="bf16x3", fw_rounds=1, fw_iters=8, fw_nT=4,
-                                fw_t_max=0.3, fw_precision="bf16x3", tabu_capacity=1 << 10,
+                                precision=prec, fw_rounds=1, fw_iters=8, fw_nT=4,
+                                fw_t_max=0.3, fw_precision=prec, tabu_capacity=1 << 10,
                                 seed=SEED)
     pop0 = seeds(n, P, rng)
     so = torch.tensor(seed_ops(P, rng), device=cuda)
