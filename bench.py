@@ -743,6 +743,85 @@ def reference_memetic_arm(args) -> None:
     }))
 
 
+def reference_islands_arm(args) -> None:
+    """The batched uneven islands with the reference's own kernels
+    (kLocalSearch<float>, kFrankWolfe<float>, kEval<float,double>, built for
+    sm_100a from its sources into oracle/_ref).  The reference launches one
+    size at a time, so the candidates run as one launch per size, one after
+    another; one 250-step segment, one Frank-Wolfe step (200 iterations) and
+    one evaluation per size are timed with CUDA events and the 5000-step
+    anneal is composed from them (20 segments and Frank-Wolfe steps, 10
+    evaluations for the migrations)."""
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref not built (reference sources absent here)"}))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from sidon_b200 import synth
+    ref = oracle.ref_main()
+    P, steps, seg, pdhg = args.islands_P, args.anneal_steps, args.fw_every, args.pdhg_iters
+    sizes = synth.uneven_sizes(P, seed=3, levels=ISLAND_LEVELS)
+    rows = synth.ragged_population(sizes, seed=3)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        rc = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        assert rc >= 0, rc
+        return a.elapsed_time(b)
+
+    pA = 2.0
+    pB = 2.0 * (1024.0 / 2.0) ** ((seg - 1) / (steps - 1))
+    per_size = {}
+    for n in ISLAND_LEVELS:
+        idx = np.nonzero(sizes == n)[0]
+        if idx.size == 0:
+            continue
+        x = torch.tensor(np.stack([rows[i] for i in idx]).astype(np.float32), device=dev)
+        Pg = x.shape[0]
+        mom, vel = torch.empty_like(x), torch.empty_like(x)
+        F = torch.empty(Pg, dtype=torch.float64, device=dev)
+        nact = torch.empty(Pg, dtype=torch.int32, device=dev)
+        ref.ref_gpu_local_search(x.data_ptr(), mom.data_ptr(), vel.data_ptr(), n, Pg, 2, pA, pA,
+                                 1e-3, 1e-3, None)
+        ls = timed(lambda: ref.ref_gpu_local_search(x.data_ptr(), mom.data_ptr(), vel.data_ptr(),
+                                                    n, Pg, seg, pA, pB, 1e-3, 1e-3, None))
+        fw = timed(lambda: ref.ref_gpu_frank_wolfe(x.data_ptr(), n, Pg, 1, pdhg, 12, 0.30, None))
+        ev = timed(lambda: ref.ref_gpu_eval(x.data_ptr(), n, Pg, F.data_ptr(), nact.data_ptr(),
+                                            1e-4, None))
+        per_size[int(n)] = {"candidates": int(Pg), "segment_ms": ls, "frank_wolfe_ms": fw,
+                            "eval_ms": ev}
+    n_seg = steps // seg
+    seg_ms = sum(v["segment_ms"] for v in per_size.values())
+    fw_ms = sum(v["frank_wolfe_ms"] for v in per_size.values())
+    ev_ms = sum(v["eval_ms"] for v in per_size.values())
+    total_s = (n_seg * (seg_ms + fw_ms) + (steps // 500) * ev_ms) / 1e3
+    print(json.dumps({
+        "impl": "reference", "metric": "island_anneal_candidate_steps_per_s",
+        "value": P * steps / total_s, "unit": "candidate-steps/s", "n_gpus": 1,
+        "higher_is_better": True, "data": "synthetic", "anneal_seconds": total_s,
+        "config": {"workload": f"batched uneven islands: P={P}, n uniform over "
+                               f"{list(ISLAND_LEVELS)}, {steps} steps, FW every {seg} "
+                               f"({pdhg} PDHG), reference kernels one launch per size",
+                   "composition": f"{n_seg} x (one {seg}-step segment + one Frank-Wolfe step) "
+                                  f"+ {steps // 500} evaluations, each timed once per size"},
+        "phase_ms": {"local_search_segment": seg_ms, "frank_wolfe_step": fw_ms,
+                     "evaluation": ev_ms},
+        "per_size": per_size,
+    }))
+
+
 # --------------------------------- large ladder -----------------------------
 LADDER = (8192, 16384, 32768, 65536)
 
@@ -907,6 +986,8 @@ def main() -> None:
             reference_memetic_arm(args)
         elif args.workload == "micro":
             reference_micro_arm(args)
+        elif args.workload == "islands":
+            reference_islands_arm(args)
         else:
             reference_arm(args)
     elif args.workload == "islands":

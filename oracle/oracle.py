@@ -127,6 +127,8 @@ def ref_main() -> C.CDLL:
         L.ref_gpu_local_search.argtypes = [_vp, _vp, _vp, _i, _i, _i, _f, _f, _f, _f, _vp]
         L.ref_gpu_eval.restype = _i
         L.ref_gpu_eval.argtypes = [_vp, _i, _i, _vp, _vp, _d, _vp]
+        L.ref_gpu_frank_wolfe.restype = _i
+        L.ref_gpu_frank_wolfe.argtypes = [_vp, _i, _i, _i, _i, _i, _f, _vp]
         L.ref_gpu_generation_search.restype = _i
         L.ref_gpu_generation_search.argtypes = [_vp] * 6 + [_i] * 4 + [_f, _i, _i] + [_vp] * 8
         L.ref_gpu_generation_vary.restype = _i

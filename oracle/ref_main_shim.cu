@@ -49,6 +49,25 @@ int ref_gpu_eval(const float* pop, int n, int P, double* fit, int* nact, double 
   return (int)cudaGetLastError();
 }
 
+// src/kernels.cuh:408 kFrankWolfe<float> on device rows, launched as
+// runFrankWolfe does (src/main.cu:170-178).  Returns 1 when it ran, 0 when
+// the candidate does not fit shared memory (the driver then skips the step),
+// -cudaError on failure.
+int ref_gpu_frank_wolfe(float* pop, int n, int P, int rounds, int pdhg, int nT, float tMax,
+                        void* stream) {
+  const size_t sm = fwSmem<float>(n);
+  int optin = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if ((int)sm > optin) return 0;
+  cudaError_t e = cudaFuncSetAttribute((const void*)kFrankWolfe<float>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return -(int)e;
+  kFrankWolfe<float><<<P, BD, sm, (cudaStream_t)stream>>>(pop, nullptr, n, rounds, pdhg, nT, tMax);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 1 : -(int)e;
+}
+
 // The numeric device steps of one generation of the reference driver
 // (src/main.cu:606-651), launched through its own helpers on a Gpu view of
 // the caller's buffers: the non-empty anneal tiers in order (skip masks
