@@ -822,6 +822,76 @@ def reference_islands_arm(args) -> None:
     }))
 
 
+def reference_ladder_arm(args) -> None:
+    """The large ladder's levels with the reference's own kernels
+    (kLocalSearch<float>, kFrankWolfe<float>, built for sm_100a from its
+    sources): per level the Adam segment and one Frank-Wolfe round on the
+    same B candidates, timed with CUDA events, where the reference's kernels
+    fit one CTA's shared memory; the others are reported as not runnable
+    (its driver refuses n > 16384, src/main.cu:391-399)."""
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref not built (reference sources absent here)"}))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from sidon_b200 import synth
+    ref = oracle.ref_main()
+    B, steps, pdhg = args.ladder_B, args.ladder_steps, args.ladder_pdhg
+    ladder = [int(x) for x in args.ladder_levels.split(",")]
+    optin = torch.cuda.get_device_properties(dev).shared_memory_per_block_optin
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        rc = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return rc, a.elapsed_time(b)
+
+    levels = []
+    for n in ladder:
+        x = torch.as_tensor(synth.population("structured", n, B, seed=4), device=dev)
+        mom, vel = torch.empty_like(x), torch.empty_like(x)
+        row = {"n": n}
+        if 4 * (3 * n + 8 + 8 + 64) > optin:      # localSearchSmem<float> (kernels.cuh:161-162)
+            row["adam"] = "not runnable: the reference's local search does not fit shared memory"
+        else:
+            ref.ref_gpu_local_search(x.data_ptr(), mom.data_ptr(), vel.data_ptr(), n, B, 2, 4.0,
+                                     4.0, 1e-3, 1e-3, None)
+            rc, ms = timed(lambda: ref.ref_gpu_local_search(x.data_ptr(), mom.data_ptr(),
+                                                            vel.data_ptr(), n, B, steps, 4.0,
+                                                            64.0, 1e-3, 1e-3, None))
+            assert rc == 0, rc
+            row["adam_steps_per_s"] = steps / (ms / 1e3)
+            row["adam_tflops_algorithmic"] = 4.0 * n * n * B * steps / (ms / 1e3) / 1e12
+        rc, ms = timed(lambda: ref.ref_gpu_frank_wolfe(x.data_ptr(), n, B, 1, pdhg, 12, 0.30, None))
+        assert rc >= 0, rc
+        if rc == 1:
+            row["fw_round_ms"] = ms
+        else:
+            row["fw"] = "not runnable: kFrankWolfe does not fit shared memory (main.cu:173)"
+        if n > 16384:
+            row["driver"] = "refused by the reference driver (n > 16384, main.cu:391-399)"
+        levels.append(row)
+    print(json.dumps({
+        "impl": "reference", "metric": "ladder_adam_steps_per_s_at_65536",
+        "value": levels[-1].get("adam_steps_per_s"), "unit": "batched steps/s",
+        "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+        "config": {"workload": f"large ladder B={B}: {ladder}, {steps} Adam steps + 1 FW round "
+                               f"({pdhg} PDHG) per level, reference kernels"},
+        "levels": levels,
+    }))
+
+
 # --------------------------------- large ladder -----------------------------
 LADDER = (8192, 16384, 32768, 65536)
 
@@ -988,6 +1058,8 @@ def main() -> None:
             reference_micro_arm(args)
         elif args.workload == "islands":
             reference_islands_arm(args)
+        elif args.workload == "ladder":
+            reference_ladder_arm(args)
         else:
             reference_arm(args)
     elif args.workload == "islands":
