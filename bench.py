@@ -23,6 +23,9 @@ seed 8400 + rank), normalised to sum 1.
 path, the fp64 L^p-Adam twin of tools/probe.cpp (localSearch, OpenMP over
 candidates as in probe.cpp:239) compiled from the reference sources into
 oracle/_ref, on all host cores, on a bounded sample of the same workload.
+With ``--workload islands|ladder|memetic|micro`` it times the reference's own
+GPU kernels (built for sm_100a from its sources into oracle/_ref, launched
+through its own helpers) on the same workload instead.
 """
 from __future__ import annotations
 
