@@ -2,7 +2,7 @@
 adjoint correlation + update) at n = 8400 cells, B = 256 candidates per GPU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|bf16x1|fp32]
-                    [--impl ours|reference] [--workload lp_adam|islands|ladder|memetic|micro]
+                    [--impl ours|reference] [--workload lp_adam|islands|ladder|memetic|micro|search]
 
 One *step* = every candidate of the batch advances one Adam step.  The timed
 region is ONE launch of the fused local-search kernel running K steps (the
@@ -25,7 +25,8 @@ candidates as in probe.cpp:239) compiled from the reference sources into
 oracle/_ref, on all host cores, on a bounded sample of the same workload.
 With ``--workload islands|ladder|memetic|micro`` it times the reference's own
 GPU kernels (built for sm_100a from its sources into oracle/_ref, launched
-through its own helpers) on the same workload instead.
+through its own helpers) on the same workload instead, and with ``search``
+its unmodified search driver under the same wall-clock budget.
 """
 from __future__ import annotations
 
@@ -895,6 +896,100 @@ def reference_ladder_arm(args) -> None:
     }))
 
 
+# --------------------------------- whole search ------------------------------
+SEARCH_LADDER = (64, 128, 256, 512, 1024, 2048)     # the reference driver's default ladder
+
+
+def search_arm(args) -> None:
+    """The whole search at the reference driver's defaults (src/main.cu:41-58:
+    ladder 64 ... 2048, 256 candidates in 8 islands, 2 elites, warm / cold
+    4000 / 20000 steps, p up to 20000, 6 Frank-Wolfe rounds of 500 iterations,
+    40000-step fp64 polish of 8 starts) for --search-seconds of wall clock,
+    through sidon_search (BF16x3 local search, fp32 Frank-Wolfe as the
+    reference).  Prints the certified F reached (lower is better)."""
+    import torch
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    import sidon_b200
+    sidon_b200.load(build=not (ROOT / "sidon-autocorrelation-bound_b200" / "libsidon_b200.so").exists())
+    from sidon_b200 import kernels
+    gens = []
+    t0 = time.perf_counter()
+    best, F = kernels.search(ladder=SEARCH_LADDER, P=256, seconds=args.search_seconds,
+                             gens_per_graph=2, polish_iters=40000, polish_top=8,
+                             gen=kernels.generation_config(precision=args.precision,
+                                                           fw_precision="fp32",
+                                                           seed=20260905),
+                             progress=lambda d, b: gens.append((d["n"], d["gen"])))
+    wall = time.perf_counter() - t0
+    if args.search_out:
+        from sidon_b200 import formats
+        formats.write_certificate(args.search_out, best, F, "sidon_b200 sidon_search")
+    per_level = {}
+    for n, g in gens:
+        per_level[n] = max(per_level.get(n, 0), g)
+    print(json.dumps({
+        "metric": "search_F_at_budget", "value": F, "unit": "F (certified, hostF)",
+        "higher_is_better": False, "n_gpus": 1, "data": "synthetic seeds",
+        "seconds": wall, "n": int(best.size), "generations_per_level": per_level,
+        "config": {"workload": f"whole search, reference defaults, {args.search_seconds:.0f} s "
+                               f"budget, ladder {list(SEARCH_LADDER)}",
+                   "precision": args.precision, "fw_precision": "fp32"},
+    }))
+
+
+def reference_search_arm(args) -> None:
+    """The reference's own search driver, unmodified (src/main.cu built for
+    sm_100a into oracle/_ref/sidon_ref), with its defaults and the same
+    wall-clock budget; its result file gives the F it reports."""
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    exe = ROOT / "oracle" / "_ref" / "sidon_ref"
+    if not exe.exists():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/sidon_ref not built (reference sources absent here)"}))
+        return
+    import tempfile
+    from sidon_b200 import formats
+    with tempfile.TemporaryDirectory() as td:
+        out = pathlib.Path(td) / "best"
+        t0 = time.perf_counter()
+        r = subprocess.run([str(exe), "--seconds", str(args.search_seconds), "--out", str(out),
+                            "--quiet"], capture_output=True, text=True,
+                           env={**os.environ, "CUDA_VISIBLE_DEVICES": str(local)})
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": f"reference driver exited {r.returncode}"}))
+            return
+        text = (pathlib.Path(str(out) + ".txt")).read_text()
+        a = formats.load_vec(str(out) + ".txt")
+    F = None
+    for ln in text.splitlines():
+        if ln.startswith("F "):
+            F = float(ln.split()[1])
+    levels = {}
+    for ln in r.stdout.splitlines():
+        if ln.startswith("=== level n=") and "done" in ln:
+            parts = ln.split()
+            levels[int(parts[2].split("=")[1].rstrip(":"))] = int(parts[parts.index("after") + 1])
+    import sidon_b200
+    hostF = sidon_b200.load().sidon_hostF(np.ascontiguousarray(a).ctypes.data, int(a.size))
+    print(json.dumps({
+        "impl": "reference", "metric": "search_F_at_budget", "value": F,
+        "unit": "F (its own report)", "hostF_of_its_vector": hostF,
+        "higher_is_better": False, "n_gpus": 1,
+        "data": "synthetic seeds", "seconds": wall, "n": int(a.size),
+        "generations_per_level": levels,
+        "config": {"workload": f"whole search, reference defaults, {args.search_seconds:.0f} s "
+                               f"budget, ladder {list(SEARCH_LADDER)}",
+                   "program": "the unmodified reference driver (src/main.cu), sm_100a build"},
+    }))
+
+
 # --------------------------------- large ladder -----------------------------
 LADDER = (8192, 16384, 32768, 65536)
 
@@ -1037,7 +1132,9 @@ def main() -> None:
     ap.add_argument("--precision", default=os.environ.get("SIDON_BENCH_PRECISION", "bf16x3"),
                     choices=["fp32", "bf16x3", "bf16x1"])
     ap.add_argument("--workload", default="lp_adam",
-                    choices=["lp_adam", "islands", "ladder", "memetic", "micro"])
+                    choices=["lp_adam", "islands", "ladder", "memetic", "micro", "search"])
+    ap.add_argument("--search-seconds", type=float, default=60.0)
+    ap.add_argument("--search-out", default="", help="write the certificate (JSON) here")
     ap.add_argument("--memetic-n", type=int, default=2048)
     ap.add_argument("--ladder-B", type=int, default=32)
     ap.add_argument("--ladder-steps", type=int, default=200)
@@ -1063,6 +1160,8 @@ def main() -> None:
             reference_islands_arm(args)
         elif args.workload == "ladder":
             reference_ladder_arm(args)
+        elif args.workload == "search":
+            reference_search_arm(args)
         else:
             reference_arm(args)
     elif args.workload == "islands":
@@ -1073,6 +1172,8 @@ def main() -> None:
         memetic_arm(args)
     elif args.workload == "micro":
         micro_arm(args)
+    elif args.workload == "search":
+        search_arm(args)
     else:
         our_arm(args)
 
