@@ -4,7 +4,8 @@
 //  reset.  One CTA = 8 warps = one tile pipeline (tc_engine.cuh).
 //
 //  Shared memory (see Layout):
-//    stages  STAGES x 6 KB   Hankel windows (hi | lo planes)
+//    stages  3 x 1, 2 x 2 or 2 x 3 windows of 6 KB (hi | lo planes):
+//            stages x windows per stage, from ring_for
 //    bc      the tile phase's B-matrix copy (hi, or hi | lo); after a
 //            tile phase, gather scratch for up to 2n-1 outputs
 //    sa      fp32 heights, padded block layout (cell i at i + 4 floor(i/64)),
@@ -18,9 +19,34 @@
 namespace sidon {
 namespace tc {
 
+// Shared memory a multi-window ring may grow the plan to: the sm_100
+// per-block opt-in limit (227 KB) less 2 KB for the kernels' static shared
+// variables.  (The three single-window stages are taken at any size.)
+constexpr size_t kSmemBudget = 232448 - 2048;
+// Tile sequences of at least this many blocks take the multi-window stages.
+// Measured per step, identical results: n = 8400 (132 blocks) 13% faster
+// with 2 x 2 windows than with 3 x 1, n = 2048 (32 blocks) 10% faster, n = 512
+// (8 blocks: 5 tiles) 4% slower.
+constexpr int kRingMinBlocks = 16;
+
+struct Ring {
+  int stages, per_stage;
+};
+// The window ring for m blocks when everything else takes `other` bytes:
+// two stages of three windows, else of two, when the sequence is long and
+// they fit the budget; else three single-window stages.
+__host__ __device__ __forceinline__ Ring ring_for(int m, size_t other) {
+  if (m >= kRingMinBlocks) {
+    if (other + 6 * (size_t)WIN_BYTES <= kSmemBudget) return Ring{2, 3};
+    if (other + 4 * (size_t)WIN_BYTES <= kSmemBudget) return Ring{2, 2};
+  }
+  return Ring{3, 1};
+}
+
 // dynamic shared memory plan (byte offsets from a 1 KB aligned base)
 struct Layout {
   int m, rc, rcc, sa_len, cb_len;
+  Ring ring;
   size_t off_bc, off_sa, off_cb, off_red, total;
   __host__ __device__ Layout(int n) {
     m = (n + BL - 1) / BL;
@@ -28,7 +54,11 @@ struct Layout {
     rcc = corr_copy_rows(m);
     sa_len = 68 * (m + 8);                 // padded heights, 136 cells of margin in front
     cb_len = 68 * (2 * m + 2);             // padded weights / gather scratch
-    size_t o = (size_t)STAGES * STAGE_BYTES;
+    ring = ring_for(m, place(0));          // the ring takes whole KB: the rest keeps its padding
+    place((size_t)ring.stages * ring.per_stage * WIN_BYTES);
+  }
+  // lay out everything after a ring of `o` bytes; returns the total
+  __host__ __device__ size_t place(size_t o) {
     off_bc = o;
     const int rows = rcc > rc ? rcc : rc;
     // one B copy (hi, or hi|lo) of up to max(rc, rcc) rows; after a tile
@@ -43,8 +73,9 @@ struct Layout {
     o += (size_t)cb_len * 4;
     o = (o + 15) & ~(size_t)15;
     off_red = o;
-    o += 64 * 4 + (2 * STAGES + 5) * 8 + 16;
+    o += 64 * 4 + (2 * MAX_STAGES + 5) * 8 + 16;
     total = o + 1024;                      // slack for aligning the dynamic base to 1 KB
+    return total;
   }
 };
 
@@ -68,11 +99,11 @@ __device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* ra
   S.red = reinterpret_cast<float*>(base + Lo.off_red);
   uint64_t* bars = reinterpret_cast<uint64_t*>(S.red + 64);
   S.C.full = bars;
-  S.C.empty = bars + STAGES;
-  S.C.bc_full = bars + 2 * STAGES;
-  S.C.bc_empty = bars + 2 * STAGES + 2;
-  S.C.bar_done = bars + 2 * STAGES + 4;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
+  S.C.empty = bars + MAX_STAGES;
+  S.C.bc_full = bars + 2 * MAX_STAGES;
+  S.C.bc_empty = bars + 2 * MAX_STAGES + 2;
+  S.C.bar_done = bars + 2 * MAX_STAGES + 4;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * MAX_STAGES + 5);
   S.C.abort = reinterpret_cast<int*>(tslot + 1);
   S.C.m = Lo.m;
   S.C.rc = Lo.rc;
@@ -82,8 +113,10 @@ __device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* ra
   S.C.three = three;
   S.C.ph = S.C.started = S.C.bc_ph = S.C.bc_started = S.C.done_ph = 0u;
   S.C.st_next = 0;
+  S.C.nst = Lo.ring.stages;
+  S.C.wps = Lo.ring.per_stage;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < MAX_STAGES; ++s) {
       mbar_init(&S.C.full[s], NBUILD_WARPS);
       mbar_init(&S.C.empty[s], 1);
     }

@@ -46,9 +46,14 @@
 //  BF16x1 keeps A_hi B_hi.  fp32 accumulation in TMEM.
 //
 //  Pipeline: one MMA warp (one elected lane issues every MMA) and builder
-//  warps; a ring of STAGES window buffers and one copy slot per phase, each
-//  guarded by a full barrier (builder arrivals) and an empty barrier
-//  (tcgen05.commit).
+//  warps; a ring of stages of one to three window buffers each, and one copy
+//  slot per phase, each guarded by a full barrier (builder arrivals) and an
+//  empty barrier (tcgen05.commit).  A stage release costs the tensor pipe
+//  far more than an MMA (fitted from phase timers at n = 8400: ~870 cycles
+//  per commit against ~70 per M128 N144 K16 instruction), so long tile
+//  sequences run two stages
+//  of two or three windows -- one commit per two or three tiles -- and short
+//  ones three single-window stages (see ring_for).
 //  Every wait gives up after ~2^31 clock cycles, records SIDON_ERR_TIMEOUT in
 //  the library's device status word and unwinds.
 // ---------------------------------------------------------------------------
@@ -63,12 +68,12 @@ namespace tc {
 constexpr int L = 128;               // UMMA M (lanes)
 constexpr int BL = 64;               // input block = K of a tile
 constexpr int KSTEPS = BL / 16;      // K16 instructions per tile and product
-constexpr int STAGES = 3;            // window ring depth
+constexpr int MAX_STAGES = 3;        // window ring: at most three stages
 constexpr int DG = 16;               // accumulator column granule of an MMA destination
 constexpr int ZP = DG;               // zero rows in front of a block-matrix copy
 constexpr int WIN_CM = 24;           // core matrices per window (23 used)
 constexpr int PLANE = WIN_CM * 128;  // bytes per hi or lo window plane
-constexpr int STAGE_BYTES = 2 * PLANE;
+constexpr int WIN_BYTES = 2 * PLANE;   // one window: hi plane | lo plane
 constexpr int NTHREADS = 256;        // 8 warps: lanes quadrant = warp % 4
 constexpr long long kWaitCycles = 1ll << 31;
 
@@ -200,10 +205,10 @@ constexpr int NBUILD = NBUILD_WARPS * 32;
 // Shared state of one CTA.  Every thread holds a copy; the pipeline counters
 // of a role are kept identical by every thread of that role.
 struct Ctx {
-  unsigned char* stages;   // STAGES x (hi plane | lo plane), 1 KB aligned
+  unsigned char* stages;   // nst x wps windows (hi plane | lo plane), 1 KB aligned
   unsigned char* bc;       // the phase's B-matrix copy (hi plane, lo plane after it)
-  uint64_t* full;          // STAGES "window ready" barriers (NBUILD_WARPS arrivals)
-  uint64_t* empty;         // STAGES "window consumed" barriers (tcgen05.commit)
+  uint64_t* full;          // nst "windows ready" barriers (NBUILD_WARPS arrivals)
+  uint64_t* empty;         // nst "windows consumed" barriers (tcgen05.commit)
   uint64_t* bc_full;       // "copy ready" barrier (NBUILD_WARPS arrivals; [0] used)
   uint64_t* bc_empty;      // "copy consumed" barrier (tcgen05.commit; [0] used)
   uint64_t* bar_done;      // "all MMAs of a phase done"
@@ -215,6 +220,7 @@ struct Ctx {
   // the copy slots; done_ph = parity of the next bar_done wait
   uint32_t ph, started, bc_ph, bc_started, done_ph;
   int st_next;             // next stage in the ring
+  int nst, wps;            // ring shape: stages, windows per stage
   int* abort;              // shared abort flag
   int m, rc, rcc, n, dmax; // blocks, conv / corr copy rows, cells, last tile
   bool three;              // BF16x3 (else BF16x1)
@@ -352,16 +358,16 @@ __device__ __forceinline__ uint32_t split_pack(float x, float lsc) {
   return (uint32_t)__bfloat16_as_ushort(h) | ((uint32_t)__bfloat16_as_ushort(l) << 16);
 }
 
-// Window of tile w into stage st: CM[q][i][j] = a[64 w - 63 + 8 q + i + j],
+// Window of tile w into window slot `slot` of the ring: CM[q][i][j] = a[64 w - 63 + 8 q + i + j],
 // planes hi and lsc * lo.  Chunk t = 8 q + i (16 bytes at offset 16 t of a
 // plane) holds the 8 cells from 64 w - 63 + t on: consecutive chunks are
 // windows shifted by one cell.  A warp covers 32 chunks: every lane splits
 // two cells (t and t + 32) once, and the 8 cells of its chunk arrive by warp
 // shuffles, so each cell is loaded and split once per warp instead of once
 // per chunk row.  Warp-uniform (all 32 lanes take part in the shuffles).
-__device__ __forceinline__ void build_window(Ctx& C, int st, const float* sa, int w, float lsc,
+__device__ __forceinline__ void build_window(Ctx& C, int slot, const float* sa, int w, float lsc,
                                              int bt) {
-  unsigned char* hi = C.stages + st * STAGE_BYTES;
+  unsigned char* hi = C.stages + slot * WIN_BYTES;
   unsigned char* lo = hi + PLANE;
   const int lane = bt & 31;
   const int base0 = 64 * w - 63;
@@ -417,11 +423,12 @@ __device__ __forceinline__ int col_corr(int m) { return conv_width(m); }
 //             (hi | lo, one slot), 3 products.
 enum TileMode { CONV_SYM = 0, CONV_X = 1, CORR = 2 };
 
-// Issue the MMAs of one tile (one thread).  three_prod selects the
-// 3-product arithmetic, otherwise the 2-product symmetric convolution.
-__device__ __forceinline__ void issue_tile(Ctx& C, int st, uint32_t b_hi, uint32_t b_lo,
+// Issue the MMAs of one tile (one thread), its window in ring slot `slot`.
+// three_prod selects the 3-product arithmetic, otherwise the 2-product
+// symmetric convolution.
+__device__ __forceinline__ void issue_tile(Ctx& C, int slot, uint32_t b_hi, uint32_t b_lo,
                                            uint32_t b_lbo_bytes, const Tile& T, bool three_prod) {
-  const uint32_t a_hi = smem_u32(C.stages + st * STAGE_BYTES);
+  const uint32_t a_hi = smem_u32(C.stages + slot * WIN_BYTES);
   const uint32_t a_lo = a_hi + PLANE;
   const uint32_t bh0 = b_hi + 16u * (uint32_t)T.x0;
   const uint32_t bl0 = b_lo + 16u * (uint32_t)T.x0;
@@ -445,15 +452,22 @@ __device__ __forceinline__ void issue_tile(Ctx& C, int st, uint32_t b_hi, uint32
 }
 
 // Run the tiles w = 0, 2, ..., dmax through the warp-specialised pipeline:
-// the builders write the phase's B copy once (one copy slot), then a window
-// per tile into the stage ring.  Ends with every MMA of the sequence
+// the builders write the phase's B copy once (one copy slot), then the
+// windows of wps consecutive tiles into each stage of the ring; the MMA lane
+// issues a stage's tiles in order and releases the stage with one commit.
+// Every accumulator receives its MMAs in the same order whatever the ring
+// shape, so the results do not depend on it.  Ends with every MMA of the sequence
 // complete (bar_done) and the accumulator readable by all warps.
 //   wsrc: padded shared heights (windows; the copy too for CONV_SYM);
 //   bsrc / blen: the copy source of CONV_X (see build_conv_copy) or the
 //   padded shared weights of CORR.
-template <int MODE, bool PREBUILT = false>
-__device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen,
-                                          unsigned int* status) {
+//   WPS: windows per stage fixed at compile time (1: three single-window
+//   stages), or 0 to take the ring shape from C.wps / C.nst.
+template <int MODE, bool PREBUILT, int WPS>
+__device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const float* bsrc,
+                                               int blen, unsigned int* status) {
+  const int wps = WPS ? WPS : C.wps;
+  const int nst = WPS ? 3 : C.nst;
   constexpr bool corr = MODE == CORR;
   constexpr bool three_prod = MODE != CONV_SYM;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -471,7 +485,7 @@ __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float
       C.bc_ph ^= 1u;
       const uint32_t bbase = smem_u32(C.bc);
       const uint32_t blo = bbase + (uint32_t)rows * 128u;
-      for (int w = 0; ok && w <= C.dmax; w += 2) {
+      auto tile_of = [&](int w) {
         Tile T;
         if (corr) {
           T.dcol = col_corr(m);
@@ -483,12 +497,16 @@ __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float
           T.x0 = t + ZP;
           T.N = round_up(m - t, 16);
         }
+        return T;
+      };
+      for (int w = 0; ok && w <= C.dmax; w += 2 * wps) {
         if (!wait_phase(C, &C.full[st], (C.ph >> st) & 1u, status)) { ok = false; break; }
         C.ph ^= 1u << st;
         fence_after();
-        issue_tile(C, st, bbase, blo, lbo, T, three_prod);
+        for (int h = 0; h < wps && w + 2 * h <= C.dmax; ++h)
+          issue_tile(C, st * wps + h, bbase, blo, lbo, tile_of(w + 2 * h), three_prod);
         mma_commit(&C.empty[st]);
-        st = (st + 1 == STAGES) ? 0 : st + 1;
+        st = (st + 1 == nst) ? 0 : st + 1;
       }
       mma_commit(&C.bc_empty[0]);
       mma_commit(C.bar_done);
@@ -511,7 +529,7 @@ __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float
       __syncwarp();
       if (lane == 0) mbar_arrive(&C.bc_full[0]);
     }
-    for (int w = 0; ok && w <= C.dmax; w += 2) {
+    for (int w = 0; ok && w <= C.dmax; w += 2 * wps) {
       if ((C.started >> st) & 1u) {
         if (!wait_phase(C, &C.empty[st], (C.ph >> st) & 1u, status)) {
           ok = false;
@@ -520,11 +538,12 @@ __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float
         C.ph ^= 1u << st;
       }
       C.started |= 1u << st;
-      build_window(C, st, wsrc, w, lsc, bt);
+      for (int h = 0; h < wps && w + 2 * h <= C.dmax; ++h)
+        build_window(C, st * wps + h, wsrc, w + 2 * h, lsc, bt);
       fence_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&C.full[st]);
-      st = (st + 1 == STAGES) ? 0 : st + 1;
+      st = (st + 1 == nst) ? 0 : st + 1;
     }
   }
   C.st_next = st;
@@ -533,6 +552,20 @@ __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float
   fence_after();
   __syncthreads();
   return ok && !*((volatile int*)C.abort);
+}
+
+// The tile sequence on the CTA's ring (ring_for).  Three single-window
+// stages run a specialisation with the shape fixed at compile time, the
+// multi-window shapes one that reads it.  Measured per step against the
+// single-window ring alone: the same within 1% at n <= 1024 and n = 9728
+// (where the ring stays single-window; reading the shape there cost 2-4%),
+// 3% / 7% / 9% faster at n = 2048 / 4096 / 8400; specialising the 2 x 2 and
+// 2 x 3 shapes as well measured 1-8% slower than reading them.
+template <int MODE, bool PREBUILT = false>
+__device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen,
+                                          unsigned int* status) {
+  if (C.wps == 1) return run_tiles_ring<MODE, PREBUILT, 1>(C, wsrc, bsrc, blen, status);
+  return run_tiles_ring<MODE, PREBUILT, 0>(C, wsrc, bsrc, blen, status);
 }
 
 // lane quadrant / column-half of the calling warp (8 warps: 4 quadrants x 2)
