@@ -353,7 +353,7 @@ k_local_search_tc_seg(float* pop, float* mom, float* vel, int P, int n,
 // As k_lp_forward: M refined in fp64 over the near-maximal k (the split
 // error of b is < 3e-5 of max b), S in fp64, R from the tensor-core b.
 constexpr int kRefineCap = 1024;
-static_assert(kRefineCap * sizeof(int) <= (size_t)3 * WIN_BYTES, "list fits the smallest ring");
+static_assert(kRefineCap * sizeof(int) <= (size_t)3 * stage_bytes(1), "list fits the smallest ring");
 
 __global__ void __launch_bounds__(NTHREADS, 1)
 k_lp_forward_tc(const float* __restrict__ pop, int n, float p, float* __restrict__ value,

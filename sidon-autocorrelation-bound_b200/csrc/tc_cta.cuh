@@ -4,8 +4,10 @@
 //  reset.  One CTA = 8 warps = one tile pipeline (tc_engine.cuh).
 //
 //  Shared memory (see Layout):
-//    stages  3 x 1, 2 x 2 or 2 x 3 windows of 6 KB (hi | lo planes):
-//            stages x windows per stage, from ring_for
+//    stages  the window ring (ring_for): 3 stages of one tile's window
+//            (6 KB: hi | lo planes of 24 core matrices) or 2 stages of the
+//            windows of T = 2 .. 5 consecutive tiles (2 x (16 T + 8) core
+//            matrices, 10-22 KB)
 //    bc      the tile phase's B-matrix copy (hi, or hi | lo); after a
 //            tile phase, gather scratch for up to 2n-1 outputs
 //    sa      fp32 heights, padded block layout (cell i at i + 4 floor(i/64)),
@@ -19,27 +21,27 @@
 namespace sidon {
 namespace tc {
 
-// Shared memory a multi-window ring may grow the plan to: the sm_100
-// per-block opt-in limit (227 KB) less 2 KB for the kernels' static shared
-// variables.  (The three single-window stages are taken at any size.)
-constexpr size_t kSmemBudget = 232448 - 2048;
-// Tile sequences of at least this many blocks take the multi-window stages.
-// Measured per step, identical results: n = 8400 (132 blocks) 13% faster
-// with 2 x 2 windows than with 3 x 1, n = 2048 (32 blocks) 10% faster, n = 512
-// (8 blocks: 5 tiles) 4% slower.
+// Shared memory a multi-tile ring may grow the plan to: the sm_100
+// per-block opt-in limit (227 KB) less 1 KB for the kernels' static shared
+// variables (at most 264 bytes).  (The single-tile ring is taken at any size.)
+constexpr size_t kSmemBudget = 232448 - 1024;
+// Tile sequences of at least this many blocks take the multi-tile stages
+// (per step, identical results: the same at n = 1024, 16 blocks; 3-9% faster
+// from n = 2048 on; at n = 512, 8 blocks and 5 tiles, two-tile stages were 4%
+// slower).
 constexpr int kRingMinBlocks = 16;
+constexpr int kMaxStageTiles = 5;
 
 struct Ring {
-  int stages, per_stage;
+  int stages, per_stage;    // stages, tiles per stage
 };
 // The window ring for m blocks when everything else takes `other` bytes:
-// two stages of three windows, else of two, when the sequence is long and
-// they fit the budget; else three single-window stages.
+// two stages of as many tiles (up to five) as the budget allows when the
+// sequence is long, else three single-tile stages.
 __host__ __device__ __forceinline__ Ring ring_for(int m, size_t other) {
-  if (m >= kRingMinBlocks) {
-    if (other + 6 * (size_t)WIN_BYTES <= kSmemBudget) return Ring{2, 3};
-    if (other + 4 * (size_t)WIN_BYTES <= kSmemBudget) return Ring{2, 2};
-  }
+  if (m >= kRingMinBlocks)
+    for (int T = kMaxStageTiles; T >= 2; --T)
+      if (other + 2 * (size_t)stage_bytes(T) <= kSmemBudget) return Ring{2, T};
   return Ring{3, 1};
 }
 
@@ -55,7 +57,7 @@ struct Layout {
     sa_len = 68 * (m + 8);                 // padded heights, 136 cells of margin in front
     cb_len = 68 * (2 * m + 2);             // padded weights / gather scratch
     ring = ring_for(m, place(0));          // the ring takes whole KB: the rest keeps its padding
-    place((size_t)ring.stages * ring.per_stage * WIN_BYTES);
+    place((size_t)ring.stages * stage_bytes(ring.per_stage));
   }
   // lay out everything after a ring of `o` bytes; returns the total
   __host__ __device__ size_t place(size_t o) {

@@ -46,14 +46,13 @@
 //  BF16x1 keeps A_hi B_hi.  fp32 accumulation in TMEM.
 //
 //  Pipeline: one MMA warp (one elected lane issues every MMA) and builder
-//  warps; a ring of stages of one to three window buffers each, and one copy
+//  warps; a ring of stages holding the windows of one to five tiles each, and one copy
 //  slot per phase, each guarded by a full barrier (builder arrivals) and an
 //  empty barrier (tcgen05.commit).  A stage release costs the tensor pipe
 //  far more than an MMA (fitted from phase timers at n = 8400: ~870 cycles
 //  per commit against ~70 per M128 N144 K16 instruction), so long tile
-//  sequences run two stages
-//  of two or three windows -- one commit per two or three tiles -- and short
-//  ones three single-window stages (see ring_for).
+//  sequences run two stages of two to five tiles -- one commit per stage --
+//  and short ones three single-tile stages (see ring_for).
 //  Every wait gives up after ~2^31 clock cycles, records SIDON_ERR_TIMEOUT in
 //  the library's device status word and unwinds.
 // ---------------------------------------------------------------------------
@@ -71,9 +70,14 @@ constexpr int KSTEPS = BL / 16;      // K16 instructions per tile and product
 constexpr int MAX_STAGES = 3;        // window ring: at most three stages
 constexpr int DG = 16;               // accumulator column granule of an MMA destination
 constexpr int ZP = DG;               // zero rows in front of a block-matrix copy
-constexpr int WIN_CM = 24;           // core matrices per window (23 used)
-constexpr int PLANE = WIN_CM * 128;  // bytes per hi or lo window plane
-constexpr int WIN_BYTES = 2 * PLANE;   // one window: hi plane | lo plane
+// A stage of the window ring holds the windows of T consecutive tiles.  The
+// window of tile w + 2 is the window of tile w moved by 128 cells = 16 core
+// matrices, so the T windows are one run of 16 T + 7 core matrices (one more
+// is built as padding) per plane: tile h of the stage starts at core matrix
+// 16 h.
+__host__ __device__ constexpr int stage_cms(int T) { return 16 * T + 8; }
+__host__ __device__ constexpr int stage_plane_bytes(int T) { return stage_cms(T) * 128; }
+__host__ __device__ constexpr int stage_bytes(int T) { return 2 * stage_plane_bytes(T); }
 constexpr int NTHREADS = 256;        // 8 warps: lanes quadrant = warp % 4
 constexpr long long kWaitCycles = 1ll << 31;
 
@@ -205,7 +209,7 @@ constexpr int NBUILD = NBUILD_WARPS * 32;
 // Shared state of one CTA.  Every thread holds a copy; the pipeline counters
 // of a role are kept identical by every thread of that role.
 struct Ctx {
-  unsigned char* stages;   // nst x wps windows (hi plane | lo plane), 1 KB aligned
+  unsigned char* stages;   // nst stages of wps tiles' windows (hi plane | lo plane), 1 KB aligned
   unsigned char* bc;       // the phase's B-matrix copy (hi plane, lo plane after it)
   uint64_t* full;          // nst "windows ready" barriers (NBUILD_WARPS arrivals)
   uint64_t* empty;         // nst "windows consumed" barriers (tcgen05.commit)
@@ -358,20 +362,24 @@ __device__ __forceinline__ uint32_t split_pack(float x, float lsc) {
   return (uint32_t)__bfloat16_as_ushort(h) | ((uint32_t)__bfloat16_as_ushort(l) << 16);
 }
 
-// Window of tile w into window slot `slot` of the ring: CM[q][i][j] = a[64 w - 63 + 8 q + i + j],
-// planes hi and lsc * lo.  Chunk t = 8 q + i (16 bytes at offset 16 t of a
-// plane) holds the 8 cells from 64 w - 63 + t on: consecutive chunks are
-// windows shifted by one cell.  A warp covers 32 chunks: every lane splits
-// two cells (t and t + 32) once, and the 8 cells of its chunk arrive by warp
-// shuffles, so each cell is loaded and split once per warp instead of once
-// per chunk row.  Warp-uniform (all 32 lanes take part in the shuffles).
-__device__ __forceinline__ void build_window(Ctx& C, int slot, const float* sa, int w, float lsc,
-                                             int bt) {
-  unsigned char* hi = C.stages + slot * WIN_BYTES;
-  unsigned char* lo = hi + PLANE;
+// Windows of the nt tiles w0, w0 + 2, ... into stage st of a ring of
+// T-tile stages: core matrices CM[q][i][j] = a[64 w0 - 63 + 8 q + i + j],
+// q < 16 nt + 8, planes hi and lsc * lo.  Chunk t = 8 q + i (16 bytes at
+// offset 16 t of a plane) holds the 8 cells from 64 w0 - 63 + t on:
+// consecutive chunks are windows shifted by one cell.  A warp covers 32
+// chunks: every lane splits two cells (t and t + 32) once, and the 8 cells of
+// its chunk arrive by warp shuffles, so each cell is loaded and split once
+// per warp instead of once per chunk row.  Warp-uniform (all 32 lanes take
+// part in the shuffles).  The highest cell read, 64 (w0 + 2 nt) + 32, is the
+// one a single window of the stage's last tile reads.
+__device__ __forceinline__ void build_stage(Ctx& C, int st, int T, const float* sa, int w0,
+                                            int nt, float lsc, int bt) {
+  unsigned char* hi = C.stages + st * stage_bytes(T);
+  unsigned char* lo = hi + stage_plane_bytes(T);
   const int lane = bt & 31;
-  const int base0 = 64 * w - 63;
-  for (int t0 = bt - lane; t0 < WIN_CM * 8; t0 += NBUILD) {
+  const int base0 = 64 * w0 - 63;
+  const int nchunk = 8 * stage_cms(nt);
+  for (int t0 = bt - lane; t0 < nchunk; t0 += NBUILD) {
     const int c = base0 + t0 + lane;
     const uint32_t p0 = split_pack(sa[pidx(c)], lsc);
     const uint32_t p1 = split_pack(sa[pidx(c + 32)], lsc);
@@ -388,7 +396,7 @@ __device__ __forceinline__ void build_window(Ctx& C, int slot, const float* sa, 
     const uint4 vl = make_uint4(__byte_perm(P[0], P[1], 0x7632), __byte_perm(P[2], P[3], 0x7632),
                                 __byte_perm(P[4], P[5], 0x7632), __byte_perm(P[6], P[7], 0x7632));
     const int t = t0 + lane;
-    if (t < WIN_CM * 8) {
+    if (t < nchunk) {
       *reinterpret_cast<uint4*>(hi + 16 * t) = vh;
       *reinterpret_cast<uint4*>(lo + 16 * t) = vl;
     }
@@ -423,13 +431,14 @@ __device__ __forceinline__ int col_corr(int m) { return conv_width(m); }
 //             (hi | lo, one slot), 3 products.
 enum TileMode { CONV_SYM = 0, CONV_X = 1, CORR = 2 };
 
-// Issue the MMAs of one tile (one thread), its window in ring slot `slot`.
-// three_prod selects the 3-product arithmetic, otherwise the 2-product
-// symmetric convolution.
-__device__ __forceinline__ void issue_tile(Ctx& C, int slot, uint32_t b_hi, uint32_t b_lo,
-                                           uint32_t b_lbo_bytes, const Tile& T, bool three_prod) {
-  const uint32_t a_hi = smem_u32(C.stages + slot * WIN_BYTES);
-  const uint32_t a_lo = a_hi + PLANE;
+// Issue the MMAs of one tile (one thread): tile h of stage st of a ring of
+// ts-tile stages.  three_prod selects the 3-product arithmetic, otherwise the
+// 2-product symmetric convolution.
+__device__ __forceinline__ void issue_tile(Ctx& C, int st, int ts, int h, uint32_t b_hi,
+                                           uint32_t b_lo, uint32_t b_lbo_bytes, const Tile& T,
+                                           bool three_prod) {
+  const uint32_t a_hi = smem_u32(C.stages + st * stage_bytes(ts)) + (uint32_t)h * 16u * 128u;
+  const uint32_t a_lo = a_hi + (uint32_t)stage_plane_bytes(ts);
   const uint32_t bh0 = b_hi + 16u * (uint32_t)T.x0;
   const uint32_t bl0 = b_lo + 16u * (uint32_t)T.x0;
   const uint32_t id = idesc_bf16(T.N);
@@ -453,7 +462,8 @@ __device__ __forceinline__ void issue_tile(Ctx& C, int slot, uint32_t b_hi, uint
 
 // Run the tiles w = 0, 2, ..., dmax through the warp-specialised pipeline:
 // the builders write the phase's B copy once (one copy slot), then the
-// windows of wps consecutive tiles into each stage of the ring; the MMA lane
+// windows of wps consecutive tiles into each stage of the ring (one run of
+// core matrices, build_stage); the MMA lane
 // issues a stage's tiles in order and releases the stage with one commit.
 // Every accumulator receives its MMAs in the same order whatever the ring
 // shape, so the results do not depend on it.  Ends with every MMA of the sequence
@@ -504,7 +514,7 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
         C.ph ^= 1u << st;
         fence_after();
         for (int h = 0; h < wps && w + 2 * h <= C.dmax; ++h)
-          issue_tile(C, st * wps + h, bbase, blo, lbo, tile_of(w + 2 * h), three_prod);
+          issue_tile(C, st, wps, h, bbase, blo, lbo, tile_of(w + 2 * h), three_prod);
         mma_commit(&C.empty[st]);
         st = (st + 1 == nst) ? 0 : st + 1;
       }
@@ -538,8 +548,8 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
         C.ph ^= 1u << st;
       }
       C.started |= 1u << st;
-      for (int h = 0; h < wps && w + 2 * h <= C.dmax; ++h)
-        build_window(C, st * wps + h, wsrc, w + 2 * h, lsc, bt);
+      const int nt = (C.dmax - w) / 2 + 1;
+      build_stage(C, st, wps, wsrc, w, nt < wps ? nt : wps, lsc, bt);
       fence_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&C.full[st]);

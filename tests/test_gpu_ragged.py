@@ -55,6 +55,22 @@ def test_ragged_local_search_matches_uniform(cuda, precision):
         assert (got[p] >= 0).all()
 
 
+@pytest.mark.parametrize("n_max", [9216, 9728])
+def test_window_ring_shape_does_not_change_results(cuda, n_max):
+    """The tensor-core CTA sizes its window ring from the batch's largest
+    row: two stages of three windows for a uniform n = 8400 or 2048, of two
+    at n_max = 9216, three single windows at n = 300 and at n_max = 9728.
+    The same rows give the same heights bit for bit under every shape."""
+    rows, b = _batch([300, 2048, 8400, n_max], 21, cuda)
+    K().run_local_search_ragged(b, 12, 2.0, 512.0, 1e-3, 1e-3, precision="bf16x3")
+    got = b.rows()
+    assert _status() == 0
+    for p, r in enumerate(rows[:3]):
+        u = torch.as_tensor(r[None, :], device=cuda)
+        K().run_local_search(u, 12, 2.0, 512.0, 1e-3, 1e-3, precision="bf16x3")
+        np.testing.assert_array_equal(got[p], u.cpu().numpy()[0], err_msg=f"candidate {p}")
+
+
 def test_ragged_local_search_order_and_skip(cuda):
     rows, b1 = _batch(SIZES, 9, cuda)
     _, b2 = _batch(SIZES, 9, cuda)
