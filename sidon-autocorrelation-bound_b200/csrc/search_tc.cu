@@ -39,20 +39,50 @@ __device__ __forceinline__ void note_bad(bool bad, unsigned int* status) {
   if (bad) atomicCAS(status, 0u, (unsigned int)SIDON_ERR_NONFINITE);
 }
 
+// The autoconvolution's B copy of the heights in S.sa (the layout of
+// build_conv_copy, hi plane), written by all threads before a candidate's
+// first step; each step's renormalisation writes the next one.  Every step
+// then takes the prebuilt form of the tile phase, so the kernels hold one
+// copy of the convolution's tile code (measured: 3-20% faster steps than
+// holding both forms, as long as the code stays small).  The caller
+// synchronises before the step.
+__device__ __forceinline__ void write_conv_copy(Shared& S) {
+  Ctx& C = S.C;
+  const int rows = C.rc;
+  for (int cq = threadIdx.x; cq < rows * 8; cq += NTHREADS) {
+    const int h = cq / rows, x = cq - h * rows, J = x - ZP;
+    float v[8];
+    if (J >= 0 && J < C.m) {
+      // cells 64 J + 56 - 8 h .. + 7, reversed (zero beyond n in the padding)
+      const float* q = S.sa + pidx(64 * J + 56 - 8 * h);
+      const float4 u0 = *reinterpret_cast<const float4*>(q);
+      const float4 u1 = *reinterpret_cast<const float4*>(q + 4);
+      v[0] = u1.w; v[1] = u1.z; v[2] = u1.y; v[3] = u1.x;
+      v[4] = u0.w; v[5] = u0.z; v[6] = u0.y; v[7] = u0.x;
+    } else {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) v[t] = 0.f;
+    }
+    conv_copy_chunk(C, x, h, v);
+  }
+  fence_async_smem();
+}
+
 // One L^p-Adam / mirror step of the candidate resident in S (n cells; its
-// Adam moments in the global rows mg, vg): convolution, max, weights written
-// into the correlation copy, correlation, update, renormalisation, and the
-// next step's autoconvolution copy (copy_ready).  b1t / b2t are beta^(step+1).
-// Returns 0, or 1 when M <= 0 stops the anneal (nothing changed), or 2 when a
-// tile phase was aborted.  Ends synchronised.
+// Adam moments in the global rows mg, vg; the autoconvolution copy of the
+// heights in place): convolution, max, weights written into the correlation
+// copy, correlation, update, renormalisation, and the next step's
+// autoconvolution copy.  b1t / b2t are beta^(step+1).  Returns 0, or 1 when
+// M <= 0 stops the anneal (nothing changed), or 2 when a tile phase was
+// aborted.  Ends synchronised.
 __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, int mode,
                                             float pexp, float lr, float beta1, float beta2,
                                             float b1t, float b2t, float* mg, float* vg,
-                                            bool& copy_ready, unsigned int* status) {
+                                            unsigned int* status) {
   Ctx& C = S.C;
   const int nb = 2 * n - 1;
   prime(C, true);
-  if (!(copy_ready ? conv_tc_prebuilt(C, S.sa, status) : conv_tc(C, S.sa, status))) return 2;
+  if (!conv_tc_prebuilt(C, S.sa, status)) return 2;
   const float M = block_max(gather_conv(C, ln, S.cb), S.red);   // b in cb
   if (!(M > 0.f)) return 1;
   // c_k = (1+d)^(p-1), R = sum c_k (1+d), d = (b_k - M)/M, written straight
@@ -168,7 +198,6 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
     }
     fence_async_smem();
   }
-  copy_ready = true;
   __syncthreads();
   return 0;
 }
@@ -211,11 +240,12 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
   }
   note_bad(bad, status);
   __syncthreads();
+  write_conv_copy(S);
+  __syncthreads();
 
   const float lnPr = (float)log((double)pEnd / (double)pStart);
   const float lnLr = (float)log((double)lrEnd / (double)lrStart);
   float b1t = 1.f, b2t = 1.f;
-  bool copy_ready = false;   // the autoconvolution copy of sa is in place
 
   for (int it = 0; it < iters; ++it) {
     const float frac = iters > 1 ? (float)it / (float)(iters - 1) : 0.f;
@@ -225,7 +255,7 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
     b1t *= beta1;
     b2t *= beta2;
     const int rs = lp_adam_step(S, ln, n, mode, pexp, lr, beta1, beta2, b1t, b2t, mg, vg,
-                                copy_ready, status);
+                                status);
     if (rs) break;
   }
   __syncthreads();
@@ -271,12 +301,13 @@ __device__ __forceinline__ void run_piece(Shared& S, const Lane& ln, float* pop,
   }
   note_bad(bad, status);
   __syncthreads();
+  write_conv_copy(S);
+  __syncthreads();
   float b1t = 1.f, b2t = 1.f;
   for (int it = 0; it < s0; ++it) {        // beta^s0, multiplied up as the fused kernel does
     b1t *= beta1;
     b2t *= beta2;
   }
-  bool copy_ready = false;
   int rs = 0;
   for (int it = s0; it < s1; ++it) {
     const float frac = iters > 1 ? (float)it / (float)(iters - 1) : 0.f;
@@ -284,8 +315,7 @@ __device__ __forceinline__ void run_piece(Shared& S, const Lane& ln, float* pop,
     const float lr = lrStart * expf(lnLr * frac);
     b1t *= beta1;
     b2t *= beta2;
-    rs = lp_adam_step(S, ln, n, mode, pexp, lr, beta1, beta2, b1t, b2t, mg, vg, copy_ready,
-                      status);
+    rs = lp_adam_step(S, ln, n, mode, pexp, lr, beta1, beta2, b1t, b2t, mg, vg, status);
     if (rs) break;          // M <= 0 stops the anneal; the heights are as they were
   }
   __syncthreads();
@@ -320,30 +350,38 @@ k_local_search_tc_seg(float* pop, float* mom, float* vel, int P, int n,
                   mode_arr ? mode_arr[pid] : mode_default, pStart, lnPr, lrStart, lnLr, beta1,
                   beta2, status);
     };
-    if (head) {
-      piece(last);
-      __threadfence();        // every thread's heights and moments reach L2 ...
-      __syncthreads();
-      if (threadIdx.x == 0) atomicExch(&flags[last], 1u);   // ... before the flag
-    }
-    for (int pid = tail ? first + 1 : first; pid <= (head ? last - 1 : last); ++pid) piece(pid);
-    if (tail && !(head && first == last)) {
-      if (threadIdx.x == 0) {
-        s_ok = 1;
-        volatile unsigned int* f = flags + first;
-        const long long t0 = clock64();
-        while (*f == 0u) {
-          if (clock64() - t0 > kWaitCycles) {
-            s_ok = 0;
-            atomicCAS(status, 0u, (unsigned int)SIDON_ERR_TIMEOUT);
-            break;
+    // the pieces in order -- the head, the whole candidates, the tail --
+    // through one call site, so the step loop is in the kernel once
+    const int mid0 = tail ? first + 1 : first, mid1 = head ? last - 1 : last;
+    const bool has_tail = tail && !(head && first == last);
+    const int npieces = (head ? 1 : 0) + (mid1 >= mid0 ? mid1 - mid0 + 1 : 0) + (has_tail ? 1 : 0);
+    for (int q = 0; q < npieces; ++q) {
+      const bool is_head = head && q == 0, is_tail = has_tail && q == npieces - 1;
+      const int pid = is_head ? last : is_tail ? first : mid0 + q - (head ? 1 : 0);
+      if (is_tail) {
+        if (threadIdx.x == 0) {
+          s_ok = 1;
+          volatile unsigned int* f = flags + first;
+          const long long t0 = clock64();
+          while (*f == 0u) {
+            if (clock64() - t0 > kWaitCycles) {
+              s_ok = 0;
+              atomicCAS(status, 0u, (unsigned int)SIDON_ERR_TIMEOUT);
+              break;
+            }
+            __nanosleep(200);
           }
-          __nanosleep(200);
+          __threadfence();
         }
-        __threadfence();
+        __syncthreads();
+        if (!s_ok) break;
       }
-      __syncthreads();
-      if (s_ok) piece(first);
+      piece(pid);
+      if (is_head) {
+        __threadfence();        // every thread's heights and moments reach L2 ...
+        __syncthreads();
+        if (threadIdx.x == 0) atomicExch(&flags[last], 1u);   // ... before the flag
+      }
     }
   }
   teardown(S);
