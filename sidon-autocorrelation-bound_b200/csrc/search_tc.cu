@@ -28,7 +28,7 @@ __device__ unsigned int g_status_word = 0u;   // SIDON_ERR_TIMEOUT after a timed
 // cells per thread of the fused step's elementwise update: every n the
 // kernels accept (conv + corr accumulators within 512 TMEM columns, n <= 9728)
 // is covered by kCellsPerThread * NTHREADS
-constexpr int kCellsPerThread = 38;
+constexpr int kCellsPerThread = 26;
 
 // ------------------------------ local search ------------------------------
 // Heights must be finite and non-negative; a candidate that is not is

@@ -1,7 +1,7 @@
 // ---------------------------------------------------------------------------
 //  tc_cta.cuh -- the per-CTA frame of the tensor-core kernels: the shared-
 //  memory plan, barrier / TMEM set-up and release, and the per-candidate
-//  reset.  One CTA = 8 warps = one tile pipeline (tc_engine.cuh).
+//  reset.  One CTA = 12 warps = one tile pipeline (tc_engine.cuh).
 //
 //  Shared memory (see Layout):
 //    stages  the window ring (ring_for): 3 stages of one tile's window

@@ -78,7 +78,12 @@ constexpr int ZP = DG;               // zero rows in front of a block-matrix cop
 __host__ __device__ constexpr int stage_cms(int T) { return 16 * T + 8; }
 __host__ __device__ constexpr int stage_plane_bytes(int T) { return stage_cms(T) * 128; }
 __host__ __device__ constexpr int stage_bytes(int T) { return 2 * stage_plane_bytes(T); }
-constexpr int NTHREADS = 256;        // 8 warps: lanes quadrant = warp % 4
+// 12 warps: lane quadrant = warp % 4 (three warps per quadrant).  Measured
+// per step against 8 and 16 warps: 6% faster than 8 at n = 8400 (256
+// candidates; the latency-bound gathers, weights and update get more warps,
+// and the step compiles without spills), 16 slower than 8 at most n.
+constexpr int NTHREADS = 384;
+constexpr int WARPS_PER_QUAD = NTHREADS / 128;
 constexpr long long kWaitCycles = 1ll << 31;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -405,9 +410,8 @@ __device__ __forceinline__ void build_stage(Ctx& C, int st, int T, const float* 
 
 // Zero accumulator columns [col0, col0 + ncols) (ncols multiple of 32).
 __device__ __forceinline__ void zero_acc(Ctx& C, int col0, int ncols) {
-  const int warp = threadIdx.x >> 5, quad = warp & 3, half = warp >> 2;
-  const int halves = (blockDim.x >> 5) / 4;
-  for (int c = half * 32; c < ncols; c += 32 * halves)
+  const int warp = threadIdx.x >> 5, quad = warp & 3, sub = warp >> 2;
+  for (int c = sub * 32; c < ncols; c += 32 * WARPS_PER_QUAD)
     tmem_zero32(C.tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(col0 + c));
   tmem_wait_st();
 }
@@ -578,25 +582,26 @@ __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float
   return run_tiles_ring<MODE, PREBUILT, 0>(C, wsrc, bsrc, blen, status);
 }
 
-// lane quadrant / column-half of the calling warp (8 warps: 4 quadrants x 2)
+// lane quadrant of the calling warp and its index among the warps of that
+// quadrant (12 warps: 4 quadrants x 3)
 struct Lane {
-  int quad, half, r;
+  int quad, sub, r;     // lane quadrant, warp index within it, TMEM lane
   __device__ Lane() {
     const int w = threadIdx.x >> 5;
     quad = w & 3;
-    half = w >> 2;
+    sub = w >> 2;
     r = 32 * quad + (threadIdx.x & 31);
   }
 };
 
-// Column chunks [c0, c1) of an accumulator, warp half h taking chunks
-// c0 + h, c0 + h + 2, ...: visit(c, v, 0) gets chunk c's 32 values (one
+// Column chunks [c0, c1) of an accumulator, the quadrant's warp h taking
+// chunks c0 + h, c0 + h + WARPS_PER_QUAD, ...: visit(c, v, 0) gets chunk c's 32 values (one
 // load and wait per chunk; batching two chunks per wait raised the register
 // pressure of the fused step and ran slower).
 template <typename Visit>
-__device__ __forceinline__ void for_chunks(uint32_t lanebase, int half, int c0, int c1,
+__device__ __forceinline__ void for_chunks(uint32_t lanebase, int sub, int c0, int c1,
                                            Visit&& visit) {
-  for (int c = c0 + half; c < c1; c += 2) {
+  for (int c = c0 + sub; c < c1; c += WARPS_PER_QUAD) {
     float v[32];
     tmem_ld32(lanebase + (uint32_t)(32 * c), v);
     visit(c, v, 0);
@@ -619,8 +624,8 @@ __device__ __forceinline__ float gather_conv(Ctx& C, const Lane& ln, float* X) {
   float mloc = 0.f;
   for (int round = 0; round < 3; ++round) {
     if (upper && round < 2) {
-      if (round == 0 && ln.half == 0) X[pidx(ln.r - 64)] = 0.f;   // k < 64: one cell only
-      for_chunks(lanebase, ln.half, round == 0 ? 0 : mid, round == 0 ? mid : nch,
+      if (round == 0 && ln.sub == 0) X[pidx(ln.r - 64)] = 0.f;   // k < 64: one cell only
+      for_chunks(lanebase, ln.sub, round == 0 ? 0 : mid, round == 0 ? mid : nch,
                  [&](int c, const float (&v)[32], int o) {
 #pragma unroll
                    for (int t = 0; t < 32; ++t) {
@@ -630,7 +635,7 @@ __device__ __forceinline__ float gather_conv(Ctx& C, const Lane& ln, float* X) {
                  });
     }
     if (!upper && round > 0) {
-      for_chunks(lanebase, ln.half, round == 1 ? 0 : mid, round == 1 ? mid : nch,
+      for_chunks(lanebase, ln.sub, round == 1 ? 0 : mid, round == 1 ? mid : nch,
                  [&](int c, const float (&v)[32], int o) {
 #pragma unroll
                    for (int t = 0; t < 32; ++t) {
@@ -659,7 +664,7 @@ __device__ __forceinline__ void gather_corr(Ctx& C, const Lane& ln, float* Y) {
   const bool upper = ln.quad >= 2;
   for (int round = 0; round < 3; ++round) {
     if (upper && round < 2) {
-      for_chunks(lanebase, ln.half, round == 0 ? mid : 0, round == 0 ? nch : mid,
+      for_chunks(lanebase, ln.sub, round == 0 ? mid : 0, round == 0 ? nch : mid,
                  [&](int c, const float (&v)[32], int o) {
 #pragma unroll
                    for (int t = 0; t < 32; ++t) {
@@ -669,7 +674,7 @@ __device__ __forceinline__ void gather_corr(Ctx& C, const Lane& ln, float* Y) {
                  });
     }
     if (!upper && round > 0) {
-      for_chunks(lanebase, ln.half, round == 1 ? mid : 0, round == 1 ? nch : mid,
+      for_chunks(lanebase, ln.sub, round == 1 ? mid : 0, round == 1 ? nch : mid,
                  [&](int c, const float (&v)[32], int o) {
 #pragma unroll
                    for (int t = 0; t < 32; ++t) {

@@ -178,7 +178,8 @@ def test_frank_wolfe_tc_improves_like_simt(cuda):
 def test_tc_largest_n(cuda):
     """The top of the single-CTA range (n = 9728: 152 blocks, 512 TMEM
     columns, all shared memory) runs every tensor-core kernel; one cell more
-    is refused with SIDON_ERR_N."""
+    is refused with SIDON_ERR_SMEM (its plan exceeds the shared-memory
+    opt-in, as the SIMT kernels report), and the size query agrees."""
     from sidon_b200 import synth, _lib
     n = 9728
     a = T(synth.population("structured", n, 2, seed=97), cuda)
@@ -196,7 +197,8 @@ def test_tc_largest_n(cuda):
     big = torch.full((1, n + 1), 1.0 / (n + 1), device=cuda)
     with pytest.raises(_lib.SidonError) as ei:
         K().run_local_search(big, 1, 2.0, 4.0, 1e-3, 1e-3, precision="bf16x3")
-    assert ei.value.status == _lib.ERR_N
+    assert ei.value.status == _lib.ERR_SMEM
+    assert K().max_n(_lib.OP_LOCAL_SEARCH_TC) == n
 
 
 @pytest.mark.parametrize("iters", [1, 7, 30])
