@@ -905,12 +905,14 @@ def search_arm(args) -> None:
     ladder 64 ... 2048, 256 candidates in 8 islands, 2 elites, warm / cold
     4000 / 20000 steps, p up to 20000, 6 Frank-Wolfe rounds of 500 iterations,
     40000-step fp64 polish of 8 starts) for --search-seconds of wall clock,
-    through sidon_search (BF16x3 local search, fp32 Frank-Wolfe as the
-    reference).  Prints the certified F reached (lower is better)."""
+    through sidon_search (BF16x3 local search; the Frank-Wolfe step in fp32
+    as the reference, or --fw-precision).  Prints the certified F reached
+    (lower is better)."""
     import torch
     ws, rank, local = _dist()
     if rank != 0:
         return
+    fw = args.fw_precision or "fp32"
     torch.cuda.set_device(local)
     import sidon_b200
     sidon_b200.load(build=not (ROOT / "sidon-autocorrelation-bound_b200" / "libsidon_b200.so").exists())
@@ -920,7 +922,7 @@ def search_arm(args) -> None:
     best, F = kernels.search(ladder=SEARCH_LADDER, P=256, seconds=args.search_seconds,
                              gens_per_graph=2, polish_iters=40000, polish_top=8,
                              gen=kernels.generation_config(precision=args.precision,
-                                                           fw_precision="fp32",
+                                                           fw_precision=fw,
                                                            seed=20260905),
                              progress=lambda d, b: gens.append((d["n"], d["gen"])))
     wall = time.perf_counter() - t0
@@ -936,7 +938,7 @@ def search_arm(args) -> None:
         "seconds": wall, "n": int(best.size), "generations_per_level": per_level,
         "config": {"workload": f"whole search, reference defaults, {args.search_seconds:.0f} s "
                                f"budget, ladder {list(SEARCH_LADDER)}",
-                   "precision": args.precision, "fw_precision": "fp32"},
+                   "precision": args.precision, "fw_precision": fw},
     }))
 
 
@@ -1145,10 +1147,13 @@ def main() -> None:
     ap.add_argument("--anneal-steps", type=int, default=5000)
     ap.add_argument("--fw-every", type=int, default=250)
     ap.add_argument("--pdhg-iters", type=int, default=200)
-    ap.add_argument("--fw-precision", default="bf16x3", choices=["fp32", "bf16x3", "bf16x1"])
+    ap.add_argument("--fw-precision", default=None, choices=["fp32", "bf16x3", "bf16x1"],
+                    help="Frank-Wolfe arithmetic (default: bf16x3; fp32 for --workload search)")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.fw_precision is None and args.workload != "search":
+        args.fw_precision = "bf16x3"
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
