@@ -46,9 +46,9 @@
 //  BF16x1 keeps A_hi B_hi.  fp32 accumulation in TMEM.
 //
 //  Pipeline: one MMA warp (one elected lane issues every MMA) and builder
-//  warps; a ring of stages holding the windows of one to five tiles each, and one copy
-//  slot per phase, each guarded by a full barrier (builder arrivals) and an
-//  empty barrier (tcgen05.commit).  A stage release costs the tensor pipe
+//  warps; a ring of stages holding the windows of one to five tiles each,
+//  and one copy slot per phase, each guarded by a full barrier (builder
+//  arrivals) and an empty barrier (tcgen05.commit).  A stage release costs the tensor pipe
 //  far more than an MMA (fitted from phase timers at n = 8400: ~870 cycles
 //  per commit against ~70 per M128 N144 K16 instruction), so long tile
 //  sequences run two stages of two to five tiles -- one commit per stage --
@@ -475,7 +475,7 @@ __device__ __forceinline__ void issue_tile(Ctx& C, int st, int ts, int h, uint32
 //   wsrc: padded shared heights (windows; the copy too for CONV_SYM);
 //   bsrc / blen: the copy source of CONV_X (see build_conv_copy) or the
 //   padded shared weights of CORR.
-//   WPS: windows per stage fixed at compile time (1: three single-window
+//   WPS: tiles per stage fixed at compile time (1: three single-tile
 //   stages), or 0 to take the ring shape from C.wps / C.nst.
 template <int MODE, bool PREBUILT, int WPS>
 __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const float* bsrc,
@@ -568,13 +568,12 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
   return ok && !*((volatile int*)C.abort);
 }
 
-// The tile sequence on the CTA's ring (ring_for).  Three single-window
+// The tile sequence on the CTA's ring (ring_for).  Three single-tile
 // stages run a specialisation with the shape fixed at compile time, the
-// multi-window shapes one that reads it.  Measured per step against the
-// single-window ring alone: the same within 1% at n <= 1024 and n = 9728
-// (where the ring stays single-window; reading the shape there cost 2-4%),
-// 3% / 7% / 9% faster at n = 2048 / 4096 / 8400; specialising the 2 x 2 and
-// 2 x 3 shapes as well measured 1-8% slower than reading them.
+// multi-tile shapes one that reads it.  Measured per step: reading the shape
+// for the single-tile ring cost 2-4% (n <= 1024 and n = 9728 keep that
+// ring); specialising the multi-tile shapes as well measured 1-8% slower
+// than reading them (a larger kernel).
 template <int MODE, bool PREBUILT = false>
 __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float* bsrc, int blen,
                                           unsigned int* status) {
