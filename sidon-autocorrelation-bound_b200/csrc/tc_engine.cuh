@@ -229,7 +229,7 @@ struct Ctx {
   // the copy slots; done_ph = parity of the next bar_done wait
   uint32_t ph, started, bc_ph, bc_started, done_ph;
   int st_next;             // next stage in the ring
-  int nst, wps;            // ring shape: stages, windows per stage
+  int nst, wps;            // ring shape: stages, tiles per stage
   int* abort;              // shared abort flag
   int m, rc, rcc, n, dmax; // blocks, conv / corr copy rows, cells, last tile
   bool three;              // BF16x3 (else BF16x1)
