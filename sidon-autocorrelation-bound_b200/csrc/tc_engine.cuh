@@ -608,47 +608,74 @@ __device__ __forceinline__ void for_chunks(uint32_t lanebase, int sub, int c0, i
 }
 
 // b = a * a into X (padded layout, k < 2n-1).  Each k is the sum of two
-// cells, (k mod 64, k / 64) in lanes 0-63 and (k mod 64 + 64, k / 64 - 1) in
-// lanes 64-127, read by different warps: the upper lanes write their cells to
-// X, the lower lanes add theirs.  Three rounds overlap the two: the upper
-// lanes write the first half of the columns, then the second half while the
-// lower lanes finish the first, then the lower lanes finish the second.
+// cells, L = (k mod 64, k / 64) in lanes 0-63 and U = (k mod 64 + 64,
+// k / 64 - 1) in lanes 64-127, read by different warps: one writes its cell
+// to X, then the other adds its own.  Two rounds keep every warp busy: for
+// the k whose lower cell lies in the first half of the column chunks the
+// upper lanes write first (round 1) and the lower lanes add (round 2), for
+// the rest the lower lanes write first and the upper lanes add; the chunk
+// holding the boundary column's upper cell is read in both rounds.  b_k is
+// U + L either way (a sum of two floats does not depend on their order).
+// (Measured: the three rounds of the earlier form took about as long each
+// with four warps as with eight -- the per-chunk TMEM load is the latency.)
 // Ends synchronised.  Returns the largest b_k the calling thread finalised
 // (every k is finalised by exactly one thread).
 __device__ __forceinline__ float gather_conv(Ctx& C, const Lane& ln, float* X) {
   const int nb = 2 * C.n - 1, nch = (2 * C.m + 1 + 31) / 32;
-  const int mid = (nch + 1) / 2;                        // first half: chunks [0, mid)
+  const int mid = (nch + 1) / 2;                        // lower chunks [0, mid): upper first
+  const int cmid = 32 * mid;                            // first lower column of the rest
   const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)COL_CONV;
   const bool upper = ln.quad >= 2;
   float mloc = 0.f;
-  for (int round = 0; round < 3; ++round) {
-    if (upper && round < 2) {
-      if (round == 0 && ln.sub == 0) X[pidx(ln.r - 64)] = 0.f;   // k < 64: one cell only
-      for_chunks(lanebase, ln.sub, round == 0 ? 0 : mid, round == 0 ? mid : nch,
-                 [&](int c, const float (&v)[32], int o) {
+  // round 1: the first cell of every k (cell (r, col): k = 64 col + r)
+  if (upper) {
+    if (ln.sub == 0) X[pidx(ln.r - 64)] = 0.f;          // k < 64: one cell only
+    for_chunks(lanebase, ln.sub, 0, mid, [&](int c, const float (&v)[32], int o) {
 #pragma unroll
-                   for (int t = 0; t < 32; ++t) {
-                     const int k = 64 * (32 * c + t) + ln.r;   // cell (r, col): k = 64 col + r
-                     if (k < nb) X[pidx(k)] = v[o + t];
-                   }
-                 });
-    }
-    if (!upper && round > 0) {
-      for_chunks(lanebase, ln.sub, round == 1 ? 0 : mid, round == 1 ? mid : nch,
-                 [&](int c, const float (&v)[32], int o) {
+      for (int t = 0; t < 32; ++t) {
+        const int col = 32 * c + t, k = 64 * col + ln.r;
+        if (col + 1 < cmid && k < nb) X[pidx(k)] = v[o + t];
+      }
+    });
+  } else {
+    for_chunks(lanebase, ln.sub, mid, nch, [&](int c, const float (&v)[32], int o) {
 #pragma unroll
-                   for (int t = 0; t < 32; ++t) {
-                     const int k = 64 * (32 * c + t) + ln.r;
-                     if (k < nb) {
-                       const float b = X[pidx(k)] + v[o + t];
-                       X[pidx(k)] = b;
-                       mloc = fmaxf(mloc, b);
-                     }
-                   }
-                 });
-    }
-    __syncthreads();
+      for (int t = 0; t < 32; ++t) {
+        const int k = 64 * (32 * c + t) + ln.r;
+        if (k < nb) X[pidx(k)] = v[o + t];
+      }
+    });
   }
+  __syncthreads();
+  // round 2: the second cell, added; its thread finalises b_k (the upper
+  // lanes have none to add when every k lies below 64 cmid)
+  if (upper) {
+    if (64 * cmid < nb)
+      for_chunks(lanebase, ln.sub, mid - 1, nch, [&](int c, const float (&v)[32], int o) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+          const int col = 32 * c + t, k = 64 * col + ln.r;
+          if (col + 1 >= cmid && k < nb) {
+            const float b = X[pidx(k)] + v[o + t];
+            X[pidx(k)] = b;
+            mloc = fmaxf(mloc, b);
+          }
+        }
+      });
+  } else {
+    for_chunks(lanebase, ln.sub, 0, mid, [&](int c, const float (&v)[32], int o) {
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const int k = 64 * (32 * c + t) + ln.r;
+        if (k < nb) {
+          const float b = X[pidx(k)] + v[o + t];
+          X[pidx(k)] = b;
+          mloc = fmaxf(mloc, b);
+        }
+      }
+    });
+  }
+  __syncthreads();
   return mloc;
 }
 
