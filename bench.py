@@ -132,7 +132,23 @@ def _config(prec: str, ws: int) -> dict:
 
 
 # --------------------------------- reference arm ---------------------------
+def _ref_batch_call(probe, pop: np.ndarray, iters: int) -> float:
+    """One call of the reference CPU twin over the whole batch: `iters` Adam
+    steps of every candidate (OpenMP over candidates, probe.cpp:239), p and lr
+    along the benchmark's schedule.  Returns its wall time in seconds."""
+    x = np.ascontiguousarray(pop.copy())
+    t0 = time.perf_counter()
+    probe.ref_probe_local_search_batch(x.ctypes.data, N_CELLS, x.shape[0], int(iters),
+                                       ANNEAL["p_start"], ANNEAL["p_end"], ANNEAL["lr_start"],
+                                       ANNEAL["lr_end"], 0.9, 0.999, 0, None)
+    return time.perf_counter() - t0
+
+
 def reference_arm(args) -> None:
+    """The reference's CPU implementation of the path (tools/probe.cpp
+    localSearch, fp64) on the whole workload: the same 256 candidates, W
+    warm-up steps in one call, then the K timed steps in one call (each call
+    anneals p over its own steps, as the GPU arm's launch does)."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
@@ -145,22 +161,10 @@ def reference_arm(args) -> None:
     from sidon_b200 import synth
     probe = oracle.ref_probe()
     threads = probe.ref_probe_threads()
-    sample_c = max(2, 2 * threads)          # candidates per timed step (bounded sample)
-    iters = 4                               # Adam steps per candidate per call
-    pop = synth.population("lognormal", N_CELLS, sample_c, seed=8400, dtype=np.float64)
-
-    def one():
-        x = np.ascontiguousarray(pop.copy())
-        t0 = time.perf_counter()
-        probe.ref_probe_local_search_batch(x.ctypes.data, N_CELLS, sample_c, iters, 2.0, 1024.0,
-                                           1e-3, 1e-3, 0.9, 0.999, 0, None)
-        return time.perf_counter() - t0
-
-    for _ in range(max(1, min(args.warmup, 1))):
-        one()
-    times = [one() for _ in range(args.steps)]
-    cand_steps_s = sample_c * iters * len(times) / sum(times)
-    v = cand_steps_s / BATCH                # batched (256-candidate) steps per second
+    pop = synth.population("lognormal", N_CELLS, BATCH, seed=8400, dtype=np.float64)
+    _ref_batch_call(probe, pop, max(1, args.warmup))
+    t = _ref_batch_call(probe, pop, args.steps)
+    v = args.steps / t                      # batched (256-candidate) steps per second
     line = {
         "impl": "reference", "metric": "lp_adam_batched_steps_per_s", "value": v,
         "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -168,17 +172,28 @@ def reference_arm(args) -> None:
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": _config(args.precision, args.gpus),
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "reference",
-                         "sample": f"tools/probe.cpp localSearch (fp64 CPU twin), {sample_c} "
-                                   f"candidates x {iters} steps per timed step, OpenMP over "
-                                   f"candidates; each call adds one final objective "
-                                   f"(~1/4 step); scaled to {BATCH}-candidate steps"},
+                         "sample": f"tools/probe.cpp localSearch (fp64 CPU twin) on all {BATCH} "
+                                   f"candidates x {args.steps} steps in one call, OpenMP over "
+                                   f"candidates on {threads} threads ({_cpu_model()}); the call "
+                                   f"adds one final objective per candidate (1/(2K) of a step)"},
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
+def _cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown CPU"
+
+
 def cpu_baseline(budget_s: float = 10.0) -> dict:
-    """The reference CPU twin on this host's cores (bounded sample)."""
+    """The reference CPU twin on this host's cores: whole 256-candidate steps,
+    as many as fit the budget (one step first to size the call)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
     from sidon_b200 import synth
@@ -187,22 +202,14 @@ def cpu_baseline(budget_s: float = 10.0) -> dict:
                 "sample": "unavailable: oracle/_ref not built"}
     probe = oracle.ref_probe()
     threads = probe.ref_probe_threads()
-    c = max(2, threads)
-    iters = 4
-    pop = synth.population("lognormal", N_CELLS, c, seed=8400, dtype=np.float64)
-    done, t = 0, 0.0
-    while t < budget_s:
-        x = np.ascontiguousarray(pop.copy())
-        t0 = time.perf_counter()
-        probe.ref_probe_local_search_batch(x.ctypes.data, N_CELLS, c, iters, 2.0, 1024.0, 1e-3,
-                                           1e-3, 0.9, 0.999, 0, None)
-        t += time.perf_counter() - t0
-        done += c * iters
-    v = done / t / BATCH
-    return {"value": v, "unit": "steps/s", "cores": threads, "kind": "reference",
-            "sample": f"tools/probe.cpp localSearch fp64 twin, n={N_CELLS}, {c} candidates x "
-                      f"{iters} steps per call, {done} candidate-steps in {t:.1f}s on {threads} "
-                      f"threads, scaled to {BATCH}-candidate steps"}
+    pop = synth.population("lognormal", N_CELLS, BATCH, seed=8400, dtype=np.float64)
+    t1 = _ref_batch_call(probe, pop, 1)
+    iters = max(1, int(budget_s / max(t1, 1e-3)))
+    t = _ref_batch_call(probe, pop, iters)
+    return {"value": iters / t, "unit": "steps/s", "cores": threads, "kind": "reference",
+            "sample": f"tools/probe.cpp localSearch fp64 twin, n={N_CELLS}, all {BATCH} "
+                      f"candidates x {iters} steps in one call ({t:.1f}s on {threads} threads, "
+                      f"{_cpu_model()})"}
 
 
 # ----------------------------------- our arm -------------------------------
@@ -224,10 +231,13 @@ def our_arm(args) -> None:
     pop = torch.as_tensor(host, device=dev)
     mom = torch.empty_like(pop)
     vel = torch.empty_like(pop)
+    # flag words of the balanced-segment launch (None where the call needs none)
+    wsp = kernels.local_search_workspace(N_CELLS, BATCH, prec, dev)
     stream = torch.cuda.current_stream()
 
     def run(x, iters):
-        kernels.run_local_search(x, iters, mom=mom, vel=vel, precision=prec, **ANNEAL)
+        kernels.run_local_search(x, iters, mom=mom, vel=vel, precision=prec, workspace=wsp,
+                                 **ANNEAL)
 
     def barrier():
         if ws > 1:
@@ -270,12 +280,19 @@ def our_arm(args) -> None:
         pop.copy_(torch.as_tensor(host, device=dev))
         run(pop, args.steps)
 
-    # search-time F (the step's own arithmetic) error vs fp64 on the final population
+    # F error vs fp64 (hostF-identical certifying evaluation) on the final
+    # population: the reported search-time objective (max b refined in fp64
+    # over the near-maximal k, sum in fp64) and the raw step arithmetic (max
+    # of the b the step itself forms, fp32 sum of the heights)
     Fcert, _ = kernels.run_eval(pop, with_nactive=False)
-    _, saved, _ = kernels.lp_forward(pop, 2.0, precision=prec)
+    _, saved, b_step = kernels.lp_forward(pop, 2.0, store_b=True, precision=prec)
     S = saved[:, 1].double()
     F32 = 2.0 * N_CELLS * saved[:, 0].double() / (S * S)
     f_rel = (F32 - Fcert).abs().div(Fcert).max().item()
+    S_raw = pop.sum(dim=1, dtype=torch.float32).double()
+    F_raw = 2.0 * N_CELLS * b_step.max(dim=1).values.double() / (S_raw * S_raw)
+    f_rel_raw = (F_raw - Fcert).abs().div(Fcert).max().item()
+    del b_step
 
     # end-to-end through the public call with host buffers: every step copies
     # its population in from pinned host memory, runs one step and copies the
@@ -303,7 +320,7 @@ def our_arm(args) -> None:
             ev_in.record(s_in)
             s_cp.wait_event(ev_in)
             kernels.run_local_search(xs[b], 1, mom=mom, vel=vel, precision=prec, stream=s_cp,
-                                     **ANNEAL)
+                                     workspace=wsp, **ANNEAL)
             ev_cp[b] = torch.cuda.Event()
             ev_cp[b].record(s_cp)
             s_out.wait_event(ev_cp[b])
@@ -362,6 +379,7 @@ def our_arm(args) -> None:
             "speedup_vs_fp32_simt": (value / ws) / simt if simt else None,
             "f_evals_per_s": value * BATCH,
             "f_rel_err_vs_fp64": f_rel,
+            "f_rel_err_vs_fp64_raw_step": f_rel_raw,
             "roofline": roof,
             "clocks": {"sm_mhz": ck["sm_mhz"], "sm_max_mhz": ck["sm_max_mhz"],
                        "reasons": ck["reasons"]},

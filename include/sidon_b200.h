@@ -75,6 +75,18 @@ SIDON_API int sidon_last_cuda_error(void);
 SIDON_API int sidon_device_status(int reset);
 /* ABI version of this library (bumped on any signature change). */
 SIDON_API int sidon_abi_version(void);
+/* Diagnostic: the clock-cycle limit after which every bounded device-side
+ * wait of the tensor-core kernels gives up (default 2^31 cycles, about 1.1 s
+ * at 1.965 GHz; cycles <= 0 restores it).  A wait that runs out records
+ * SIDON_ERR_TIMEOUT in the status word (sidon_device_status), and the kernel
+ * unwinds: it still waits (with the default limit) for the tensor-core
+ * operations it already issued, releases its tensor memory and returns, so
+ * the context stays usable.  A tiny limit makes the pipeline's own waits run
+ * out; tests use it to exercise that path.  Synchronous; applies to later
+ * launches on the current device.
+ * No reference counterpart: the reference's kernels have no waits, and its
+ * CUDA_OK macro exits the process on any error (src/kernels.cuh:20-28). */
+SIDON_API int sidon_set_wait_limit(long long cycles);
 
 /* Dynamic shared memory one CTA of `op` needs at size n and dtype, in bytes;
  * 0 if the combination is unsupported.
@@ -119,6 +131,10 @@ SIDON_API int sidon_certify(const void* pop, int dtype, int n, int P, double* ou
  * overrides mode_default per candidate.  mom/vel: device [P][n] scratch of
  * dtype, zeroed at entry as in the reference.  dtype SIDON_F32 with
  * precision FP32_SIMT / BF16X1 / BF16X3, or SIDON_F64 with FP64_SIMT.
+ * One CTA per candidate, as in the reference: a batch of more candidates
+ * than SMs runs in waves (sidon_local_search_ws balances them).  Uses no
+ * library-global memory besides the status word, so calls on different
+ * streams may overlap freely.
  * Replaces kLocalSearch<T> + runLocalSearch (src/kernels.cuh:177-289,
  * src/main.cu:152-159) and the fp64 polish launch (src/main.cu:837-839). */
 SIDON_API int sidon_local_search(void* pop, void* mom, void* vel, const int* skip, const int* mode_arr,
@@ -126,20 +142,45 @@ SIDON_API int sidon_local_search(void* pop, void* mom, void* vel, const int* ski
                        double lr_end, double beta1, double beta2, int mode_default, int dtype,
                        int precision, void* stream);
 
+/* Workspace sidon_local_search_ws needs (bytes; 0 when the call needs none:
+ * fp32 SIMT, fp64, or arguments out of range). */
+SIDON_API size_t sidon_local_search_workspace_bytes(int n, int P, int dtype, int precision);
+/* sidon_local_search with a caller workspace (device memory, 4-byte
+ * aligned, >= sidon_local_search_workspace_bytes): a uniform BF16X1 / BF16X3
+ * batch of more candidates than SMs then runs as balanced step segments
+ * instead of waves -- the P chains of `iters` steps are laid end to end and
+ * cut into one equal segment per SM, a candidate split between two CTAs
+ * handing its heights and moments over through memory behind a flag word in
+ * the workspace (zeroed on the stream before the launch).  Every candidate's
+ * result equals sidon_local_search's bit for bit.  Calls that overlap on the
+ * GPU need distinct workspaces.  The launch is cooperative (all CTAs
+ * resident), and a stream capture records it as a cooperative kernel node.
+ * Same counterpart as sidon_local_search. */
+SIDON_API int sidon_local_search_ws(void* pop, void* mom, void* vel, const int* skip,
+                                    const int* mode_arr, int n, int P, int iters, double p_start,
+                                    double p_end, double lr_start, double lr_end, double beta1,
+                                    double beta2, int mode_default, int dtype, int precision,
+                                    void* workspace, size_t workspace_bytes, void* stream);
+
 /* The fused local search of sidon_local_search for callers that cannot
  * allocate device memory -- e.g. a plugin inside an application whose
  * allocator owns every device byte, or a hot path that must never call
  * cudaMalloc/cudaFree because they can synchronise the device.  Such a caller
  * passes only its population (fp32, [P][n], in place, plus the optional skip
- * and mode_arr); the Adam moments live in a fixed 8 MiB device array inside
- * the library, held by every GPU that loads it until the process exits.
+ * and mode_arr); the Adam moments, and the hand-over flags of a BF16 batch
+ * of more candidates than SMs (run as sidon_local_search_ws runs it), live
+ * in a fixed device array inside the library (8 MiB + 256 KiB), held by
+ * every GPU that loads it until the process exits.
  * Limit: P * n <= 1048576 cells per call, else SIDON_ERR_CAPACITY.  precision:
  * FP32_SIMT, BF16X1 or BF16X3.  Nothing is allocated: the first call on a
  * device (with that device current) looks up the array's device address with
  * cudaGetSymbolAddress and caches it, so make that first call before any
- * stream capture.  All calls share the one array: the kernels zero a
- * candidate's moments before using them, and calls that overlap on the GPU
- * (concurrent streams) race on it.
+ * stream capture, and do not use this entry point after a cudaDeviceReset
+ * (the cached address belongs to the context that reset destroyed).  All
+ * calls share the one array: the kernels zero a candidate's moments before
+ * using them and the flags are zeroed on the stream before each launch, but
+ * calls that overlap on the GPU (concurrent streams) race on both.  The
+ * array is private to this entry point: no other call touches it.
  * No counterpart in the reference (its driver always allocates the moment
  * buffers, src/main.cu:118-137). */
 SIDON_API int sidon_local_search_noalloc(float* pop, const int* skip, const int* mode_arr, int n,
@@ -285,6 +326,40 @@ SIDON_API size_t sidon_large_workspace_bytes(int n, int P, int q, int precision)
 SIDON_API int sidon_autotune_large(int n, int P, int precision, int* out_q,
                                    float* out_ms_per_step);
 
+/* The fused local search's schedule for a uniform batch: choices that never
+ * change a result bit, only the time.
+ *   lane_tile    fp32 SIMT: outputs per lane (odd, 7..15; a narrower tile
+ *                spreads small n over more warps);
+ *   ring_tiles   tensor cores: tiles per stage of the window ring (1 = three
+ *                single-tile stages, 2..5 = two stages of that many tiles);
+ *   balanced     tensor cores, more candidates than SMs: balanced step
+ *                segments (1, when the call has a workspace) or waves of one
+ *                CTA per candidate (0);
+ *   ms_per_step  the tuner's measurement (0 when not tuned);
+ *   tuned        1 if the tuner chose it, 0 for the built-in default. */
+typedef struct sidon_ls_schedule {
+  int lane_tile;
+  int ring_tiles;
+  int balanced;
+  float ms_per_step;
+  int tuned;
+} sidon_ls_schedule;
+
+/* The schedule tuner of the fused local search: times a short anneal of P
+ * uniform candidates of n cells under every schedule above (lane tiles for
+ * FP32_SIMT; ring shapes and, for P > SMs, segments vs waves for BF16X1 /
+ * BF16X3) and remembers the fastest for (device, n, P, precision); later
+ * uniform calls (sidon_local_search, _ws, _noalloc, the anneal) then use it.
+ * Results are unchanged bit for bit.  It allocates scratch with cudaMalloc
+ * and synchronises: call it before any stream capture.
+ * Replaces the reference's fixed tiling constants TK / TI
+ * (src/kernels.cuh:30-33). */
+SIDON_API int sidon_autotune_local_search(int n, int P, int precision, sidon_ls_schedule* out);
+/* The schedule the next uniform call at (n, P, precision) will use: the
+ * tuned one if the tuner ran for it in this process, else the default
+ * (tuned = 0).  No reference counterpart. */
+SIDON_API int sidon_local_search_schedule(int n, int P, int precision, sidon_ls_schedule* out);
+
 /* sidon_local_search (fp32 [P][n], Adam moments in mom/vel) for any n. */
 SIDON_API int sidon_local_search_large(float* pop, float* mom, float* vel, const int* skip,
                                        const int* mode_arr, int n, int P, int iters,
@@ -392,7 +467,10 @@ typedef struct sidon_anneal_config {
 /* pop: fp32, ragged (offsets != NULL) or uniform [P][n_max] (offsets ==
  * NULL); mom/vel: scratch of pop's layout; fit: device double [P] (fp64 F
  * at the end); rank: device int [P] (island ranking scratch, required when
- * migrating); order: as for the ragged calls. */
+ * migrating; may be NULL otherwise; its contents on return are unspecified:
+ * between migrations it also holds the hand-over flags with which a uniform
+ * tensor-core batch of more candidates than SMs runs as balanced step
+ * segments, see sidon_local_search_ws); order: as for the ragged calls. */
 SIDON_API int sidon_anneal(float* pop, float* mom, float* vel, const long long* offsets,
                            const int* order, int n_max, int P, double* fit, int* rank,
                            const sidon_anneal_config* cfg, void* stream);

@@ -27,6 +27,7 @@ SIGNATURES = {
     "sidon_last_cuda_error": (_i, []),
     "sidon_abi_version": (_i, []),
     "sidon_device_status": (_i, [_i]),
+    "sidon_set_wait_limit": (_i, [C.c_longlong]),
     "sidon_smem_bytes": (_sz, [_i, _i, _i]),
     "sidon_max_n": (_i, [_i, _i]),
     "sidon_hostF": (_d, [_vp, _i]),
@@ -34,6 +35,9 @@ SIGNATURES = {
     "sidon_certify": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "sidon_local_search": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _d, _i,
                                 _i, _i, _vp]),
+    "sidon_local_search_workspace_bytes": (_sz, [_i, _i, _i, _i]),
+    "sidon_local_search_ws": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _d,
+                                   _i, _i, _i, _vp, _sz, _vp]),
     "sidon_local_search_noalloc": (_i, [_vp, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _d, _i, _i,
                                         _vp]),
     "sidon_lp_forward": (_i, [_vp, _i, _i, _d, _vp, _vp, _vp, _i, _vp]),
@@ -50,6 +54,8 @@ SIGNATURES = {
     "sidon_polish": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "sidon_large_workspace_bytes": (_sz, [_i, _i, _i, _i]),
     "sidon_autotune_large": (_i, [_i, _i, _i, _vp, _vp]),
+    "sidon_autotune_local_search": (_i, [_i, _i, _i, _vp]),
+    "sidon_local_search_schedule": (_i, [_i, _i, _i, _vp]),
     "sidon_local_search_large": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _d,
                                       _i, _i, _i, _vp, _sz, _vp]),
     "sidon_frank_wolfe_large": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _f, _f, _f, _i, _i, _vp, _sz,
@@ -80,6 +86,16 @@ SIGNATURES = {
     "sidon_seed_level": (_i, [_vp, _vp, _i, _i, _i, _vp, _i, C.c_ulonglong]),
     "sidon_search": (_i, [_vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _vp]),
 }
+
+
+class LsSchedule(C.Structure):
+    """struct sidon_ls_schedule."""
+
+    _fields_ = [("lane_tile", _i), ("ring_tiles", _i), ("balanced", _i), ("ms_per_step", _f),
+                ("tuned", _i)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class AnnealConfig(C.Structure):

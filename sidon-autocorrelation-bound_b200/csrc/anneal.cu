@@ -22,7 +22,7 @@ int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* 
                            const int* order, int P, int n_fixed, int n_max, const int* skip,
                            const int* mode_arr, int iters, double pS, double pE, double lrS,
                            double lrE, double b1, double b2, int mode_default, int precision,
-                           cudaStream_t st);
+                           unsigned int* seg_flags, cudaStream_t st);
 int launch_eval(const void* pop, int dtype, const long long* offsets, const int* order, int P,
                 int n_fixed, int n_max, double* outF, int* outN, double tol, cudaStream_t st);
 int launch_frank_wolfe(float* pop, const long long* offsets, const int* order, int P, int n_fixed,
@@ -111,7 +111,7 @@ int enqueue(const Args& a, cudaStream_t st) {
     if (tc)
       rc = launch_local_search_tc(a.pop, a.mom, a.vel, a.offsets, a.order, a.P, n_fixed, a.n_max,
                                   nullptr, nullptr, L, pA, pB, lA, lB, c.beta1, c.beta2, 0,
-                                  c.precision, st);
+                                  c.precision, a.offsets ? nullptr : (unsigned int*)a.rank, st);
     else
       rc = launch_local_search(a.pop, a.mom, a.vel, a.offsets, a.order, a.P, n_fixed, a.n_max,
                                nullptr, nullptr, L, pA, pB, lA, lB, c.beta1, c.beta2, 0,

@@ -573,7 +573,7 @@ int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* 
                            const int* order, int P, int n_fixed, int n_max, const int* skip,
                            const int* mode_arr, int iters, double pS, double pE, double lrS,
                            double lrE, double b1, double b2, int mode_default, int precision,
-                           cudaStream_t st);
+                           unsigned int* seg_flags, cudaStream_t st);
 bool fused_fits(int n);
 int tuned_q(int n, int P, int precision);
 
@@ -587,7 +587,7 @@ int launch_local_search_big(float* pop, float* mom, float* vel, const int* skip,
   if (Q <= 0) Q = big_default_q(n);
   if (Q >= n && fused_fits(n))
     return launch_local_search_tc(pop, mom, vel, nullptr, nullptr, P, n, n, skip, mode_arr, iters,
-                                  pS, pE, lrS, lrE, b1, b2, mode_default, precision, st);
+                                  pS, pE, lrS, lrE, b1, b2, mode_default, precision, nullptr, st);
   if (Q % 64) return SIDON_ERR_ARG;
   int rc = big_prep(Q);
   if (rc) return rc;

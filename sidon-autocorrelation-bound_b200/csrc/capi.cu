@@ -27,7 +27,7 @@ int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* 
                            const int* order, int P, int n_fixed, int n_max, const int* skip,
                            const int* mode_arr, int iters, double pS, double pE, double lrS,
                            double lrE, double b1, double b2, int mode_default, int precision,
-                           cudaStream_t st);
+                           unsigned int* seg_flags, cudaStream_t st);
 int launch_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
                       float* b_out, cudaStream_t st);
 int launch_lp_forward_tc(const float* a, int n, int P, double p, float* value, float* saved,
@@ -35,6 +35,7 @@ int launch_lp_forward_tc(const float* a, int n, int P, double p, float* value, f
 int launch_lp_backward_tc(const float* a, const float* saved, const float* b_in, int n, int P,
                           double p, float* grad, int precision, cudaStream_t st);
 int device_status(int reset);
+int set_wait_limit(long long cycles);
 int launch_lp_backward(const float* a, const float* saved, const float* b_in, int n, int P,
                        double p, float* grad, cudaStream_t st);
 int launch_eval(const void* pop, int dtype, const long long* offsets, const int* order, int P,
@@ -58,6 +59,9 @@ size_t big_workspace_bytes(int n, int P, int Q);
 int big_default_q(int n);
 int tuned_q(int n, int P, int precision);
 int autotune_local_search(int n, int P, int precision, int* out_q, float* out_ms);
+int autotune_ls_schedule(int n, int P, int precision, sidon_ls_schedule* out);
+int ls_schedule(int n, int P, int precision, sidon_ls_schedule* out);
+int tc_n_ok_public(int n);
 int launch_local_search_big(float* pop, float* mom, float* vel, const int* skip,
                             const int* mode_arr, int n, int P, int iters, double pS, double pE,
                             double lrS, double lrE, double b1, double b2, int mode_default,
@@ -182,6 +186,11 @@ int sidon_device_status(int reset) {
   if (rc) return rc;
   return device_status(reset);
 }
+int sidon_set_wait_limit(long long cycles) {
+  int rc = device_ok();
+  if (rc) return rc;
+  return set_wait_limit(cycles);
+}
 int sidon_abi_version(void) { return 1; }
 
 size_t sidon_smem_bytes(int op, int n, int dtype) {
@@ -267,7 +276,7 @@ int sidon_local_search(void* pop, void* mom, void* vel, const int* skip, const i
     if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
       return launch_local_search_tc((float*)pop, (float*)mom, (float*)vel, nullptr, nullptr, P,
                                     n, n, skip, mode_arr, iters, p_start, p_end, lr_start, lr_end,
-                                    beta1, beta2, mode_default, precision, S(stream));
+                                    beta1, beta2, mode_default, precision, nullptr, S(stream));
     return SIDON_ERR_DTYPE;
   }
   if (dtype == SIDON_F64 && precision == SIDON_PREC_FP64_SIMT)
@@ -275,6 +284,35 @@ int sidon_local_search(void* pop, void* mom, void* vel, const int* skip, const i
                                p_start, p_end, lr_start, lr_end, beta1, beta2, mode_default,
                                dtype, S(stream));
   return SIDON_ERR_DTYPE;
+}
+
+size_t sidon_local_search_workspace_bytes(int n, int P, int dtype, int precision) {
+  if (n < 1 || P < 1 || dtype != SIDON_F32) return 0;
+  if (precision != SIDON_PREC_BF16X1 && precision != SIDON_PREC_BF16X3) return 0;
+  return ((size_t)P * sizeof(unsigned int) + 255) / 256 * 256;
+}
+
+int sidon_local_search_ws(void* pop, void* mom, void* vel, const int* skip, const int* mode_arr,
+                          int n, int P, int iters, double p_start, double p_end, double lr_start,
+                          double lr_end, double beta1, double beta2, int mode_default, int dtype,
+                          int precision, void* workspace, size_t workspace_bytes, void* stream) {
+  const size_t need = sidon_local_search_workspace_bytes(n, P, dtype, precision);
+  if (need == 0)
+    return sidon_local_search(pop, mom, vel, skip, mode_arr, n, P, iters, p_start, p_end,
+                              lr_start, lr_end, beta1, beta2, mode_default, dtype, precision,
+                              stream);
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (iters <= 0) return SIDON_OK;
+  if (!pop || !mom || !vel) return SIDON_ERR_ARG;
+  if (!workspace || workspace_bytes < need || (reinterpret_cast<uintptr_t>(workspace) & 3))
+    return SIDON_ERR_ARG;
+  if (!(p_start > 0.0) || !(p_end > 0.0) || !(lr_start > 0.0) || !(lr_end > 0.0))
+    return SIDON_ERR_ARG;
+  return launch_local_search_tc((float*)pop, (float*)mom, (float*)vel, nullptr, nullptr, P, n, n,
+                                skip, mode_arr, iters, p_start, p_end, lr_start, lr_end, beta1,
+                                beta2, mode_default, precision, (unsigned int*)workspace,
+                                S(stream));
 }
 
 int sidon_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
@@ -386,6 +424,30 @@ int sidon_autotune_large(int n, int P, int precision, int* out_q, float* out_ms_
   return autotune_local_search(n, P, precision, out_q, out_ms_per_step);
 }
 
+int sidon_autotune_local_search(int n, int P, int precision, sidon_ls_schedule* out) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P < 1 || !out) return SIDON_ERR_ARG;
+  if (precision == SIDON_PREC_FP32_SIMT) {
+    if ((long long)smem_local_search(n, SIDON_F32) > smem_optin()) return SIDON_ERR_SMEM;
+  } else if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3) {
+    if (tc_n_ok_public(n)) return SIDON_ERR_N;
+  } else {
+    return SIDON_ERR_DTYPE;
+  }
+  return autotune_ls_schedule(n, P, precision, out);
+}
+
+int sidon_local_search_schedule(int n, int P, int precision, sidon_ls_schedule* out) {
+  int rc = pre(n, P);
+  if (rc) return rc;
+  if (P < 1 || !out) return SIDON_ERR_ARG;
+  if (precision != SIDON_PREC_FP32_SIMT && precision != SIDON_PREC_BF16X1 &&
+      precision != SIDON_PREC_BF16X3)
+    return SIDON_ERR_DTYPE;
+  return ls_schedule(n, P, precision, out);
+}
+
 int sidon_local_search_large(float* pop, float* mom, float* vel, const int* skip,
                              const int* mode_arr, int n, int P, int iters, double p_start,
                              double p_end, double lr_start, double lr_end, double beta1,
@@ -475,7 +537,7 @@ int sidon_local_search_ragged(float* pop, float* mom, float* vel, const long lon
   if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
     return launch_local_search_tc(pop, mom, vel, offsets, order, P, 0, n_max, skip, mode_arr,
                                   iters, p_start, p_end, lr_start, lr_end, beta1, beta2,
-                                  mode_default, precision, S(stream));
+                                  mode_default, precision, nullptr, S(stream));
   return SIDON_ERR_DTYPE;
 }
 

@@ -11,6 +11,7 @@
 // ---------------------------------------------------------------------------
 #pragma once
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "../../include/sidon_b200.h"
@@ -134,6 +135,21 @@ __device__ __forceinline__ Cand cand_of(int slot, const long long* __restrict__ 
 
 // round-up helper
 __host__ __device__ constexpr inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// The library's device-side state word (one per device): the first error a
+// kernel recorded (SIDON_ERR_TIMEOUT, SIDON_ERR_NONFINITE) and the clock-cycle
+// limit of every bounded wait.  Kernels receive the address of `status`; the
+// limit sits behind it in the same struct.
+constexpr long long kDefaultWaitCycles = 1ll << 31;   // ~1.1 s at 1.965 GHz
+struct DeviceState {
+  unsigned int status;
+  unsigned int reserved;
+  long long wait_cycles;
+};
+static_assert(offsetof(DeviceState, status) == 0, "kernels address the state by its status word");
+__device__ __forceinline__ long long wait_limit(const unsigned int* status) {
+  return reinterpret_cast<const DeviceState*>(status)->wait_cycles;
+}
 
 }  // namespace sidon
 

@@ -11,10 +11,13 @@
 //  caller cannot provide the [P][n] moment buffers sidon_local_search wants.
 //
 //  The moments live in g_moment_scratch below: a file-scope __device__ array
-//  of 2 x kMaxCells floats (8 MiB), which every GPU that loads the library
-//  holds until the process exits.  Host code cannot use the array's name as a
-//  device address, so on the first call on each device (with that device
-//  current) the address is looked up with cudaGetSymbolAddress and cached.
+//  of 2 x kMaxCells floats (8 MiB) followed by kMaxFlags words (256 KiB) for
+//  the hand-over flags of the balanced-segment kernel, which every GPU that
+//  loads the library holds until the process exits.  Host code cannot use
+//  the array's name as a device address, so on the first call on each device
+//  (with that device current) the address is looked up with
+//  cudaGetSymbolAddress and cached; that cache assumes the device's context
+//  lives as long as the library (do not call this after cudaDeviceReset).
 //  No call here allocates: no cudaMalloc, cudaFree or allocating library
 //  routine is used.
 // ---------------------------------------------------------------------------
@@ -32,16 +35,20 @@ int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* 
                            const int* order, int P, int n_fixed, int n_max, const int* skip,
                            const int* mode_arr, int iters, double pS, double pE, double lrS,
                            double lrE, double b1, double b2, int mode_default, int precision,
-                           cudaStream_t st);
+                           unsigned int* seg_flags, cudaStream_t st);
 }  // namespace sidon_host
 
 namespace {
 
 // P * n of one call may not exceed this (the first moment uses the first
-// half of the array, the second moment the second half).
+// kMaxCells floats of the array, the second moment the next kMaxCells).
 constexpr long long kMaxCells = 1ll << 20;
+// Batches of more candidates than SMs run as balanced step segments with one
+// hand-over flag per candidate in the array's last kMaxFlags words; larger
+// batches (P > kMaxFlags, i.e. n <= 16) run the one-CTA-per-candidate kernel.
+constexpr int kMaxFlags = 1 << 16;
 
-static __device__ __align__(256) float g_moment_scratch[2 * kMaxCells];
+static __device__ __align__(256) float g_moment_scratch[2 * kMaxCells + kMaxFlags];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
@@ -84,10 +91,14 @@ int sidon_local_search_noalloc(float* pop, const int* skip, const int* mode_arr,
   float* scratch = nullptr;
   rc = scratch_address(&scratch);
   if (rc) return rc;
-  // the kernels zero the moments of every candidate they run at entry, so
-  // whatever an earlier call left in the array never leaks into this one
+  // the kernels zero the moments of every candidate they run at entry, and
+  // the segment flags are zeroed on the stream before the launch, so what an
+  // earlier call left in the array never leaks into this one (calls that
+  // overlap on the GPU race on it all the same)
   float* mom = scratch;
   float* vel = scratch + kMaxCells;
+  unsigned int* flags =
+      P <= kMaxFlags ? reinterpret_cast<unsigned int*>(scratch + 2 * kMaxCells) : nullptr;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (precision == SIDON_PREC_FP32_SIMT)
     return sidon_host::launch_local_search(pop, mom, vel, nullptr, nullptr, P, n, n, skip,
@@ -96,7 +107,8 @@ int sidon_local_search_noalloc(float* pop, const int* skip, const int* mode_arr,
   if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
     return sidon_host::launch_local_search_tc(pop, mom, vel, nullptr, nullptr, P, n, n, skip,
                                               mode_arr, iters, p_start, p_end, lr_start, lr_end,
-                                              beta1, beta2, mode_default, precision, st);
+                                              beta1, beta2, mode_default, precision, flags,
+                                              st);
   return SIDON_ERR_DTYPE;
 }
 

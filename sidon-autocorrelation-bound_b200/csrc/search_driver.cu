@@ -38,6 +38,105 @@ void inject(const std::vector<double>& v, float* dst, int n) {
     for (int i = 0; i < n; ++i) dst[i] = (float)(dst[i] / S);
 }
 
+// ------------------------------ level seeding ------------------------------
+// A fresh row is one of two random families.  Its description is drawn
+// first, all at once, in the order the reference driver draws it (so level 0
+// reproduces the reference's first rows); the row is then rendered from the
+// description.
+struct FreshRow {
+  int nf = 0;                   // cosine terms (2..7)
+  double freq[8] = {}, phase[8] = {};
+  bool structured = false;      // the structured prior, else a smooth profile
+  // structured prior: segments of the unit interval with a level and a
+  // roughness amplitude each, an atom at one end
+  bool flip = false;
+  double atom = 0.0;
+  double edge[5] = {};          // right edges of segments 0..4
+  double level[6] = {4.2, 0.7, 5.2, 2.0, 0.0, 0.0};
+  double rough_amp[6] = {0.45, 0.80, 0.30, 0.70, 0.0, 0.20};
+  // smooth profile: base + amp * (mean of the cosines) + 0.3 N(0, 1)
+  double base = 0.0, amp = 0.0;
+};
+
+// The random streams of one level: one generator, and one normal
+// distribution for the whole level (it keeps the second value of each pair
+// it draws for the next call, so it must not restart per row).
+struct LevelDraws {
+  std::mt19937_64 rng;
+  std::uniform_real_distribution<double> U{0.0, 1.0};
+  std::normal_distribution<double> N{0.0, 1.0};
+  explicit LevelDraws(unsigned long long s) : rng(s) {}
+  double uniform() { return U(rng); }
+  double normal() { return N(rng); }
+};
+
+FreshRow draw_fresh(LevelDraws& g) {
+  FreshRow r;
+  r.nf = 2 + (int)(g.uniform() * 6);
+  for (int f = 0; f < r.nf; ++f) {
+    r.freq[f] = 1 + g.uniform() * 10;
+    r.phase[f] = g.uniform() * 6.283185307;
+  }
+  r.structured = g.uniform() < 0.6;
+  if (r.structured) {
+    r.flip = g.uniform() < 0.5;
+    r.atom = 30 + 250 * g.uniform();
+    r.edge[0] = 0.28 + 0.16 * g.uniform();                  // plateau
+    r.edge[1] = r.edge[0] + 0.10 + 0.14 * g.uniform();      // depression
+    r.edge[2] = r.edge[1] + 0.02 + 0.08 * g.uniform();      // hump
+    r.edge[3] = 0.70 + 0.16 * g.uniform();                  // ragged band
+    r.edge[4] = r.edge[3] + 0.05 + 0.15 * g.uniform();      // hard gap
+    r.level[5] = 3.0 + 14.0 * g.uniform();                  // terminal spike
+  } else {
+    r.base = 0.3 + 0.7 * g.uniform();
+    r.amp = 0.2 + 1.2 * g.uniform();
+  }
+  return r;
+}
+
+// Render a fresh row into dst (n cells, clipped at zero).  The smooth
+// family draws one normal per cell, in cell order.
+void render_fresh(const FreshRow& r, float* dst, int n, LevelDraws& g) {
+  for (int i = 0; i < n; ++i) {
+    double v;
+    if (r.structured) {
+      const int d = r.flip ? (n - 1 - i) : i;         // distance from the atom's end
+      const double x = (d + 0.5) / n;
+      double rough = 0;
+      for (int f = 0; f < r.nf; ++f)
+        rough += std::cos(6.283185307 * (2 + 6 * r.freq[f]) * x + r.phase[f]);
+      rough /= r.nf;
+      int s = 0;                                       // first segment whose edge lies past x
+      while (s < 5 && !(x < r.edge[s])) ++s;
+      v = s == 4 ? 0.0 : r.level[s] * (1 + r.rough_amp[s] * rough);
+      if (d == 0) v += r.atom;
+      else if (d < 4) v += r.atom * 0.10 / d;
+    } else {
+      double m = 0;
+      for (int f = 0; f < r.nf; ++f) m += std::cos(6.283185307 * r.freq[f] * i / n + r.phase[f]);
+      v = r.base + r.amp * m / r.nf + 0.3 * g.normal();
+    }
+    dst[i] = (float)std::max(0.0, v);
+  }
+}
+
+// The previous level's row carried to n cells: each cell duplicated when n
+// doubles, else the nearest-neighbour resample.
+void carry_over(const float* src, int n_prev, float* dst, int n) {
+  if (n == 2 * n_prev) {
+    for (int i = 0; i < n_prev; ++i) dst[2 * i] = dst[2 * i + 1] = src[i];
+    return;
+  }
+  for (int i = 0; i < n; ++i) dst[i] = src[std::min(n_prev - 1, (int)((long long)i * n_prev / n))];
+}
+
+// sum 1 in fp64 (cell order); the uniform row when the sum is not positive
+void normalise_row(float* dst, int n) {
+  double S = 0;
+  for (int i = 0; i < n; ++i) S += dst[i];
+  for (int i = 0; i < n; ++i) dst[i] = S <= 0 ? 1.f / n : (float)(dst[i] / S);
+}
+
 // device buffers of a search, freed on every exit path
 struct Buffers {
   void* ws = nullptr;
@@ -63,100 +162,31 @@ struct Buffers {
 extern "C" {
 
 // Seeding of a ladder level (main.cu:483-553): row p refines the previous
-// level's row p (duplicate when n = 2 n_prev, else nearest-neighbour
-// resample) and keeps it (seed_op 20), except that the last 20 % of the rows
-// start afresh; an empty row gets a fresh start (seed_op 9): with
-// probability 0.6 the structured prior (endpoint atom, plateau, depression,
-// hump, ragged band, hard gap, terminal spike), else a smooth random profile
-// with gaussian noise; every row is normalised to sum 1 (uniform when the
-// sum is not positive).  Draws: std::mt19937_64 seeded with seed + level,
-// through std::uniform_real_distribution / std::normal_distribution in the
-// reference's order (level 0 draws exactly the reference's first numbers;
-// later levels differ, because the reference's generator also serves its
-// host-side selection draws, which run on the device here).
+// level's row p and keeps it (seed_op 20), except that the last 20 % of the
+// rows start afresh; a row with no positive cell gets a fresh start (seed_op
+// 9) from draw_fresh / render_fresh: with probability 0.6 the structured
+// prior (endpoint atom, plateau, depression, hump, ragged band, hard gap,
+// terminal spike), else a smooth random profile with gaussian noise.  Every
+// row ends normalised to sum 1.  Draws: std::mt19937_64 seeded with
+// seed + level, in the reference's order (level 0 draws exactly the
+// reference's first numbers; later levels differ, because the reference's
+// generator also serves its host-side selection draws, which run on the
+// device here).
 int sidon_seed_level(float* pop, int* seed_op, int n, int P, int level, const float* prev,
                      int n_prev, unsigned long long seed) {
   if (!pop || !seed_op || P < 1 || level < 0) return SIDON_ERR_ARG;
   if (n < 1) return SIDON_ERR_N;
   if (prev && n_prev < 1) return SIDON_ERR_ARG;
-  std::mt19937_64 rng(seed + (unsigned long long)level);
-  std::uniform_real_distribution<double> U01(0.0, 1.0);
-  std::normal_distribution<double> N01(0.0, 1.0);
+  LevelDraws draws(seed + (unsigned long long)level);
+  const int keep = (level > 0 && prev) ? (int)(0.8 * P) : 0;   // carried-over rows
   for (int p = 0; p < P; ++p) {
     float* dst = pop + (size_t)p * n;
-    seed_op[p] = 9;
-    for (int i = 0; i < n; ++i) dst[i] = 0.f;
-    if (level > 0 && prev) {
-      const float* src = prev + (size_t)p * n_prev;
-      if (n == 2 * n_prev) {
-        for (int i = 0; i < n_prev; ++i) dst[2 * i] = dst[2 * i + 1] = src[i];
-      } else {
-        for (int i = 0; i < n; ++i)
-          dst[i] = src[std::min(n_prev - 1, (int)((long long)i * n_prev / n))];
-      }
-      if (p >= (int)(0.8 * P))
-        for (int i = 0; i < n; ++i) dst[i] = 0.f;
-      else
-        seed_op[p] = 20;
-    }
-    bool empty = true;
-    for (int i = 0; i < n; ++i)
-      if (dst[i] > 0.f) {
-        empty = false;
-        break;
-      }
-    if (empty) {
-      seed_op[p] = 9;
-      const int nf = 2 + (int)(U01(rng) * 6);
-      std::vector<double> fr(nf), ph(nf);
-      for (int f = 0; f < nf; ++f) {
-        fr[f] = 1 + U01(rng) * 10;
-        ph[f] = U01(rng) * 6.283185307;
-      }
-      if (U01(rng) < 0.6) {
-        const bool flip = U01(rng) < 0.5;
-        const double atom = 30 + 250 * U01(rng);
-        const double pl1 = 0.28 + 0.16 * U01(rng);
-        const double pl2 = pl1 + 0.10 + 0.14 * U01(rng);
-        const double hmp = pl2 + 0.02 + 0.08 * U01(rng);
-        const double gp0 = 0.70 + 0.16 * U01(rng);
-        const double gp1 = gp0 + 0.05 + 0.15 * U01(rng);
-        const double tail = 3.0 + 14.0 * U01(rng);
-        for (int i = 0; i < n; ++i) {
-          const int d = flip ? (n - 1 - i) : i;
-          const double x = (d + 0.5) / n;
-          double rough = 0;
-          for (int f = 0; f < nf; ++f) rough += std::cos(6.283185307 * (2 + 6 * fr[f]) * x + ph[f]);
-          rough /= nf;
-          double v;
-          if (x < pl1) v = 4.2 * (1 + 0.45 * rough);
-          else if (x < pl2) v = 0.7 * (1 + 0.80 * rough);
-          else if (x < hmp) v = 5.2 * (1 + 0.30 * rough);
-          else if (x < gp0) v = 2.0 * (1 + 0.70 * rough);
-          else if (x < gp1) v = 0.0;
-          else v = tail * (1 + 0.20 * rough);
-          if (d == 0) v += atom;
-          else if (d < 4) v += atom * 0.10 / d;
-          dst[i] = (float)std::max(0.0, v);
-        }
-      } else {
-        const double base = 0.3 + 0.7 * U01(rng);
-        const double amp = 0.2 + 1.2 * U01(rng);
-        for (int i = 0; i < n; ++i) {
-          double m = 0;
-          for (int f = 0; f < nf; ++f) m += std::cos(6.283185307 * fr[f] * i / n + ph[f]);
-          const double v = base + amp * m / nf + 0.3 * N01(rng);
-          dst[i] = (float)std::max(0.0, v);
-        }
-      }
-    }
-    double S = 0;
-    for (int i = 0; i < n; ++i) S += dst[i];
-    if (S <= 0) {
-      for (int i = 0; i < n; ++i) dst[i] = 1.f / n;
-    } else {
-      for (int i = 0; i < n; ++i) dst[i] = (float)(dst[i] / S);
-    }
+    std::fill(dst, dst + n, 0.f);
+    if (p < keep) carry_over(prev + (size_t)p * n_prev, n_prev, dst, n);
+    const bool live = std::any_of(dst, dst + n, [](float x) { return x > 0.f; });
+    seed_op[p] = (p < keep && live) ? 20 : 9;
+    if (!live) render_fresh(draw_fresh(draws), dst, n, draws);
+    normalise_row(dst, n);
   }
   return SIDON_OK;
 }

@@ -471,11 +471,31 @@ int prepare_simt(int n_max, bool local_search) {
   return rc;
 }
 
+bool tuned_simt_tile(int n, int P, int* tk);
+int launch_local_search_simt_tile(void* pop, void* mom, void* vel, int P, int n, const int* skip,
+                                  const int* mode_arr, int iters, double pS, double pE,
+                                  double lrS, double lrE, double b1, double b2, int mode_default,
+                                  int tk, cudaStream_t st);
+
+int simt_tile_default(int n) { return tile_for(n); }
+
+// the odd lane tiles the fp32 local search can run at n (all give the same
+// results bit for bit), narrowest first; returns their count
+int simt_tile_choices(int n, int* out, int cap) {
+  int cnt = 0;
+  for (int tk = tile_for(n); tk <= kTK32 && cnt < cap; tk += 2) out[cnt++] = tk;
+  return cnt;
+}
+
 int launch_local_search(void* pop, void* mom, void* vel, const long long* offsets,
                         const int* order, int P, int n_fixed, int n_max, const int* skip,
                         const int* mode_arr, int iters, double pS, double pE, double lrS,
                         double lrE, double b1, double b2, int mode_default, int dtype,
                         cudaStream_t st) {
+  int tk = tile_for(n_max);
+  if (dtype == SIDON_F32 && !offsets && tuned_simt_tile(n_max, P, &tk))
+    return launch_local_search_simt_tile(pop, mom, vel, P, n_max, skip, mode_arr, iters, pS, pE,
+                                         lrS, lrE, b1, b2, mode_default, tk, st);
   if (dtype == SIDON_F32 && !offsets && tile_for(n_max) < kTK32) {
     // uniform candidates of n <= 1664: narrower lane tiles over the same
     // 4-warp team (bitwise the kTK32 kernel's results)
@@ -508,6 +528,34 @@ int launch_local_search(void* pop, void* mom, void* vel, const long long* offset
         mode_arr, iters, pS, pE, lrS, lrE, b1, b2, mode_default);
   }
   return check_launch();
+}
+
+// The uniform fp32 local search with lane tile tk (one of simt_tile_choices).
+int launch_local_search_simt_tile(void* pop, void* mom, void* vel, int P, int n, const int* skip,
+                                  const int* mode_arr, int iters, double pS, double pE,
+                                  double lrS, double lrE, double b1, double b2, int mode_default,
+                                  int tk, cudaStream_t st) {
+  switch (tk) {
+    case 7: return launch_ls_tiles<7>(pop, mom, vel, P, n, skip, mode_arr, iters, pS, pE, lrS,
+                                      lrE, b1, b2, mode_default, st);
+    case 9: return launch_ls_tiles<9>(pop, mom, vel, P, n, skip, mode_arr, iters, pS, pE, lrS,
+                                      lrE, b1, b2, mode_default, st);
+    case 11: return launch_ls_tiles<11>(pop, mom, vel, P, n, skip, mode_arr, iters, pS, pE, lrS,
+                                        lrE, b1, b2, mode_default, st);
+    case 13: return launch_ls_tiles<13>(pop, mom, vel, P, n, skip, mode_arr, iters, pS, pE, lrS,
+                                        lrE, b1, b2, mode_default, st);
+    case kTK32: {
+      const size_t sm = smem_local_search(n, SIDON_F32);
+      const void* fn = (const void*)k_local_search<float, kTK32>;
+      int rc = prep(fn, sm);
+      if (rc) return rc;
+      k_local_search<float, kTK32><<<P, 32 * warps_for<kTK32>(n), sm, st>>>(
+          (float*)pop, (float*)mom, (float*)vel, nullptr, nullptr, n, n, skip, mode_arr, iters,
+          (float)pS, (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default);
+      return check_launch();
+    }
+    default: return SIDON_ERR_ARG;
+  }
 }
 
 int launch_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,

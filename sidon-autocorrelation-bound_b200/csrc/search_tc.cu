@@ -15,15 +15,23 @@
 //  weights beyond 2n-1 stay zero for the whole launch (the correlation
 //  copies read whole blocks).
 // ---------------------------------------------------------------------------
+#include <algorithm>
 #include <mutex>
 
 #include "conv_simt.cuh"
 #include "tc_cta.cuh"
 
+// Phase marks inside the fused step: no code unless a profiling build
+// defines SIDON_PHASE(k) (phase k of the step has just ended).
+#ifndef SIDON_PHASE
+#define SIDON_PHASE(k)
+#endif
+
 namespace sidon {
 namespace tc {
 
-__device__ unsigned int g_status_word = 0u;   // SIDON_ERR_TIMEOUT after a timed-out wait
+// the device status word and the wait limit (common.cuh DeviceState)
+__device__ DeviceState g_dev_state = {0u, 0u, kDefaultWaitCycles};
 
 // cells per thread of the fused step's elementwise update: every n the
 // kernels accept (conv + corr accumulators within 512 TMEM columns, n <= 9728)
@@ -81,9 +89,13 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
                                             unsigned int* status) {
   Ctx& C = S.C;
   const int nb = 2 * n - 1;
+  SIDON_PHASE(0);
   prime(C, true);
+  SIDON_PHASE(1);
   if (!conv_tc_prebuilt(C, S.sa, status)) return 2;
+  SIDON_PHASE(2);
   const float M = block_max(gather_conv(C, ln, S.cb), S.red);   // b in cb
+  SIDON_PHASE(3);
   if (!(M > 0.f)) return 1;
   // c_k = (1+d)^(p-1), R = sum c_k (1+d), d = (b_k - M)/M, written straight
   // into the correlation's B copy: thread q takes chunks (row x, K group h)
@@ -117,6 +129,7 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
     fence_async_smem();
   }
   const float R = block_sum(rloc, S.red);      // barrier: weights complete
+  SIDON_PHASE(4);
   const float bc1 = 1.f / (1.f - b1t), bc2 = 1.f / (1.f - b2t);
   const float lrn = lr / (float)n;
 
@@ -134,8 +147,11 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
   }
   fence_before();
   __syncthreads();
+  SIDON_PHASE(5);
   if (!corr_tc_prebuilt(C, S.sa, status)) return 2;
+  SIDON_PHASE(6);
   gather_corr(C, ln, S.cb);                     // G in cb
+  SIDON_PHASE(7);
 
   // Adam / mirror step (cells i = thread + u * NTHREADS)
   float sloc = 0.f;
@@ -167,6 +183,7 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
   // renormalise (sum <= 0: the uniform 1/n), chunk by chunk of 8 cells,
   // and write the next step's autoconvolution B copy from the same chunks
   const float Ssum = block_sum(sloc, S.red);
+  SIDON_PHASE(8);
   const bool reset = !(Ssum > 0.f);
   const float inv = 1.f / (reset ? 1.f : Ssum);
   const float uniform = 1.f / (float)n;
@@ -199,6 +216,7 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
     fence_async_smem();
   }
   __syncthreads();
+  SIDON_PHASE(9);
   return 0;
 }
 
@@ -213,9 +231,9 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
                   const int* __restrict__ order, int P, int n_fixed, int n_max,
                   const int* __restrict__ skip, const int* __restrict__ mode_arr, int iters,
                   float pStart, float pEnd, float lrStart, float lrEnd, float beta1, float beta2,
-                  int mode_default, int three, unsigned int* status) {
+                  int mode_default, int three, unsigned int* status, int ring) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  Shared S = setup(n_max, three != 0, smem_raw);
+  Shared S = setup(n_max, three != 0, smem_raw, ring);
   Ctx& C = S.C;
   const Lane ln;
   for (int slot = blockIdx.x; slot < P; slot += gridDim.x) {
@@ -278,10 +296,10 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
 // so the wait is a formality.  Heights and moments cross between CTAs through
 // L2 (ld.global.cg); each step is lp_adam_step, the fused kernel's arithmetic,
 // so every candidate's trajectory is the fused kernel's bit for bit.  The
-// flags are reset by the host before each launch; the wait gives up after
-// ~2^31 cycles (SIDON_ERR_TIMEOUT).
-constexpr int kMaxSegCandidates = 1 << 16;
-__device__ unsigned int g_seg_flags[kMaxSegCandidates];
+// hand-over flags (one word per candidate) are caller memory, zeroed on the
+// launch's stream before it starts, so launches on different streams with
+// different flag words never see each other's; the wait gives up after the
+// device state's wait limit (SIDON_ERR_TIMEOUT).
 
 // steps [s0, s1) of candidate pid, its state read from and written to HBM
 __device__ __forceinline__ void run_piece(Shared& S, const Lane& ln, float* pop, float* mom,
@@ -292,17 +310,21 @@ __device__ __forceinline__ void run_piece(Shared& S, const Lane& ln, float* pop,
   float* a = pop + (size_t)pid * n;
   float* mg = mom + (size_t)pid * n;
   float* vg = vel + (size_t)pid * n;
+  SIDON_PHASE(10);
   begin(S, n, n);
-  bool bad = false;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float x = __ldcg(a + i);
-    if (s0 == 0) { bad |= bad_height(x); mg[i] = 0.f; vg[i] = 0.f; }
-    S.sa[pidx(i)] = x;
+  load_heights(S, a, n, status);
+  if (s0 == 0) {
+    bool bad = false;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      bad |= bad_height(S.sa[pidx(i)]);
+      mg[i] = 0.f;
+      vg[i] = 0.f;
+    }
+    note_bad(bad, status);
   }
-  note_bad(bad, status);
-  __syncthreads();
   write_conv_copy(S);
   __syncthreads();
+  SIDON_PHASE(11);
   float b1t = 1.f, b2t = 1.f;
   for (int it = 0; it < s0; ++it) {        // beta^s0, multiplied up as the fused kernel does
     b1t *= beta1;
@@ -321,6 +343,7 @@ __device__ __forceinline__ void run_piece(Shared& S, const Lane& ln, float* pop,
   __syncthreads();
   if (rs != 2)
     for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = S.sa[pidx(i)];
+  SIDON_PHASE(12);
 }
 
 __global__ void __launch_bounds__(NTHREADS, 1)
@@ -328,10 +351,11 @@ k_local_search_tc_seg(float* pop, float* mom, float* vel, int P, int n,
                       const int* __restrict__ skip, const int* __restrict__ mode_arr, int iters,
                       float pStart, float pEnd, float lrStart, float lrEnd, float beta1,
                       float beta2, int mode_default, int three, unsigned int* status,
-                      unsigned int* flags) {
+                      unsigned int* flags, int ring) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ int s_ok;
-  Shared S = setup(n, three != 0, smem_raw);
+  Shared S = setup(n, three != 0, smem_raw, ring);
+  SIDON_PHASE(15);
   const Lane ln;
   const float lnPr = (float)log((double)pEnd / (double)pStart);
   const float lnLr = (float)log((double)lrEnd / (double)lrStart);
@@ -362,9 +386,9 @@ k_local_search_tc_seg(float* pop, float* mom, float* vel, int P, int n,
         if (threadIdx.x == 0) {
           s_ok = 1;
           volatile unsigned int* f = flags + first;
-          const long long t0 = clock64();
+          const long long t0 = clock64(), lim = wait_limit(status);
           while (*f == 0u) {
-            if (clock64() - t0 > kWaitCycles) {
+            if (clock64() - t0 > lim) {
               s_ok = 0;
               atomicCAS(status, 0u, (unsigned int)SIDON_ERR_TIMEOUT);
               break;
@@ -654,8 +678,8 @@ static unsigned int* status_word() {
   std::lock_guard<std::mutex> lock(mu);
   if (!addr[dev]) {
     void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, tc::g_status_word) != cudaSuccess) return nullptr;
-    addr[dev] = (unsigned int*)p;
+    if (cudaGetSymbolAddress(&p, tc::g_dev_state) != cudaSuccess) return nullptr;
+    addr[dev] = &static_cast<DeviceState*>(p)->status;
   }
   return addr[dev];
 }
@@ -664,17 +688,28 @@ unsigned int* tc_status_word() { return status_word(); }
 
 int device_status(int reset) {
   unsigned int v = 0;
-  cudaError_t e = cudaMemcpyFromSymbol(&v, tc::g_status_word, sizeof(v));
+  cudaError_t e = cudaMemcpyFromSymbol(&v, tc::g_dev_state, sizeof(v),
+                                       offsetof(DeviceState, status));
   if (e != cudaSuccess) return set_cuda_error(e);
   if (reset) {
     const unsigned int z = 0;
-    e = cudaMemcpyToSymbol(tc::g_status_word, &z, sizeof(z));
+    e = cudaMemcpyToSymbol(tc::g_dev_state, &z, sizeof(z), offsetof(DeviceState, status));
     if (e != cudaSuccess) return set_cuda_error(e);
   }
   return (int)v;
 }
 
+// the clock-cycle limit of the bounded waits on the current device
+// (cycles <= 0: the default)
+int set_wait_limit(long long cycles) {
+  const long long v = cycles > 0 ? cycles : kDefaultWaitCycles;
+  const cudaError_t e =
+      cudaMemcpyToSymbol(tc::g_dev_state, &v, sizeof(v), offsetof(DeviceState, wait_cycles));
+  return e == cudaSuccess ? SIDON_OK : set_cuda_error(e);
+}
+
 size_t smem_local_search_tc(int n) { return tc::Layout(n).total; }
+static size_t smem_local_search_tc(int n, int ring) { return tc::Layout(n, ring).total; }
 static size_t smem_lp_forward_tc(int n) { return tc::Layout(n).total; }
 
 // the two accumulators must fit the 512 TMEM columns
@@ -692,30 +727,37 @@ int tc_n_ok_public(int n) { return tc_n_ok(n); }
 // Everything a local-search launch at n_max sets up on the host side (the
 // shared-memory attribute, the status word's address), done ahead of a
 // stream capture.
+int tc_ring_choices(int n, int* out, int cap);
+
 int prepare_local_search_tc(int n_max) {
   int rc = tc_n_ok(n_max);
   if (rc) return rc;
-  rc = prep_tc((const void*)tc::k_local_search_tc, smem_local_search_tc(n_max));
+  // the largest plan of any window ring the tuner may pick, for both kernels
+  size_t sm = smem_local_search_tc(n_max);
+  int rings[8];
+  const int nr = tc_ring_choices(n_max, rings, 8);
+  for (int r = 0; r < nr; ++r) sm = std::max(sm, smem_local_search_tc(n_max, rings[r]));
+  rc = prep_tc((const void*)tc::k_local_search_tc, sm);
+  if (!rc) rc = prep_tc((const void*)tc::k_local_search_tc_seg, sm);
   if (rc) return rc;
   return status_word() ? SIDON_OK : SIDON_ERR_CUDA;
 }
 
 // The balanced-segment kernel, or kNotHere when it does not apply (no
-// cooperative launch, fewer resident CTAs than SMs, more candidates than
-// flags, or the stream is being captured).
+// cooperative launch on the device, fewer resident CTAs than SMs, or fewer
+// candidates than SMs).  flags: P caller-owned words, zeroed here on the
+// stream.  The launch is a cooperative one (every CTA resident at once), made
+// through cudaLaunchKernelEx so that a stream capture records it as a
+// cooperative kernel node.
 constexpr int kNotHere = -1;
 static int launch_local_search_tc_seg(float* pop, float* mom, float* vel, int P, int n,
                                       const int* skip, const int* mode_arr, int iters, double pS,
                                       double pE, double lrS, double lrE, double b1, double b2,
-                                      int mode_default, int precision, size_t sm,
-                                      unsigned int* sw, cudaStream_t st) {
+                                      int mode_default, int precision, int ring, size_t sm,
+                                      unsigned int* sw, unsigned int* flags, cudaStream_t st) {
   int dev = 0, coop = 0, per_sm = 0;
-  if (P > tc::kMaxSegCandidates) return kNotHere;
   if (cudaGetDevice(&dev) != cudaSuccess) return kNotHere;
   if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
-    return kNotHere;
-  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
     return kNotHere;
   int rc = set_dyn_smem((const void*)tc::k_local_search_tc_seg, sm);
   if (rc) return rc;
@@ -725,66 +767,38 @@ static int launch_local_search_tc_seg(float* pop, float* mom, float* vel, int P,
     return kNotHere;
   const int G = sm_count();
   if (P < G) return kNotHere;
-  void* addr = nullptr;                    // the per-candidate flags (looked up per call)
-  cudaError_t e = cudaGetSymbolAddress(&addr, tc::g_seg_flags);
+  cudaError_t e = cudaMemsetAsync(flags, 0, (size_t)P * sizeof(unsigned int), st);
   if (e != cudaSuccess) return set_cuda_error(e);
-  unsigned int* flags = (unsigned int*)addr;
-  e = cudaMemsetAsync(flags, 0, (size_t)P * sizeof(unsigned int), st);
-  if (e != cudaSuccess) return set_cuda_error(e);
-  float fpS = (float)pS, fpE = (float)pE, flS = (float)lrS, flE = (float)lrE, fb1 = (float)b1,
-        fb2 = (float)b2;
-  int three = precision == SIDON_PREC_BF16X3 ? 1 : 0;
-  void* args[] = {&pop, &mom, &vel, &P, &n, &skip, &mode_arr, &iters, &fpS, &fpE, &flS, &flE,
-                  &fb1, &fb2, &mode_default, &three, &sw, &flags};
-  e = cudaLaunchCooperativeKernel((const void*)tc::k_local_search_tc_seg, dim3(G),
-                                  dim3(tc::NTHREADS), args, sm, st);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(G);
+  cfg.blockDim = dim3(tc::NTHREADS);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  e = cudaLaunchKernelEx(&cfg, tc::k_local_search_tc_seg, pop, mom, vel, P, n, skip, mode_arr,
+                         iters, (float)pS, (float)pE, (float)lrS, (float)lrE, (float)b1,
+                         (float)b2, mode_default, precision == SIDON_PREC_BF16X3 ? 1 : 0, sw,
+                         flags, ring);
   if (e != cudaSuccess) return set_cuda_error(e);
   return SIDON_OK;
 }
 
-int launch_local_search_tc_plain(float* pop, float* mom, float* vel, const long long* offsets,
-                                 const int* order, int P, int n_fixed, int n_max, const int* skip,
-                                 const int* mode_arr, int iters, double pS, double pE,
-                                 double lrS, double lrE, double b1, double b2, int mode_default,
-                                 int precision, cudaStream_t st);
-
-int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* offsets,
-                           const int* order, int P, int n_fixed, int n_max, const int* skip,
-                           const int* mode_arr, int iters, double pS, double pE, double lrS,
-                           double lrE, double b1, double b2, int mode_default, int precision,
-                           cudaStream_t st) {
-  int rc = tc_n_ok(n_max);
-  if (rc) return rc;
-  const size_t sm = smem_local_search_tc(n_max);
-  rc = prep_tc((const void*)tc::k_local_search_tc, sm);
-  if (rc) return rc;
-  unsigned int* sw = status_word();
-  if (!sw) return SIDON_ERR_CUDA;
-  // a uniform batch larger than one wave: balanced step segments over one
-  // resident CTA per SM (not inside a stream capture)
-  if (!offsets && P > sm_count()) {
-    const int r = launch_local_search_tc_seg(pop, mom, vel, P, n_fixed, skip, mode_arr, iters,
-                                             pS, pE, lrS, lrE, b1, b2, mode_default, precision,
-                                             sm, sw, st);
-    if (r != kNotHere) return r;              // else: the one-CTA-per-candidate kernel
-  }
-  return launch_local_search_tc_plain(pop, mom, vel, offsets, order, P, n_fixed, n_max, skip,
-                                      mode_arr, iters, pS, pE, lrS, lrE, b1, b2, mode_default,
-                                      precision, st);
-}
-
-// The fused kernel alone: one CTA per candidate for a uniform batch (CTAs of
+// The fused kernel, one CTA per candidate for a uniform batch (CTAs of
 // skipped candidates exit at once, so launches on disjoint candidate sets can
 // share the SMs from concurrent streams); persistent (one CTA per SM) for a
-// ragged batch.
-int launch_local_search_tc_plain(float* pop, float* mom, float* vel, const long long* offsets,
-                                 const int* order, int P, int n_fixed, int n_max, const int* skip,
-                                 const int* mode_arr, int iters, double pS, double pE,
-                                 double lrS, double lrE, double b1, double b2, int mode_default,
-                                 int precision, cudaStream_t st) {
+// ragged batch.  ring: the window ring's tiles per stage (0: ring_for).
+static int launch_plain(float* pop, float* mom, float* vel, const long long* offsets,
+                        const int* order, int P, int n_fixed, int n_max, const int* skip,
+                        const int* mode_arr, int iters, double pS, double pE, double lrS,
+                        double lrE, double b1, double b2, int mode_default, int precision,
+                        int ring, cudaStream_t st) {
   int rc = tc_n_ok(n_max);
   if (rc) return rc;
-  const size_t sm = smem_local_search_tc(n_max);
+  const size_t sm = smem_local_search_tc(n_max, ring);
   rc = prep_tc((const void*)tc::k_local_search_tc, sm);
   if (rc) return rc;
   unsigned int* sw = status_word();
@@ -793,8 +807,82 @@ int launch_local_search_tc_plain(float* pop, float* mom, float* vel, const long 
   tc::k_local_search_tc<<<grid, tc::NTHREADS, sm, st>>>(
       pop, mom, vel, offsets, order, P, n_fixed, n_max, skip, mode_arr, iters, (float)pS,
       (float)pE, (float)lrS, (float)lrE, (float)b1, (float)b2, mode_default,
-      precision == SIDON_PREC_BF16X3 ? 1 : 0, sw);
+      precision == SIDON_PREC_BF16X3 ? 1 : 0, sw, ring);
   return check_launch();
+}
+
+int launch_local_search_tc_plain(float* pop, float* mom, float* vel, const long long* offsets,
+                                 const int* order, int P, int n_fixed, int n_max, const int* skip,
+                                 const int* mode_arr, int iters, double pS, double pE,
+                                 double lrS, double lrE, double b1, double b2, int mode_default,
+                                 int precision, cudaStream_t st) {
+  return launch_plain(pop, mom, vel, offsets, order, P, n_fixed, n_max, skip, mode_arr, iters, pS,
+                      pE, lrS, lrE, b1, b2, mode_default, precision, 0, st);
+}
+
+bool tuned_tc_schedule(int n, int P, int precision, int* ring, int* balanced);
+
+// The tensor-core local search.  seg_flags (P words of caller memory, or
+// NULL) lets a uniform batch of more candidates than SMs run as balanced
+// step segments; without it the batch runs in waves of the one-CTA-per-
+// candidate kernel.  A uniform batch takes the window ring and the
+// segment / wave choice the schedule tuner measured for (n, P, precision),
+// if it ran; every choice gives the same results bit for bit.
+int launch_local_search_tc_sched(float* pop, float* mom, float* vel, const long long* offsets,
+                                 const int* order, int P, int n_fixed, int n_max, const int* skip,
+                                 const int* mode_arr, int iters, double pS, double pE,
+                                 double lrS, double lrE, double b1, double b2, int mode_default,
+                                 int precision, int ring, int balanced, unsigned int* seg_flags,
+                                 cudaStream_t st);
+
+int launch_local_search_tc(float* pop, float* mom, float* vel, const long long* offsets,
+                           const int* order, int P, int n_fixed, int n_max, const int* skip,
+                           const int* mode_arr, int iters, double pS, double pE, double lrS,
+                           double lrE, double b1, double b2, int mode_default, int precision,
+                           unsigned int* seg_flags, cudaStream_t st) {
+  int ring = 0, balanced = 1;
+  if (!offsets) tuned_tc_schedule(n_fixed, P, precision, &ring, &balanced);
+  return launch_local_search_tc_sched(pop, mom, vel, offsets, order, P, n_fixed, n_max, skip,
+                                      mode_arr, iters, pS, pE, lrS, lrE, b1, b2, mode_default,
+                                      precision, ring, balanced, seg_flags, st);
+}
+
+// the same with the schedule given: window ring (tiles per stage, 0 =
+// ring_for) and balanced segments (used when seg_flags is given and P > SMs)
+int launch_local_search_tc_sched(float* pop, float* mom, float* vel, const long long* offsets,
+                                 const int* order, int P, int n_fixed, int n_max, const int* skip,
+                                 const int* mode_arr, int iters, double pS, double pE,
+                                 double lrS, double lrE, double b1, double b2, int mode_default,
+                                 int precision, int ring, int balanced, unsigned int* seg_flags,
+                                 cudaStream_t st) {
+  int rc = tc_n_ok(n_max);
+  if (rc) return rc;
+  const size_t sm = smem_local_search_tc(n_max, ring);
+  unsigned int* sw = status_word();
+  if (!sw) return SIDON_ERR_CUDA;
+  if (seg_flags && balanced && !offsets && P > sm_count()) {
+    const int r = launch_local_search_tc_seg(pop, mom, vel, P, n_fixed, skip, mode_arr, iters,
+                                             pS, pE, lrS, lrE, b1, b2, mode_default, precision,
+                                             ring, sm, sw, seg_flags, st);
+    if (r != kNotHere) return r;              // else: the one-CTA-per-candidate kernel
+  }
+  return launch_plain(pop, mom, vel, offsets, order, P, n_fixed, n_max, skip, mode_arr, iters,
+                      pS, pE, lrS, lrE, b1, b2, mode_default, precision, ring, st);
+}
+
+// the window ring ring_for picks at n (tiles per stage; 1 = three single-tile stages)
+int tc_ring_default(int n) { return tc::Layout(n).ring.per_stage; }
+
+// the window ring shapes (tiles per stage) the fused kernel can run at n
+// within the shared-memory opt-in, in the tuner's order of trial
+int tc_ring_choices(int n, int* out, int cap) {
+  const tc::Layout auto_lo(n);
+  int cnt = 0;
+  for (int T = 1; T <= tc::kMaxStageTiles && cnt < cap; ++T) {
+    if (T > 1 && auto_lo.m < tc::kRingMinBlocks) break;   // short sequences: single tiles
+    if (tc::Layout(n, T).total <= tc::kSmemBudget) out[cnt++] = T;
+  }
+  return cnt;
 }
 
 size_t smem_frank_wolfe_tc(int n) { return tc::Layout(n).total; }

@@ -44,19 +44,27 @@ __host__ __device__ __forceinline__ Ring ring_for(int m, size_t other) {
       if (other + 2 * (size_t)stage_bytes(T) <= kSmemBudget) return Ring{2, T};
   return Ring{3, 1};
 }
+// A ring chosen by the schedule tuner: tiles per stage T (1: three
+// single-tile stages, 2..5: two stages of T tiles), 0 = ring_for's choice.
+// Every shape gives the same results bit for bit (each accumulator receives
+// its MMAs in the same order); the tuner offers only shapes that fit.
+__host__ __device__ __forceinline__ Ring ring_of(int tiles) {
+  return tiles == 1 ? Ring{3, 1} : Ring{2, tiles};
+}
 
 // dynamic shared memory plan (byte offsets from a 1 KB aligned base)
 struct Layout {
   int m, rc, rcc, sa_len, cb_len;
   Ring ring;
   size_t off_bc, off_sa, off_cb, off_red, total;
-  __host__ __device__ Layout(int n) {
+  __host__ __device__ Layout(int n, int ring_tiles = 0) {
     m = (n + BL - 1) / BL;
     rc = conv_copy_rows(m);
     rcc = corr_copy_rows(m);
     sa_len = 68 * (m + 8);                 // padded heights, 136 cells of margin in front
     cb_len = 68 * (2 * m + 2);             // padded weights / gather scratch
-    ring = ring_for(m, place(0));          // the ring takes whole KB: the rest keeps its padding
+    // the ring takes whole KB: the rest keeps its padding
+    ring = ring_tiles > 0 ? ring_of(ring_tiles) : ring_for(m, place(0));
     place((size_t)ring.stages * stage_bytes(ring.per_stage));
   }
   // lay out everything after a ring of `o` bytes; returns the total
@@ -75,7 +83,7 @@ struct Layout {
     o += (size_t)cb_len * 4;
     o = (o + 15) & ~(size_t)15;
     off_red = o;
-    o += 64 * 4 + (2 * MAX_STAGES + 5) * 8 + 16;
+    o += 64 * 4 + (2 * MAX_STAGES + 6) * 8 + 16;
     total = o + 1024;                      // slack for aligning the dynamic base to 1 KB
     return total;
   }
@@ -90,8 +98,9 @@ struct Shared {
 
 // Per-CTA set-up for candidates of up to n_max cells: buffer addresses,
 // barriers, TMEM.  begin() then prepares one candidate.
-__device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* raw) {
-  const Layout Lo(n_max);
+__device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* raw,
+                                        int ring_tiles = 0) {
+  const Layout Lo(n_max, ring_tiles);
   unsigned char* base = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
   Shared S;
   S.C.stages = base;
@@ -104,8 +113,8 @@ __device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* ra
   S.C.empty = bars + MAX_STAGES;
   S.C.bc_full = bars + 2 * MAX_STAGES;
   S.C.bc_empty = bars + 2 * MAX_STAGES + 2;
-  S.C.bar_done = bars + 2 * MAX_STAGES + 4;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * MAX_STAGES + 5);
+  S.C.bar_done = bars + 2 * MAX_STAGES + 4;      // bar_done + 1: bulk copies
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * MAX_STAGES + 6);
   S.C.abort = reinterpret_cast<int*>(tslot + 1);
   S.C.m = Lo.m;
   S.C.rc = Lo.rc;
@@ -127,8 +136,10 @@ __device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* ra
       mbar_init(&S.C.bc_empty[s], 1);
     }
     mbar_init(S.C.bar_done, 1);
+    mbar_init(S.C.bar_done + 1, 1);
     mbar_fence_init();
-    *S.C.abort = 0;
+    S.C.abort[0] = 0;
+    S.C.abort[1] = 0;                      // parity of the bulk-copy barrier
   }
   if ((threadIdx.x >> 5) == 0) tmem_alloc(tslot, 512);
   fence_before();
@@ -153,6 +164,41 @@ __device__ __forceinline__ void begin(Shared& S, int n, int n_max) {
   S.C.rcc = Ln.rcc;
   S.C.dmax = last_tile(n);
   __syncthreads();
+}
+
+// Heights of a candidate (global row a, n cells) into the padded shared
+// layout S.sa.  When the row and its length allow (16-byte aligned start, n
+// a multiple of 4), one thread issues a 1-D bulk copy per 64-cell block
+// (cp.async.bulk, the TMA engine; this GPU's memory, no multicast) and the
+// CTA waits for the bytes on bar_load -- a wait that ignores the abort flag,
+// as copies in flight must land before the buffer is reused; otherwise
+// every thread loads through L2.  begin() must have run (it zeroes the
+// margins; its barrier orders those stores before the copies).  Ends
+// synchronised.  Returns whether the bulk path was taken.
+__device__ __forceinline__ bool load_heights(Shared& S, const float* a, int n,
+                                             unsigned int* status) {
+  uint64_t* bar = S.C.bar_done + 1;
+  volatile int* parity = S.C.abort + 1;
+  const bool bulk = ((reinterpret_cast<uintptr_t>(a) & 15) == 0) && (n % 4 == 0);
+  if (bulk) {
+    fence_async_smem();            // begin()'s stores before the copies' writes
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      fence_proxy_async_all();     // rows published to this thread before its copies
+      mbar_arrive_tx(bar, (uint32_t)n * 4u);
+      for (int J = 0; 64 * J < n; ++J) {
+        const int len = n - 64 * J < 64 ? n - 64 * J : 64;
+        bulk_load(S.sa + pidx(64 * J), a + 64 * J, (uint32_t)len * 4u, bar);
+      }
+    }
+    drain_phase(bar, (uint32_t)*parity, status);
+    __syncthreads();
+    if (threadIdx.x == 0) *parity ^= 1;
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] = __ldcg(a + i);
+  }
+  __syncthreads();
+  return bulk;
 }
 
 __device__ __forceinline__ void teardown(Shared& S) {

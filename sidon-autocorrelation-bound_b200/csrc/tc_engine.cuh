@@ -53,8 +53,11 @@
 //  per commit against ~70 per M128 N144 K16 instruction), so long tile
 //  sequences run two stages of two to five tiles -- one commit per stage --
 //  and short ones three single-tile stages (see ring_for).
-//  Every wait gives up after ~2^31 clock cycles, records SIDON_ERR_TIMEOUT in
-//  the library's device status word and unwinds.
+//  Every pipeline wait gives up after the device state's wait limit (2^31
+//  clock cycles unless sidon_set_wait_limit changed it), records
+//  SIDON_ERR_TIMEOUT in the library's device status word and unwinds; the
+//  unwinding still waits for the MMAs already issued (drain_phase) before
+//  the accumulators or the tensor memory are given up.
 // ---------------------------------------------------------------------------
 #pragma once
 #include <cuda_bf16.h>
@@ -84,7 +87,7 @@ __host__ __device__ constexpr int stage_bytes(int T) { return 2 * stage_plane_by
 // and the step compiles without spills), 16 slower than 8 at most n.
 constexpr int NTHREADS = 384;
 constexpr int WARPS_PER_QUAD = NTHREADS / 128;
-constexpr long long kWaitCycles = 1ll << 31;
+constexpr long long kWaitCycles = kDefaultWaitCycles;   // limit of the drain wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -220,7 +223,8 @@ struct Ctx {
   uint64_t* empty;         // nst "windows consumed" barriers (tcgen05.commit)
   uint64_t* bc_full;       // "copy ready" barrier (NBUILD_WARPS arrivals; [0] used)
   uint64_t* bc_empty;      // "copy consumed" barrier (tcgen05.commit; [0] used)
-  uint64_t* bar_done;      // "all MMAs of a phase done"
+  uint64_t* bar_done;      // "all MMAs of a phase done" (the next barrier,
+                           // bar_done + 1, counts the bytes of bulk copies)
   uint32_t tmem;           // TMEM base address (512 columns)
   // pipeline phases as bit masks (registers, no dynamic indexing): bit s of
   // ph = parity of this thread's next wait on stage s (full for the MMA
@@ -230,7 +234,8 @@ struct Ctx {
   uint32_t ph, started, bc_ph, bc_started, done_ph;
   int st_next;             // next stage in the ring
   int nst, wps;            // ring shape: stages, tiles per stage
-  int* abort;              // shared abort flag
+  int* abort;              // shared abort flag (the next word: the parity of
+                           // the bulk-copy barrier's next phase)
   int m, rc, rcc, n, dmax; // blocks, conv / corr copy rows, cells, last tile
   bool three;              // BF16x3 (else BF16x1)
 };
@@ -242,15 +247,35 @@ __host__ __device__ __forceinline__ int conv_width(int m) { return round_up(2 * 
 __host__ __device__ __forceinline__ int corr_n(int m) { return round_up(m + 1, 16); }
 __host__ __device__ __forceinline__ int corr_width(int m) { return round_up(corr_n(m), 32); }
 
-// bounded wait on an mbarrier phase; sets the abort flag on timeout
+// Bounded wait on an mbarrier phase inside the tile pipeline: gives up when
+// another thread has aborted, or after the device state's wait limit
+// (sidon_set_wait_limit), in which case it records SIDON_ERR_TIMEOUT and sets
+// the abort flag.
 __device__ __forceinline__ bool wait_phase(Ctx& C, uint64_t* bar, uint32_t parity,
                                            unsigned int* status) {
   if (mbar_try(bar, parity)) return true;
-  const long long t0 = clock64();
+  const long long t0 = clock64(), lim = wait_limit(status);
   while (!mbar_try(bar, parity)) {
     if (*((volatile int*)C.abort)) return false;
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > lim) {
       atomicExch(C.abort, 1);
+      atomicCAS(status, 0u, (unsigned int)SIDON_ERR_TIMEOUT);
+      return false;
+    }
+  }
+  return true;
+}
+
+// The end-of-phase wait for the MMA lane's final commit.  It must see every
+// issued MMA complete before the CTA reads the accumulators, reuses the
+// stages or releases the tensor memory, so it ignores the abort flag and the
+// configurable limit: the commit arrives once the tensor pipe has drained,
+// which needs no other thread.  Bounded by kWaitCycles all the same.
+__device__ __forceinline__ bool drain_phase(uint64_t* bar, uint32_t parity, unsigned int* status) {
+  if (mbar_try(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try(bar, parity)) {
+    if (clock64() - t0 > kWaitCycles) {
       atomicCAS(status, 0u, (unsigned int)SIDON_ERR_TIMEOUT);
       return false;
     }
@@ -260,6 +285,29 @@ __device__ __forceinline__ bool wait_phase(Ctx& C, uint64_t* bar, uint32_t parit
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// ---- 1-D bulk copies (TMA engine, no tensor map, no multicast) ----
+// Global -> this CTA's shared memory, completing on `bar` by byte count.
+// dst, src and bytes must be multiples of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :
+      : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// the issuing thread's arrival on `bar`, announcing `bytes` of bulk copies
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// order this thread's earlier generic-proxy accesses before later
+// async-proxy (bulk copy) accesses
+__device__ __forceinline__ void fence_proxy_async_all() {
+  asm volatile("fence.proxy.async;" ::: "memory");
 }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float first, float second) {
@@ -561,7 +609,7 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
     }
   }
   C.st_next = st;
-  const bool ok = wait_phase(C, C.bar_done, C.done_ph, status);
+  const bool ok = drain_phase(C.bar_done, C.done_ph, status);
   C.done_ph ^= 1u;
   fence_after();
   __syncthreads();
@@ -681,36 +729,56 @@ __device__ __forceinline__ float gather_conv(Ctx& C, const Lane& ln, float* X) {
 
 // G_i into Y (padded layout, i < n) from the correlation accumulator: cell
 // (r, col) holds a part of i = 64 col + 63 - r; the upper-lane cell of i sits
-// one column right of its lower-lane cell, so the rounds run the halves in
-// the opposite order to gather_conv.
+// one column right of its lower-lane cell.  Two rounds, every warp busy in
+// both: for the i whose lower cell lies in the first `cmid` columns the lower
+// lanes write first and the upper lanes add (their cell lies at most at
+// column cmid, so the upper warps also read the chunk holding column cmid),
+// for the rest the upper lanes write first and the lower lanes add.  G_i is
+// L + U either way (a sum of two floats does not depend on their order).
+// Ends synchronised.
 __device__ __forceinline__ void gather_corr(Ctx& C, const Lane& ln, float* Y) {
   const int n = C.n, nch = (corr_n(C.m) + 31) / 32;
-  const int mid = (nch + 1) / 2;
+  const int mid = nch / 2, cmid = 32 * mid;
   const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)col_corr(C.m);
   const bool upper = ln.quad >= 2;
-  for (int round = 0; round < 3; ++round) {
-    if (upper && round < 2) {
-      for_chunks(lanebase, ln.sub, round == 0 ? mid : 0, round == 0 ? nch : mid,
-                 [&](int c, const float (&v)[32], int o) {
+  // round 1: lower cells of columns < cmid, upper cells of columns > cmid
+  if (upper) {
+    for_chunks(lanebase, ln.sub, mid, nch, [&](int c, const float (&v)[32], int o) {
 #pragma unroll
-                   for (int t = 0; t < 32; ++t) {
-                     const int i = 64 * (32 * c + t) + 63 - ln.r;
-                     if (i >= 0 && i < n) Y[pidx(i)] = v[o + t];
-                   }
-                 });
-    }
-    if (!upper && round > 0) {
-      for_chunks(lanebase, ln.sub, round == 1 ? mid : 0, round == 1 ? nch : mid,
-                 [&](int c, const float (&v)[32], int o) {
+      for (int t = 0; t < 32; ++t) {
+        const int col = 32 * c + t, i = 64 * col + 63 - ln.r;
+        if (col > cmid && i < n) Y[pidx(i)] = v[o + t];
+      }
+    });
+  } else {
+    for_chunks(lanebase, ln.sub, 0, mid, [&](int c, const float (&v)[32], int o) {
 #pragma unroll
-                   for (int t = 0; t < 32; ++t) {
-                     const int i = 64 * (32 * c + t) + 63 - ln.r;
-                     if (i >= 0 && i < n) Y[pidx(i)] += v[o + t];
-                   }
-                 });
-    }
-    __syncthreads();
+      for (int t = 0; t < 32; ++t) {
+        const int i = 64 * (32 * c + t) + 63 - ln.r;
+        if (i < n) Y[pidx(i)] = v[o + t];
+      }
+    });
   }
+  __syncthreads();
+  // round 2: the partner cells, added
+  if (upper) {
+    for_chunks(lanebase, ln.sub, 0, mid < nch ? mid + 1 : nch, [&](int c, const float (&v)[32], int o) {
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const int col = 32 * c + t, i = 64 * col + 63 - ln.r;
+        if (col <= cmid && i >= 0 && i < n) Y[pidx(i)] += v[o + t];
+      }
+    });
+  } else {
+    for_chunks(lanebase, ln.sub, mid, nch, [&](int c, const float (&v)[32], int o) {
+#pragma unroll
+      for (int t = 0; t < 32; ++t) {
+        const int i = 64 * (32 * c + t) + 63 - ln.r;
+        if (i < n) Y[pidx(i)] += v[o + t];
+      }
+    });
+  }
+  __syncthreads();
 }
 
 // b = a * a (accumulator at COL_CONV)

@@ -85,6 +85,20 @@ def max_n(op: int, dtype_code: int = _lib.F32) -> int:
 
 
 # ------------------------------ host oracle --------------------------------
+def device_status(reset: bool = False) -> int:
+    """The device-side status word of the tensor-core kernels (0, or the first
+    SIDON_ERR_TIMEOUT / SIDON_ERR_NONFINITE since the last reset)."""
+    rc = _lib.load().sidon_device_status(1 if reset else 0)
+    if rc < 0:
+        raise SidonError("sidon_device_status", rc)
+    return rc
+
+
+def set_wait_limit(cycles: int = 0) -> None:
+    """Clock-cycle limit of the kernels' bounded waits (0: the default 2^31)."""
+    _lib.call("sidon_set_wait_limit", int(cycles))
+
+
 def host_f(a) -> float:
     """fp64 F on the host, bit-identical to hostF (src/main.cu:95-105)."""
     arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
@@ -92,14 +106,30 @@ def host_f(a) -> float:
 
 
 # ------------------------------ operators ----------------------------------
+def local_search_workspace(n: int, P: int, precision: str = "bf16x3", device="cuda",
+                           dtype=torch.float32) -> torch.Tensor | None:
+    """Workspace of run_local_search's balanced-segment form (None if the call
+    needs none)."""
+    code = _lib.F32 if dtype == torch.float32 else _lib.F64
+    nb = _lib.load().sidon_local_search_workspace_bytes(n, P, code, PRECISIONS[precision])
+    return torch.empty(nb, dtype=torch.uint8, device=device) if nb else None
+
+
 def run_local_search(pop: torch.Tensor, iters: int, p_start: float, p_end: float,
                      lr_start: float, lr_end: float, mode_arr: torch.Tensor | None = None,
                      skip: torch.Tensor | None = None, mom: torch.Tensor | None = None,
                      vel: torch.Tensor | None = None, beta1: float = 0.9, beta2: float = 0.999,
-                     mode_default: int = 0, precision: str | None = None, stream=None) -> None:
+                     mode_default: int = 0, precision: str | None = None, stream=None,
+                     workspace: torch.Tensor | None = None, balanced: bool = True) -> None:
     """L^p-annealed projected Adam / mirror descent on every non-skipped
     candidate, in place (kLocalSearch + runLocalSearch,
-    src/kernels.cuh:177-289, src/main.cu:152-159)."""
+    src/kernels.cuh:177-289, src/main.cu:152-159).
+
+    With ``balanced`` (default) a tensor-core batch of more candidates than
+    SMs runs as balanced step segments through sidon_local_search_ws, its
+    flag words in ``workspace`` (allocated here when None); ``balanced=False``
+    calls sidon_local_search, one CTA per candidate.  Results are the same
+    bit for bit."""
     n, P = _pop_shape(pop)
     code = _dtype_code(pop)
     if precision is None:
@@ -108,11 +138,21 @@ def run_local_search(pop: torch.Tensor, iters: int, p_start: float, p_end: float
         mom = torch.empty_like(pop)
     if vel is None:
         vel = torch.empty_like(pop)
-    _lib.call("sidon_local_search", _dev(pop, "pop"), _dev(mom, "mom", pop.dtype),
-              _dev(vel, "vel", pop.dtype), _opt(skip, "skip", torch.int32),
-              _opt(mode_arr, "mode_arr", torch.int32), n, P, int(iters), float(p_start),
-              float(p_end), float(lr_start), float(lr_end), float(beta1), float(beta2),
-              int(mode_default), code, PRECISIONS[precision], _stream(stream))
+    args = (_dev(pop, "pop"), _dev(mom, "mom", pop.dtype), _dev(vel, "vel", pop.dtype),
+            _opt(skip, "skip", torch.int32), _opt(mode_arr, "mode_arr", torch.int32), n, P,
+            int(iters), float(p_start), float(p_end), float(lr_start), float(lr_end),
+            float(beta1), float(beta2), int(mode_default), code, PRECISIONS[precision])
+    nb = _lib.load().sidon_local_search_workspace_bytes(n, P, code, PRECISIONS[precision])
+    if not balanced or nb == 0:
+        _lib.call("sidon_local_search", *args, _stream(stream))
+        return
+    if workspace is None:
+        workspace = torch.empty(nb, dtype=torch.uint8, device=pop.device)
+        if stream is not None:
+            workspace.record_stream(stream)      # freed here, in use on `stream`
+    _dev(workspace, "workspace")
+    _lib.call("sidon_local_search_ws", *args, workspace.data_ptr(), workspace.numel(),
+              _stream(stream))
 
 
 # P * n limit of run_local_search_noalloc (the library's fixed moment array)
@@ -355,6 +395,23 @@ def polish(best_a, K: int = 8, iters: int = 40000, passes: int = 6, seed: int = 
 
 
 # ----------------------------- large candidates ----------------------------
+def autotune_local_search(n: int, P: int, precision: str = "bf16x3") -> dict:
+    """Time every schedule of the fused local search at (n, P, precision) --
+    lane tile (fp32), window ring and segments vs waves (tensor cores) --
+    and keep the fastest for this process; results are unchanged bit for bit.
+    Returns the chosen schedule."""
+    s = _lib.LsSchedule()
+    _lib.call("sidon_autotune_local_search", int(n), int(P), PRECISIONS[precision], C.byref(s))
+    return s.as_dict()
+
+
+def local_search_schedule(n: int, P: int, precision: str = "bf16x3") -> dict:
+    """The schedule the next uniform local search at (n, P, precision) uses."""
+    s = _lib.LsSchedule()
+    _lib.call("sidon_local_search_schedule", int(n), int(P), PRECISIONS[precision], C.byref(s))
+    return s.as_dict()
+
+
 def autotune_large(n: int, P: int, precision: str = "bf16x3") -> tuple[int, float]:
     """Measure and remember the fastest schedule for (n, P): returns (q, ms
     per step); q >= n is the fused single-CTA kernel."""

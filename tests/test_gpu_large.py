@@ -61,6 +61,27 @@ def test_large_search_tracks_oracle(cuda, orc):
         assert abs(Fg - Fw) <= 1e-4 * Fw, (p, Fg, Fw)
 
 
+def test_large_search_production_geometry_tracks_oracle(cuda, orc):
+    """The ladder's own geometry: n = 16384 in two 8192-cell super-blocks
+    (three convolution jobs, four correlation jobs per step), a few steps,
+    against the fp32 oracle at the BF16x3 bar."""
+    from sidon_b200 import synth
+    n = 16384
+    pop = synth.population("structured", n, 2, seed=67)
+    a = T(pop, cuda)
+    K().run_local_search_large(a, 4, 2.0, 16.0, 1e-3, 1e-3, q=8192)
+    assert _status() == 0
+    want = orc.local_search(pop, 4, 2.0, 16.0, 1e-3, 1e-3)
+    got = a.cpu().numpy()
+    assert (got >= 0).all()
+    for p in range(2):
+        Fg = orc.host_f(got[p].astype(np.float64))
+        Fw = orc.host_f(want[p].astype(np.float64))
+        F0 = orc.host_f(pop[p].astype(np.float64))
+        assert Fw < F0
+        assert abs(Fg - Fw) <= 1e-4 * Fw, (p, Fg, Fw)
+
+
 def test_large_search_skip_mode_and_zero(cuda):
     from sidon_b200 import synth
     n = 700

@@ -22,7 +22,12 @@ def _start(n, P, seed):
     return synth.population("structured", n, P, seed=seed)
 
 
-@pytest.mark.parametrize("precision,n,P", [("fp32", 700, 6), ("bf16x3", 1000, 4)])
+# (fp32, 700, 6): narrow-tile SIMT kernel; (fp32, 2048, 8): 15-output SIMT
+# kernel; (bf16x3, 1000, 4): one CTA per candidate; (bf16x3, 4096, 200): more
+# candidates than SMs, so the balanced-segment kernel runs with its hand-over
+# flags in the library's array (P n = 819200 cells, within the limit).
+@pytest.mark.parametrize("precision,n,P", [("fp32", 700, 6), ("fp32", 2048, 8),
+                                           ("bf16x3", 1000, 4), ("bf16x3", 4096, 200)])
 def test_noalloc_matches_regular_entry_point_twice(cuda, precision, n, P):
     from sidon_b200 import kernels
     args = (25, 4.0, 64.0, 0.02, 0.005)
