@@ -51,7 +51,9 @@ enum sidon_precision {
   SIDON_PREC_FP32_SIMT = 0,   /* fp32 FFMA chains on the CUDA cores            */
   SIDON_PREC_BF16X1 = 1,      /* tcgen05 block-Toeplitz, hi*hi                 */
   SIDON_PREC_BF16X3 = 2,      /* tcgen05 block-Toeplitz, hi*hi + hi*lo + lo*hi */
-  SIDON_PREC_FP64_SIMT = 3    /* fp64 DFMA chains (the polish instantiation)   */
+  SIDON_PREC_FP64_SIMT = 3,   /* fp64 DFMA chains (the polish instantiation)   */
+  SIDON_PREC_TF32X3 = 4       /* tcgen05 kind::tf32, hi*hi + hi*lo + lo*hi;
+                                 G_p forward / backward only                    */
 };
 
 /* operator ids for sidon_smem_bytes */
@@ -193,7 +195,9 @@ SIDON_API int sidon_local_search_noalloc(float* pop, const int* skip, const int*
  * heights, any scale).  Writes value[P] (device) and saved[P*4] (device,
  * {M = max b, S = sum a, R = sum (b/M)^p, G_p}); b itself is not stored
  * unless b_out != NULL ([P][2n-1] device, for the stored-b comparison).
- * precision FP32_SIMT, or BF16X1 / BF16X3 (b on the tensor cores).
+ * precision FP32_SIMT, or BF16X1 / BF16X3 / TF32X3 (b on the tensor cores;
+ * TF32X3 up to the n its plan fits in shared memory, about 8700, else
+ * SIDON_ERR_SMEM).
  * No reference counterpart as an entry point: it exposes the objective of
  * the anneal (src/kernels.cuh:168-172). */
 SIDON_API int sidon_lp_forward(const float* a, int n, int P, double p, float* value, float* saved,
@@ -203,7 +207,7 @@ SIDON_API int sidon_lp_forward(const float* a, int n, int P, double p, float* va
  * G_i = sum_j (b_{i+j}/M)^(p-1) a_j.  b is recomputed tile by tile from a
  * (b_in == NULL) or read from a stored [P][2n-1] array (b_in != NULL).
  * precision as for sidon_lp_forward (the correlation on the tensor cores
- * for BF16X1 / BF16X3).
+ * for BF16X1 / BF16X3 / TF32X3).
  * saved: the forward's [P*4].  grad: device [P][n] fp32.
  * Replaces the gradient that exists only inside kLocalSearch
  * (src/kernels.cuh:221-244) and its CPU twin (tools/probe.cpp:77-92). */

@@ -14,6 +14,7 @@ never does.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import pathlib
 import subprocess
 
@@ -25,7 +26,11 @@ REF_DIR = HERE / "_ref"
 REF_PROBE = REF_DIR / "libref_probe.so"
 REF_MAIN = REF_DIR / "libref_main.so"
 REF_PROBE_EXE = REF_DIR / "probe"
-REFERENCE_TREE = pathlib.Path("/root/reference")
+# Where the reference project's sources lie, for building oracle/_ref: the
+# SIDON_REFERENCE_ROOT environment variable, else the reference checkout of the
+# development container this checker was written in.  Machines without it
+# (the GPU boxes) use the oracle/_ref built beforehand.
+REFERENCE_TREE = pathlib.Path(os.environ.get("SIDON_REFERENCE_ROOT") or "/root/reference")
 
 _vp, _i, _d, _f = C.c_void_p, C.c_int, C.c_double, C.c_float
 _LD = C.c_longdouble
@@ -73,9 +78,9 @@ _main = None
 def build() -> None:
     """Build the C restatement (and oracle/_ref when the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    if REFERENCE_TREE.exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True,
-                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    if (REFERENCE_TREE / "src").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REFERENCE_TREE}"],
+                       check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
 
 
 def lib() -> C.CDLL:

@@ -16,7 +16,7 @@ LIB_PATH = HERE / "libsidon_b200.so"
 OK, ERR_ARG, ERR_N, ERR_SMEM, ERR_CUDA, ERR_DTYPE, ERR_NONFINITE, ERR_TIMEOUT, ERR_DEVICE = range(9)
 ERR_CAPACITY = 9
 F32, F64 = 0, 1
-PREC_FP32_SIMT, PREC_BF16X1, PREC_BF16X3, PREC_FP64_SIMT = 0, 1, 2, 3
+PREC_FP32_SIMT, PREC_BF16X1, PREC_BF16X3, PREC_FP64_SIMT, PREC_TF32X3 = 0, 1, 2, 3, 4
 OP_LOCAL_SEARCH, OP_EVAL, OP_FRANK_WOLFE, OP_LOCAL_SEARCH_TC = 0, 1, 2, 3
 
 _vp, _i, _d, _f, _sz = C.c_void_p, C.c_int, C.c_double, C.c_float, C.c_size_t

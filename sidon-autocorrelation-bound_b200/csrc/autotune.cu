@@ -210,8 +210,8 @@ int autotune_ls_schedule(int n, int P, int precision, sidon_ls_schedule* out) {
     const int nt = simt_tile_choices(n, tk, 8);
     for (int i = 0; i < nt; ++i) cands.push_back(sidon_ls_schedule{tk[i], 0, 0, 0.f, 1});
   } else {
-    int rings[8];
-    const int nr = tc_ring_choices(n, rings, 8);
+    int rings[20];
+    const int nr = tc_ring_choices(n, rings, 20);
     for (int i = 0; i < nr; ++i) {
       cands.push_back(sidon_ls_schedule{0, rings[i], 0, 0.f, 1});
       if (P > sm_count()) cands.push_back(sidon_ls_schedule{0, rings[i], 1, 0.f, 1});

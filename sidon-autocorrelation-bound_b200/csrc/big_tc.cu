@@ -543,7 +543,7 @@ int job_grid(long long jobs) {
 }  // namespace
 
 int tc_n_ok_public(int n);
-size_t smem_local_search_tc(int n);
+size_t smem_tc_plain(int n);
 
 size_t big_workspace_bytes(int n, int P, int Q) {
   if (n < 1 || P < 0 || Q < 64 || Q % 64) return 0;
@@ -562,7 +562,7 @@ int big_default_q(int n) {
 static int big_prep(int Q) {
   int rc = tc_n_ok_public(Q);
   if (rc) return rc;
-  const size_t sm = smem_local_search_tc(Q);
+  const size_t sm = smem_tc_plain(Q);
   rc = set_dyn_smem((const void*)big::k_conv_jobs, sm);
   if (!rc) rc = set_dyn_smem((const void*)big::k_corr_jobs, sm);
   if (rc) return rc;
@@ -596,7 +596,7 @@ int launch_local_search_big(float* pop, float* mom, float* vel, const int* skip,
   const int R = (n + Q - 1) / Q;
   const int three = precision == SIDON_PREC_BF16X3 ? 1 : 0;
   unsigned int* sw = tc_status_word();
-  const size_t sm = smem_local_search_tc(Q);
+  const size_t sm = smem_tc_plain(Q);
   const dim3 eg_b(big::NCH, P), eg_n(big::NCH, P);
   big::k_ls_init<<<sm_count() * 4, 256, 0, st>>>(skip, n, P, w.flags, w.bstate, mom, vel);
   rc = check_launch();
@@ -646,7 +646,7 @@ int launch_frank_wolfe_big(float* pop, const int* skip, int n, int P, int rounds
   const int R = (n + Q - 1) / Q;
   const int three = precision == SIDON_PREC_BF16X3 ? 1 : 0;
   unsigned int* sw = tc_status_word();
-  const size_t sm = smem_local_search_tc(Q);
+  const size_t sm = smem_tc_plain(Q);
   const dim3 eg(big::NCH, P);
   if (!(tau > 0.f)) tau = 0.9f / (float)n;
   if (!(sig > 0.f)) sig = 0.9f * (float)n;

@@ -35,6 +35,10 @@ int launch_lp_forward_tc(const float* a, int n, int P, double p, float* value, f
 int launch_lp_backward_tc(const float* a, const float* saved, const float* b_in, int n, int P,
                           double p, float* grad, int precision, cudaStream_t st);
 int device_status(int reset);
+int launch_lp_forward_tf32(const float* a, int n, int P, double p, float* value, float* saved,
+                           float* b_out, cudaStream_t st);
+int launch_lp_backward_tf32(const float* a, const float* saved, const float* b_in, int n, int P,
+                            double p, float* grad, cudaStream_t st);
 int set_wait_limit(long long cycles);
 int launch_lp_backward(const float* a, const float* saved, const float* b_in, int n, int P,
                        double p, float* grad, cudaStream_t st);
@@ -199,7 +203,8 @@ size_t sidon_smem_bytes(int op, int n, int dtype) {
     case SIDON_OP_LOCAL_SEARCH: return smem_local_search(n, dtype);
     case SIDON_OP_EVAL: return (dtype == SIDON_F32 || dtype == SIDON_F64) ? smem_eval(n) : 0;
     case SIDON_OP_FRANK_WOLFE: return dtype == SIDON_F32 ? smem_fw(n) : 0;
-    case SIDON_OP_LOCAL_SEARCH_TC: return dtype == SIDON_F32 ? smem_local_search_tc(n) : 0;
+    case SIDON_OP_LOCAL_SEARCH_TC:
+      return (dtype == SIDON_F32 && tc_n_ok_public(n) == SIDON_OK) ? smem_local_search_tc(n) : 0;
     default: return 0;
   }
 }
@@ -325,6 +330,8 @@ int sidon_lp_forward(const float* a, int n, int P, double p, float* value, float
     return launch_lp_forward(a, n, P, p, value, saved, b_out, S(stream));
   if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
     return launch_lp_forward_tc(a, n, P, p, value, saved, b_out, precision, S(stream));
+  if (precision == SIDON_PREC_TF32X3)
+    return launch_lp_forward_tf32(a, n, P, p, value, saved, b_out, S(stream));
   return SIDON_ERR_DTYPE;
 }
 
@@ -338,6 +345,8 @@ int sidon_lp_backward(const float* a, const float* saved, const float* b_in, int
     return launch_lp_backward(a, saved, b_in, n, P, p, grad, S(stream));
   if (precision == SIDON_PREC_BF16X1 || precision == SIDON_PREC_BF16X3)
     return launch_lp_backward_tc(a, saved, b_in, n, P, p, grad, precision, S(stream));
+  if (precision == SIDON_PREC_TF32X3)
+    return launch_lp_backward_tf32(a, saved, b_in, n, P, p, grad, S(stream));
   return SIDON_ERR_DTYPE;
 }
 

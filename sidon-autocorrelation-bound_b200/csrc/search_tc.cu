@@ -136,6 +136,7 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
   // the Adam moments of this thread's cells, loaded now so that the
   // correlation phase hides their L2 / HBM latency
   float pm[kCellsPerThread], pv[kCellsPerThread];
+  static_assert(kCellsPerThread % 2 == 0, "the update takes cells in pairs");
   if (mode == 0) {
 #pragma unroll
     for (int u = 0; u < kCellsPerThread; ++u) {
@@ -153,21 +154,23 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
   gather_corr(C, ln, S.cb);                     // G in cb
   SIDON_PHASE(7);
 
-  // Adam / mirror step (cells i = thread + u * NTHREADS)
+  // Adam / mirror step (cells i = thread + u * NTHREADS), two cells at a
+  // time so that their dependent chains (the division and the square root)
+  // interleave; the second cell of the last pair is computed past n from the
+  // zero padding and dropped.  The sum runs in cell order as before.
   float sloc = 0.f;
   const float invR = 1.f / R;
-#pragma unroll
-  for (int u = 0; u < kCellsPerThread; ++u) {
-    const int i = threadIdx.x + u * NTHREADS;
-    if (i >= n) break;          // (a predicated tail would cost all 38 bodies at small n)
+  auto new_height = [&](int u, int i, bool keep) {
     const float gi = S.cb[pidx(i)] * invR - M;
     const float x0 = S.sa[pidx(i)];
     float x;
     if (mode == 0) {
       const float mm = __fmaf_rn(beta1, pm[u], (1.f - beta1) * gi);
       const float vv = __fmaf_rn(beta2, pv[u], (1.f - beta2) * gi * gi);
-      mg[i] = mm;
-      vg[i] = vv;
+      if (keep) {
+        mg[i] = mm;
+        vg[i] = vv;
+      }
       const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
       x = x0 - step;
       if (x < 0.f) x = 0.f;
@@ -177,8 +180,21 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
       if (e < -4.f) e = -4.f;
       x = x0 * __expf(e);
     }
-    S.sa[pidx(i)] = x;
-    sloc += x;
+    return x;
+  };
+#pragma unroll
+  for (int u = 0; u < kCellsPerThread; u += 2) {
+    const int i0 = threadIdx.x + u * NTHREADS, i1 = i0 + NTHREADS;
+    if (i0 >= n) break;         // (a tail predicated over all pairs would cost them all at small n)
+    const bool has1 = i1 < n;
+    const float x0 = new_height(u, i0, true);
+    const float x1 = new_height(u + 1, i1, has1);
+    S.sa[pidx(i0)] = x0;
+    sloc += x0;
+    if (has1) {
+      S.sa[pidx(i1)] = x1;
+      sloc += x1;
+    }
   }
   // renormalise (sum <= 0: the uniform 1/n), chunk by chunk of 8 cells,
   // and write the next step's autoconvolution B copy from the same chunks
@@ -233,7 +249,7 @@ k_local_search_tc(float* pop, float* mom, float* vel, const long long* __restric
                   float pStart, float pEnd, float lrStart, float lrEnd, float beta1, float beta2,
                   int mode_default, int three, unsigned int* status, int ring) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  Shared S = setup(n_max, three != 0, smem_raw, ring);
+  Shared S = setup(n_max, three != 0, smem_raw, ring, true);
   Ctx& C = S.C;
   const Lane ln;
   for (int slot = blockIdx.x; slot < P; slot += gridDim.x) {
@@ -354,7 +370,7 @@ k_local_search_tc_seg(float* pop, float* mom, float* vel, int P, int n,
                       unsigned int* flags, int ring) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ int s_ok;
-  Shared S = setup(n, three != 0, smem_raw, ring);
+  Shared S = setup(n, three != 0, smem_raw, ring, true);
   SIDON_PHASE(15);
   const Lane ln;
   const float lnPr = (float)log((double)pEnd / (double)pStart);
@@ -708,8 +724,12 @@ int set_wait_limit(long long cycles) {
   return e == cudaSuccess ? SIDON_OK : set_cuda_error(e);
 }
 
-size_t smem_local_search_tc(int n) { return tc::Layout(n).total; }
-static size_t smem_local_search_tc(int n, int ring) { return tc::Layout(n, ring).total; }
+// the fused local search's plan (the ring shares its region with cb)
+size_t smem_local_search_tc(int n) { return tc::Layout(n, 0, true).total; }
+static size_t smem_local_search_tc(int n, int ring) { return tc::Layout(n, ring, true).total; }
+// the plan of the other single-CTA tensor-core kernels (G_p pair, the
+// super-block jobs, Frank-Wolfe): cb holds data through their tile phases
+size_t smem_tc_plain(int n) { return tc::Layout(n).total; }
 static size_t smem_lp_forward_tc(int n) { return tc::Layout(n).total; }
 
 // the two accumulators must fit the 512 TMEM columns
@@ -734,8 +754,8 @@ int prepare_local_search_tc(int n_max) {
   if (rc) return rc;
   // the largest plan of any window ring the tuner may pick, for both kernels
   size_t sm = smem_local_search_tc(n_max);
-  int rings[8];
-  const int nr = tc_ring_choices(n_max, rings, 8);
+  int rings[20];
+  const int nr = tc_ring_choices(n_max, rings, 20);
   for (int r = 0; r < nr; ++r) sm = std::max(sm, smem_local_search_tc(n_max, rings[r]));
   rc = prep_tc((const void*)tc::k_local_search_tc, sm);
   if (!rc) rc = prep_tc((const void*)tc::k_local_search_tc_seg, sm);
@@ -871,16 +891,16 @@ int launch_local_search_tc_sched(float* pop, float* mom, float* vel, const long 
 }
 
 // the window ring ring_for picks at n (tiles per stage; 1 = three single-tile stages)
-int tc_ring_default(int n) { return tc::Layout(n).ring.per_stage; }
+int tc_ring_default(int n) { return tc::Layout(n, 0, true).ring.per_stage; }
 
 // the window ring shapes (tiles per stage) the fused kernel can run at n
 // within the shared-memory opt-in, in the tuner's order of trial
 int tc_ring_choices(int n, int* out, int cap) {
-  const tc::Layout auto_lo(n);
+  const tc::Layout auto_lo(n, 0, true);
   int cnt = 0;
-  for (int T = 1; T <= tc::kMaxStageTiles && cnt < cap; ++T) {
+  for (int T = 1; T <= tc::kMaxWideTiles && cnt < cap; ++T) {
     if (T > 1 && auto_lo.m < tc::kRingMinBlocks) break;   // short sequences: single tiles
-    if (tc::Layout(n, T).total <= tc::kSmemBudget) out[cnt++] = T;
+    if (tc::Layout(n, T, true).total <= tc::kSmemBudget) out[cnt++] = T;
   }
   return cnt;
 }
@@ -931,7 +951,7 @@ int launch_lp_backward_tc(const float* a, const float* saved, const float* b_in,
                           double p, float* grad, int precision, cudaStream_t st) {
   int rc = tc_n_ok(n);
   if (rc) return rc;
-  const size_t sm = smem_local_search_tc(n);
+  const size_t sm = smem_tc_plain(n);
   rc = prep_tc((const void*)tc::k_lp_backward_tc, sm);
   if (rc) return rc;
   unsigned int* sw = status_word();

@@ -52,20 +52,70 @@ __host__ __device__ __forceinline__ Ring ring_of(int tiles) {
   return tiles == 1 ? Ring{3, 1} : Ring{2, tiles};
 }
 
+// The widest two-stage ring a plan can hold when the ring shares its space
+// with the scratch cb (the fused local search: cb is dead during both tile
+// phases of a step) and everything else takes `other` bytes.
+constexpr int kMaxWideTiles = 16;
+__host__ __device__ __forceinline__ int wide_tiles(size_t other) {
+  int T = 0;
+  for (int t = 2; t <= kMaxWideTiles; ++t)
+    if (other + 2 * (size_t)stage_bytes(t) <= kSmemBudget) T = t;
+  return T;
+}
+
 // dynamic shared memory plan (byte offsets from a 1 KB aligned base)
+//   wide = false: [ring][copy region][sa][cb][red];
+//   wide = true:  [ring | cb][copy region][sa][red] -- the ring and the
+//   scratch cb share one region, for kernels that use cb only outside tile
+//   phases (the fused local search); the ring then grows to as many tiles
+//   per stage as the budget allows (13 at n = 8400), so a tile phase commits
+//   fewer stages.
 struct Layout {
   int m, rc, rcc, sa_len, cb_len;
   Ring ring;
+  bool wide;
   size_t off_bc, off_sa, off_cb, off_red, total;
-  __host__ __device__ Layout(int n, int ring_tiles = 0) {
+  __host__ __device__ Layout(int n, int ring_tiles = 0, bool wide_plan = false) {
     m = (n + BL - 1) / BL;
     rc = conv_copy_rows(m);
     rcc = corr_copy_rows(m);
     sa_len = 68 * (m + 8);                 // padded heights, 136 cells of margin in front
     cb_len = 68 * (2 * m + 2);             // padded weights / gather scratch
+    wide = wide_plan;
+    if (wide) {
+      const size_t cb_bytes = ((size_t)cb_len * 4 + 1023) & ~(size_t)1023;
+      // as wide as fits, but about five stages per tile phase at least (the
+      // first stage is built before the first MMA; small n keeps five tiles)
+      const int tiles = last_tile(n) / 2 + 1;
+      int T = wide_tiles(place_wide(0));
+      const int want = (tiles + 4) / 5 > kMaxStageTiles ? (tiles + 4) / 5 : kMaxStageTiles;
+      if (T > want) T = want;
+      if (ring_tiles > 0) ring = ring_of(ring_tiles);
+      else if (m >= kRingMinBlocks && T >= 2) ring = Ring{2, T};
+      else ring = ring_for(m, place_wide(cb_bytes));
+      const size_t rb = (size_t)ring.stages * stage_bytes(ring.per_stage);
+      place_wide(rb > cb_bytes ? rb : cb_bytes);
+      return;
+    }
     // the ring takes whole KB: the rest keeps its padding
     ring = ring_tiles > 0 ? ring_of(ring_tiles) : ring_for(m, place(0));
     place((size_t)ring.stages * stage_bytes(ring.per_stage));
+  }
+  // wide plan: cb at the start of a shared region of `o` bytes, the rest after
+  // it; returns the total
+  __host__ __device__ size_t place_wide(size_t o) {
+    off_cb = 0;
+    off_bc = o;
+    const int rows = rcc > rc ? rcc : rc;
+    const size_t region = (size_t)2 * rows * 128;
+    o += region > (size_t)cb_len * 4 ? region : (size_t)cb_len * 4;
+    off_sa = o;
+    o += (size_t)sa_len * 4;
+    o = (o + 15) & ~(size_t)15;
+    off_red = o;
+    o += 64 * 4 + (2 * MAX_STAGES + 6) * 8 + 16;
+    total = o + 1024;
+    return total;
   }
   // lay out everything after a ring of `o` bytes; returns the total
   __host__ __device__ size_t place(size_t o) {
@@ -99,8 +149,8 @@ struct Shared {
 // Per-CTA set-up for candidates of up to n_max cells: buffer addresses,
 // barriers, TMEM.  begin() then prepares one candidate.
 __device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* raw,
-                                        int ring_tiles = 0) {
-  const Layout Lo(n_max, ring_tiles);
+                                        int ring_tiles = 0, bool wide = false) {
+  const Layout Lo(n_max, ring_tiles, wide);
   unsigned char* base = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
   Shared S;
   S.C.stages = base;

@@ -25,6 +25,7 @@ PRECISIONS = {
     "bf16x1": _lib.PREC_BF16X1,
     "bf16x3": _lib.PREC_BF16X3,
     "fp64": _lib.PREC_FP64_SIMT,
+    "tf32x3": _lib.PREC_TF32X3,
 }
 
 

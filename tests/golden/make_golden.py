@@ -1,7 +1,8 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container that has the reference tree (default /root/reference) and
-oracle/_ref built (``make -C oracle ref``):
+Run in a container that has the reference tree (the argument, else
+oracle.REFERENCE_TREE: SIDON_REFERENCE_ROOT or the development checkout) and
+oracle/_ref built (``make -C oracle ref REF=<root>``):
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
 
@@ -111,8 +112,8 @@ def _probe_verify(a: np.ndarray) -> dict:
     }
 
 
-def main(ref_root: str = "/root/reference") -> None:
-    ref = pathlib.Path(ref_root)
+def main(ref_root: str | None = None) -> None:
+    ref = pathlib.Path(ref_root) if ref_root else oracle.REFERENCE_TREE
     if not oracle.have_ref():
         oracle.build()
     spec = importlib.util.spec_from_file_location("ref_verify", ref / "verify.py")

@@ -101,19 +101,21 @@ def test_smem_sizers_are_monotone_and_cover_the_working_set(lib):
     assert lib.sidon_smem_bytes(99, 100, L.F32) == 0
 
 
-def test_tensor_core_plan_fits_the_optin_up_to_9728(lib):
-    """The tcgen05 kernels' shared-memory plan (heights, scratch, B copies and
-    a window ring of as many tiles per stage as fit) stays within the sm_100
-    per-block opt-in (227 KB) at every n of the single-CTA range, and the
-    first n beyond it (9729: one more block) does not fit."""
+def test_tensor_core_plan_fits_the_optin_up_to_9984(lib):
+    """The fused tensor-core local search's shared-memory plan (heights,
+    B copies, and a window ring that shares its region with the scratch)
+    stays within the sm_100 per-block opt-in (227 KB) at every n of its
+    range, which ends where the accumulators fill the 512 TMEM columns and
+    the update's 26 cells per thread run out (n = 9984); the size query
+    reports 0 beyond it."""
     import sidon_b200._lib as L
     optin = 232448
-    sizes = [lib.sidon_smem_bytes(L.OP_LOCAL_SEARCH_TC, n, L.F32) for n in range(1, 9729)]
+    sizes = [lib.sidon_smem_bytes(L.OP_LOCAL_SEARCH_TC, n, L.F32) for n in range(1, 9985)]
     assert all(0 < s <= optin for s in sizes)
     assert max(sizes) > optin - 4096                        # the top of the range uses it
-    assert lib.sidon_smem_bytes(L.OP_LOCAL_SEARCH_TC, 9729, L.F32) > optin
+    assert lib.sidon_smem_bytes(L.OP_LOCAL_SEARCH_TC, 9985, L.F32) == 0
     # the multi-tile ring leaves room for the kernels' static shared variables
-    assert all(s <= optin - 1024 for n, s in enumerate(sizes, 1) if 1024 <= n <= 9216)
+    assert all(s <= optin - 1024 for n, s in enumerate(sizes, 1) if 1024 <= n)
 
 
 def test_formats_roundtrip_with_reference_loadvec(tmp_path):

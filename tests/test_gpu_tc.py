@@ -176,10 +176,11 @@ def test_frank_wolfe_tc_improves_like_simt(cuda):
 
 
 def test_tc_largest_n(cuda):
-    """The top of the single-CTA range (n = 9728: 152 blocks, 512 TMEM
-    columns, all shared memory) runs every tensor-core kernel; one cell more
-    is refused with SIDON_ERR_SMEM (its plan exceeds the shared-memory
-    opt-in, as the SIMT kernels report), and the size query agrees."""
+    """The top of the single-CTA ranges.  n = 9728 (152 blocks, 512 TMEM
+    columns, all shared memory) runs every tensor-core kernel; the fused
+    local search, whose window ring shares its region with the scratch,
+    reaches n = 9984 (26 cells per thread, 512 TMEM columns); one cell more
+    is refused with SIDON_ERR_N, and the size query agrees."""
     from sidon_b200 import synth, _lib
     n = 9728
     a = T(synth.population("structured", n, 2, seed=97), cuda)
@@ -194,11 +195,20 @@ def test_tc_largest_n(cuda):
     F1, _ = K().run_eval(y, with_nactive=False)
     assert bool((F1 <= F0 * (1 + 1e-9)).all())
     assert _status() == 0
-    big = torch.full((1, n + 1), 1.0 / (n + 1), device=cuda)
+    top = 9984
+    pop = synth.population("structured", top, 2, seed=98)
+    z = T(pop, cuda)
+    K().run_local_search(z, 6, 2.0, 16.0, 1e-3, 1e-3, precision="bf16x3")
+    assert _status() == 0
+    Fz, _ = K().run_eval(z, with_nactive=False)
+    Fp, _ = K().run_eval(T(pop, cuda), with_nactive=False)
+    assert bool((Fz < Fp).all())
+    assert bool((z >= 0).all())
+    big = torch.full((1, top + 1), 1.0 / (top + 1), device=cuda)
     with pytest.raises(_lib.SidonError) as ei:
         K().run_local_search(big, 1, 2.0, 4.0, 1e-3, 1e-3, precision="bf16x3")
-    assert ei.value.status == _lib.ERR_SMEM
-    assert K().max_n(_lib.OP_LOCAL_SEARCH_TC) == n
+    assert ei.value.status == _lib.ERR_N
+    assert K().max_n(_lib.OP_LOCAL_SEARCH_TC) == top
 
 
 @pytest.mark.parametrize("iters", [1, 7, 30])
