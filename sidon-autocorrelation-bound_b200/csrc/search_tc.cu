@@ -17,6 +17,8 @@
 // ---------------------------------------------------------------------------
 #include <algorithm>
 #include <mutex>
+#include <utility>
+#include <vector>
 
 #include "conv_simt.cuh"
 #include "tc_cta.cuh"
@@ -763,6 +765,26 @@ int prepare_local_search_tc(int n_max) {
   return status_word() ? SIDON_OK : SIDON_ERR_CUDA;
 }
 
+// Whether the balanced-segment kernel can run on device dev with sm bytes
+// of dynamic shared memory (cooperative launch supported, at least one
+// resident CTA per SM), looked up once per (device, size): the occupancy
+// query costs more host time than the rest of a launch.
+static bool seg_viable(int dev, size_t sm) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<int, size_t>, bool>> known;
+  std::lock_guard<std::mutex> lock(mu);
+  for (const auto& k : known)
+    if (k.first.first == dev && k.first.second == sm) return k.second;
+  int coop = 0, per_sm = 0;
+  bool ok = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess &&
+            coop &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_local_search_tc_seg,
+                                                          tc::NTHREADS, sm) == cudaSuccess &&
+            per_sm >= 1;
+  known.push_back({{dev, sm}, ok});
+  return ok;
+}
+
 // The balanced-segment kernel, or kNotHere when it does not apply (no
 // cooperative launch on the device, fewer resident CTAs than SMs, or fewer
 // candidates than SMs).  flags: P caller-owned words, zeroed here on the
@@ -775,16 +797,11 @@ static int launch_local_search_tc_seg(float* pop, float* mom, float* vel, int P,
                                       double pE, double lrS, double lrE, double b1, double b2,
                                       int mode_default, int precision, int ring, size_t sm,
                                       unsigned int* sw, unsigned int* flags, cudaStream_t st) {
-  int dev = 0, coop = 0, per_sm = 0;
+  int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return kNotHere;
-  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
-    return kNotHere;
   int rc = set_dyn_smem((const void*)tc::k_local_search_tc_seg, sm);
   if (rc) return rc;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc::k_local_search_tc_seg,
-                                                    tc::NTHREADS, sm) != cudaSuccess ||
-      per_sm < 1)
-    return kNotHere;
+  if (!seg_viable(dev, sm)) return kNotHere;
   const int G = sm_count();
   if (P < G) return kNotHere;
   cudaError_t e = cudaMemsetAsync(flags, 0, (size_t)P * sizeof(unsigned int), st);

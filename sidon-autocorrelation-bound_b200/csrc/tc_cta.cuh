@@ -218,7 +218,7 @@ __device__ __forceinline__ void begin(Shared& S, int n, int n_max) {
 
 // Heights of a candidate (global row a, n cells) into the padded shared
 // layout S.sa.  When the row and its length allow (16-byte aligned start, n
-// a multiple of 4), one thread issues a 1-D bulk copy per 64-cell block
+// a multiple of 4), the lanes of warp 0 issue a 1-D bulk copy per 64-cell block
 // (cp.async.bulk, the TMA engine; this GPU's memory, no multicast) and the
 // CTA waits for the bytes on bar_load -- a wait that ignores the abort flag,
 // as copies in flight must land before the buffer is reused; otherwise
@@ -233,10 +233,11 @@ __device__ __forceinline__ bool load_heights(Shared& S, const float* a, int n,
   if (bulk) {
     fence_async_smem();            // begin()'s stores before the copies' writes
     __syncthreads();
-    if (threadIdx.x == 0) {
-      fence_proxy_async_all();     // rows published to this thread before its copies
-      mbar_arrive_tx(bar, (uint32_t)n * 4u);
-      for (int J = 0; 64 * J < n; ++J) {
+    if (threadIdx.x < 32) {        // warp 0: lane 0 announces the bytes, every lane copies blocks
+      fence_proxy_async_all();     // rows published to this warp before its copies
+      if (threadIdx.x == 0) mbar_arrive_tx(bar, (uint32_t)n * 4u);
+      __syncwarp();
+      for (int J = threadIdx.x; 64 * J < n; J += 32) {
         const int len = n - 64 * J < 64 ? n - 64 * J : 64;
         bulk_load(S.sa + pidx(64 * J), a + 64 * J, (uint32_t)len * 4u, bar);
       }
