@@ -116,6 +116,10 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
         const float4 u1 = *reinterpret_cast<const float4*>(S.cb + pidx(k0) + 4);
         const float bv[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
 #pragma unroll
+        // (lanes beyond 2n-1 read the zeros begin() wrote or what the window
+        // ring, which shares the scratch's region, left there: bf16 pairs of
+        // finite heights, finite as fp32; their weight 0 times (1 + d) adds
+        // exactly 0 to R)
         for (int j = 0; j < 8; ++j) {
           const float d = (bv[j] - M) * invM;
           const float cw = (k0 + j < nb && d > -1.f) ? pow_from_d_fast(d, q) : 0.f;
