@@ -71,9 +71,32 @@ __device__ __forceinline__ T block_sum(T v, T* scratch) {
 // src/kernels.cuh:36-44).  The accurate libdevice exp/log1p are used.
 __device__ __forceinline__ float pow_from_d(float d, float q) { return expf(q * log1pf(d)); }
 __device__ __forceinline__ double pow_from_d(double d, double q) { return exp(q * log1p(d)); }
-// Search-time weights of the tensor-core kernels: the reference's own form,
-// __expf(q * log1pf(d)) (src/kernels.cuh:43); log1pf keeps d near 0 exact.
-__device__ __forceinline__ float pow_from_d_fast(float d, float q) { return __expf(q * log1pf(d)); }
+// log1p(d) for d in (-1, 0] (and small positive d) with the digits of d
+// kept near 0: for d >= -1/4 the odd series of 2 atanh(s), s = d / (2 + d),
+// |s| <= 1/7, to s^9 (truncation below 4e-10; with fp32 operations 1.5e-7
+// relative at most, checked against fp64 log1p, plus 2 ulp of the fast
+// division), below it log(1 + d), whose argument then lies in (0, 3/4]
+// (absolute error of __logf about 4e-7 there).
+__device__ __forceinline__ float log1p_nonpos(float d) {
+  if (d >= -0.25f) {
+    const float s = __fdividef(d, 2.f + d), s2 = s * s;
+    float t = fmaf(s2, 1.f / 9.f, 1.f / 7.f);
+    t = fmaf(s2, t, 1.f / 5.f);
+    t = fmaf(s2, t, 1.f / 3.f);
+    return 2.f * fmaf(s * s2, t, s);
+  }
+  return __logf(1.f + d);
+}
+// Search-time weights of the tensor-core kernels: (1 + d)^q = exp(q
+// log1p(d)) as in the reference's form __expf(q * log1pf(d))
+// (src/kernels.cuh:43), with log1p_nonpos for log1pf (the libdevice log1pf
+// took two thirds of the weights phase) and exact zeros without evaluation
+// where q d < -110: there q log1p(d) <= q d < -110, so the power lies below
+// 2^-158 and its fp32 value is 0 either way.
+__device__ __forceinline__ float pow_from_d_fast(float d, float q) {
+  if (q * d < -110.f) return 0.f;
+  return __expf(q * log1p_nonpos(d));
+}
 __device__ __forceinline__ float dev_exp(float x) { return expf(x); }
 __device__ __forceinline__ double dev_exp(double x) { return exp(x); }
 __device__ __forceinline__ float dev_sqrt(float x) { return sqrtf(x); }

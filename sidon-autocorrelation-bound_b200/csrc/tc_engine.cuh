@@ -124,6 +124,28 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "r"(smem_u32(bar))
                : "memory");
 }
+// the same, issued by the calling thread when `issuer` is non-zero (the
+// calling warp stays converged)
+__device__ __forceinline__ void mma_bf16_by(uint32_t issuer, uint32_t dtmem, uint64_t adesc,
+                                            uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "setp.ne.b32 q, %5, 0;\n\t"
+      "@q tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(issuer)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit_by(uint32_t issuer, uint64_t* bar) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\t"
+      "setp.ne.b32 q, %1, 0;\n\t"
+      "@q tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n"
+      :
+      : "r"(smem_u32(bar)), "r"(issuer)
+      : "memory");
+}
 __device__ __forceinline__ void fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -464,8 +486,8 @@ __device__ __forceinline__ void zero_acc(Ctx& C, int col0, int ncols) {
   tmem_wait_st();
 }
 
-// Tile geometry: accumulator column dcol (multiple of DG), B descriptor start
-// row x0 in the class copy (multiple of 8), width N (multiple of 16).
+// Tile geometry (the TF32 kernels): accumulator column dcol (multiple of
+// DG), B descriptor start row x0 in the copy, width N (multiple of 16).
 struct Tile {
   int dcol, x0, N;
 };
@@ -483,31 +505,23 @@ __device__ __forceinline__ int col_corr(int m) { return conv_width(m); }
 //             (hi | lo, one slot), 3 products.
 enum TileMode { CONV_SYM = 0, CONV_X = 1, CORR = 2 };
 
-// Issue the MMAs of one tile (one thread): tile h of stage st of a ring of
-// ts-tile stages.  three_prod selects the 3-product arithmetic, otherwise the
-// 2-product symmetric convolution.
-__device__ __forceinline__ void issue_tile(Ctx& C, int st, int ts, int h, uint32_t b_hi,
-                                           uint32_t b_lo, uint32_t b_lbo_bytes, const Tile& T,
-                                           bool three_prod) {
-  const uint32_t a_hi = smem_u32(C.stages + st * stage_bytes(ts)) + (uint32_t)h * 16u * 128u;
-  const uint32_t a_lo = a_hi + (uint32_t)stage_plane_bytes(ts);
-  const uint32_t bh0 = b_hi + 16u * (uint32_t)T.x0;
-  const uint32_t bl0 = b_lo + 16u * (uint32_t)T.x0;
-  const uint32_t id = idesc_bf16(T.N);
-  const uint32_t d = C.tmem + (uint32_t)T.dcol;
+// Issue the MMAs of one tile: A descriptors ah / al (window hi / lo planes
+// at K step 0), B descriptors bh / bl (copy hi / lo planes at the tile's
+// first row), bstep = the B advance of one K16 step (16-byte units).  Called
+// by the whole MMA warp with warp-uniform operands; `issuer` (lane 0) issues.
+// three_prod selects the 3-product arithmetic, otherwise the 2-product
+// symmetric convolution.
+__device__ __forceinline__ void issue_tile(uint32_t issuer, uint32_t d, uint32_t id, uint64_t ah,
+                                           uint64_t al, uint64_t bh, uint64_t bl, uint64_t bstep,
+                                           bool three, bool three_prod) {
 #pragma unroll
   for (int kc = 0; kc < KSTEPS; ++kc) {
-    // K16 step kc = K groups 2kc, 2kc+1
-    const uint64_t ah = sdesc(a_hi + kc * 256, 128, 128);
-    const uint64_t bh = sdesc(bh0 + 2u * kc * b_lbo_bytes, b_lbo_bytes, 128);
-    mma_bf16(d, ah, bh, id, 1u);
-    if (C.three) {
-      const uint64_t al = sdesc(a_lo + kc * 256, 128, 128);
-      mma_bf16(d, al, bh, id, 1u);
-      if (three_prod) {
-        const uint64_t bl = sdesc(bl0 + 2u * kc * b_lbo_bytes, b_lbo_bytes, 128);
-        mma_bf16(d, ah, bl, id, 1u);
-      }
+    // K16 step kc = K groups 2kc, 2kc+1: A moves by 256 B, B by two K groups
+    const uint64_t a = ah + (uint64_t)(16 * kc), b = bh + bstep * (uint64_t)kc;
+    mma_bf16_by(issuer, d, a, b, id, 1u);
+    if (three) {
+      mma_bf16_by(issuer, d, al + (uint64_t)(16 * kc), b, id, 1u);
+      if (three_prod) mma_bf16_by(issuer, d, a, bl + bstep * (uint64_t)kc, id, 1u);
     }
   }
 }
@@ -541,32 +555,44 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
   int st = C.st_next;
   if (warp == MMA_WARP) {
     if (lane == 0) {
+      // Descriptors advance by additions (addresses below 256 KB: the
+      // 14-bit address field never carries).
+      const uint32_t issuer = 1u;
       fence_after();
-      const int cb_cols = corr_n(m);
       bool ok = wait_phase(C, &C.bc_full[0], C.bc_ph & 1u, status);
       C.bc_ph ^= 1u;
       const uint32_t bbase = smem_u32(C.bc);
-      const uint32_t blo = bbase + (uint32_t)rows * 128u;
-      auto tile_of = [&](int w) {
-        Tile T;
-        if (corr) {
-          T.dcol = col_corr(m);
-          T.x0 = w;
-          T.N = cb_cols;
-        } else {
-          const int off = (w / DG) * DG, t = off - w;
-          T.dcol = COL_CONV + off;
-          T.x0 = t + ZP;
-          T.N = round_up(m - t, 16);
-        }
-        return T;
-      };
+      const uint64_t bh0 = sdesc(bbase, lbo, 128);
+      const uint64_t bl0 = sdesc(bbase + (uint32_t)rows * 128u, lbo, 128);
+      const uint64_t bstep = (uint64_t)((2u * lbo) >> 4);
+      const uint64_t a0 = sdesc(smem_u32(C.stages), 128, 128);
+      const uint64_t sstep = (uint64_t)(stage_bytes(wps) >> 4);
+      const uint64_t aplane = (uint64_t)(stage_plane_bytes(wps) >> 4);
+      const uint32_t id0 = idesc_bf16(0);
+      const bool three = C.three;
       for (int w = 0; ok && w <= C.dmax; w += 2 * wps) {
         if (!wait_phase(C, &C.full[st], (C.ph >> st) & 1u, status)) { ok = false; break; }
         C.ph ^= 1u << st;
         fence_after();
-        for (int h = 0; h < wps && w + 2 * h <= C.dmax; ++h)
-          issue_tile(C, st, wps, h, bbase, blo, lbo, tile_of(w + 2 * h), three_prod);
+        uint64_t ah = a0 + sstep * (uint64_t)st;
+        const int hn = (C.dmax - w) / 2 + 1;
+        for (int h = 0; h < wps && h < hn; ++h, ah += 128) {
+          // tile v = w + 2h: accumulator columns from dcol, B rows from x0
+          const int v = w + 2 * h;
+          int dcol, x0, N;
+          if (corr) {
+            dcol = col_corr(m);
+            x0 = v;
+            N = corr_n(m);
+          } else {
+            const int off = v & ~(DG - 1), t = off - v;
+            dcol = COL_CONV + off;
+            x0 = t + ZP;
+            N = round_up(m - t, 16);
+          }
+          issue_tile(issuer, C.tmem + (uint32_t)dcol, id0 | ((uint32_t)(N >> 3) << 17), ah,
+                     ah + aplane, bh0 + (uint64_t)x0, bl0 + (uint64_t)x0, bstep, three, three_prod);
+        }
         mma_commit(&C.empty[st]);
         st = (st + 1 == nst) ? 0 : st + 1;
       }
@@ -675,24 +701,31 @@ __device__ __forceinline__ float gather_conv(Ctx& C, const Lane& ln, float* X) {
   const int cmid = 32 * mid;                            // first lower column of the rest
   const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)COL_CONV;
   const bool upper = ln.quad >= 2;
+  // cell (r, col) holds a part of k = 64 (col + sh) + rr, at X[68 (col + sh) + rr];
+  // k < nb up to column kcol.  A chunk's 32 cells sit 68 floats apart, so
+  // each store takes a fixed offset from the chunk's base.
+  const int rr = ln.r & 63, sh = ln.r >> 6;
+  const int kcol = ((nb - 1 - rr) >> 6) - sh;
+  const int xr = 68 * sh + rr;
   float mloc = 0.f;
-  // round 1: the first cell of every k (cell (r, col): k = 64 col + r)
+  // round 1: the first cell of every k
   if (upper) {
     if (ln.sub == 0) X[pidx(ln.r - 64)] = 0.f;          // k < 64: one cell only
+    const int hi = kcol < cmid - 2 ? kcol : cmid - 2;   // the upper cell comes first below cmid - 1
     for_chunks(lanebase, ln.sub, 0, mid, [&](int c, const float (&v)[32], int o) {
+      float* xc = X + (xr + 68 * 32 * c);
+      const int th = hi - 32 * c;
 #pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int col = 32 * c + t, k = 64 * col + ln.r;
-        if (col + 1 < cmid && k < nb) X[pidx(k)] = v[o + t];
-      }
+      for (int t = 0; t < 32; ++t)
+        if (t <= th) xc[68 * t] = v[o + t];
     });
   } else {
     for_chunks(lanebase, ln.sub, mid, nch, [&](int c, const float (&v)[32], int o) {
+      float* xc = X + (xr + 68 * 32 * c);
+      const int th = kcol - 32 * c;
 #pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int k = 64 * (32 * c + t) + ln.r;
-        if (k < nb) X[pidx(k)] = v[o + t];
-      }
+      for (int t = 0; t < 32; ++t)
+        if (t <= th) xc[68 * t] = v[o + t];
     });
   }
   __syncthreads();
@@ -701,27 +734,27 @@ __device__ __forceinline__ float gather_conv(Ctx& C, const Lane& ln, float* X) {
   if (upper) {
     if (64 * cmid < nb)
       for_chunks(lanebase, ln.sub, mid - 1, nch, [&](int c, const float (&v)[32], int o) {
+        float* xc = X + (xr + 68 * 32 * c);
+        const int tl = cmid - 1 - 32 * c, th = kcol - 32 * c;
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
-          const int col = 32 * c + t, k = 64 * col + ln.r;
-          if (col + 1 >= cmid && k < nb) {
-            const float b = X[pidx(k)] + v[o + t];
-            X[pidx(k)] = b;
+        for (int t = 0; t < 32; ++t)
+          if (t >= tl && t <= th) {
+            const float b = xc[68 * t] + v[o + t];
+            xc[68 * t] = b;
             mloc = fmaxf(mloc, b);
           }
-        }
       });
   } else {
     for_chunks(lanebase, ln.sub, 0, mid, [&](int c, const float (&v)[32], int o) {
+      float* xc = X + (xr + 68 * 32 * c);
+      const int th = kcol - 32 * c;
 #pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int k = 64 * (32 * c + t) + ln.r;
-        if (k < nb) {
-          const float b = X[pidx(k)] + v[o + t];
-          X[pidx(k)] = b;
+      for (int t = 0; t < 32; ++t)
+        if (t <= th) {
+          const float b = xc[68 * t] + v[o + t];
+          xc[68 * t] = b;
           mloc = fmaxf(mloc, b);
         }
-      }
     });
   }
   __syncthreads();
@@ -742,41 +775,48 @@ __device__ __forceinline__ void gather_corr(Ctx& C, const Lane& ln, float* Y) {
   const int mid = nch / 2, cmid = 32 * mid;
   const uint32_t lanebase = C.tmem + ((uint32_t)(32 * ln.quad) << 16) + (uint32_t)col_corr(C.m);
   const bool upper = ln.quad >= 2;
+  // cell (r, col) holds a part of i = 64 (col - sh) + ri, at Y[68 (col - sh) + ri];
+  // 0 <= i < n for columns sh .. icol
+  const int ri = 63 - (ln.r & 63), sh = ln.r >> 6;
+  const int icol = ((n - 1 - ri) >> 6) + sh;
+  const int yr = ri - 68 * sh;
   // round 1: lower cells of columns < cmid, upper cells of columns > cmid
   if (upper) {
+    const int lo = cmid + 1;
     for_chunks(lanebase, ln.sub, mid, nch, [&](int c, const float (&v)[32], int o) {
+      const int yc = yr + 68 * 32 * c;
+      const int tl = lo - 32 * c, th = icol - 32 * c;
 #pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int col = 32 * c + t, i = 64 * col + 63 - ln.r;
-        if (col > cmid && i < n) Y[pidx(i)] = v[o + t];
-      }
+      for (int t = 0; t < 32; ++t)
+        if (t >= tl && t <= th) Y[yc + 68 * t] = v[o + t];
     });
   } else {
     for_chunks(lanebase, ln.sub, 0, mid, [&](int c, const float (&v)[32], int o) {
+      const int yc = yr + 68 * 32 * c;
+      const int th = icol - 32 * c;
 #pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int i = 64 * (32 * c + t) + 63 - ln.r;
-        if (i < n) Y[pidx(i)] = v[o + t];
-      }
+      for (int t = 0; t < 32; ++t)
+        if (t <= th) Y[yc + 68 * t] = v[o + t];
     });
   }
   __syncthreads();
   // round 2: the partner cells, added
   if (upper) {
+    const int hi = icol < cmid ? icol : cmid;
     for_chunks(lanebase, ln.sub, 0, mid < nch ? mid + 1 : nch, [&](int c, const float (&v)[32], int o) {
+      const int yc = yr + 68 * 32 * c;
+      const int tl = sh - 32 * c, th = hi - 32 * c;
 #pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int col = 32 * c + t, i = 64 * col + 63 - ln.r;
-        if (col <= cmid && i >= 0 && i < n) Y[pidx(i)] += v[o + t];
-      }
+      for (int t = 0; t < 32; ++t)
+        if (t >= tl && t <= th) Y[yc + 68 * t] += v[o + t];
     });
   } else {
     for_chunks(lanebase, ln.sub, mid, nch, [&](int c, const float (&v)[32], int o) {
+      const int yc = yr + 68 * 32 * c;
+      const int th = icol - 32 * c;
 #pragma unroll
-      for (int t = 0; t < 32; ++t) {
-        const int i = 64 * (32 * c + t) + 63 - ln.r;
-        if (i < n) Y[pidx(i)] += v[o + t];
-      }
+      for (int t = 0; t < 32; ++t)
+        if (t <= th) Y[yc + 68 * t] += v[o + t];
     });
   }
   __syncthreads();
