@@ -72,30 +72,30 @@ __device__ __forceinline__ T block_sum(T v, T* scratch) {
 __device__ __forceinline__ float pow_from_d(float d, float q) { return expf(q * log1pf(d)); }
 __device__ __forceinline__ double pow_from_d(double d, double q) { return exp(q * log1p(d)); }
 // log1p(d) for d in (-1, 0] (and small positive d) with the digits of d
-// kept near 0: for d >= -1/4 the odd series of 2 atanh(s), s = d / (2 + d),
-// |s| <= 1/7, to s^9 (truncation below 4e-10; with fp32 operations 1.5e-7
-// relative at most, checked against fp64 log1p, plus 2 ulp of the fast
-// division), below it log(1 + d), whose argument then lies in (0, 3/4]
-// (absolute error of __logf about 4e-7 there).
+// kept near 0: the Taylor series to d^8 for d >= -1/16 (fp32 Horner: 6.2e-8
+// relative at most, checked against fp64 log1p), __logf(1 + d) below
+// (absolute error about 4e-7).  Both are evaluated and one is selected:
+// without a branch the weights of a chunk interleave (measured at n = 8400:
+// weights phase 12.8k -> 10.6k cycles against libdevice log1pf).
 __device__ __forceinline__ float log1p_nonpos(float d) {
-  if (d >= -0.25f) {
-    const float s = __fdividef(d, 2.f + d), s2 = s * s;
-    float t = fmaf(s2, 1.f / 9.f, 1.f / 7.f);
-    t = fmaf(s2, t, 1.f / 5.f);
-    t = fmaf(s2, t, 1.f / 3.f);
-    return 2.f * fmaf(s * s2, t, s);
-  }
-  return __logf(1.f + d);
+  float t = fmaf(d, -1.f / 8.f, 1.f / 7.f);
+  t = fmaf(d, t, -1.f / 6.f);
+  t = fmaf(d, t, 1.f / 5.f);
+  t = fmaf(d, t, -1.f / 4.f);
+  t = fmaf(d, t, 1.f / 3.f);
+  t = fmaf(d, t, -1.f / 2.f);
+  const float series = fmaf(d * d, t, d);
+  const float lg = __logf(1.f + d);
+  return d >= -0.0625f ? series : lg;
 }
 // Search-time weights of the tensor-core kernels: (1 + d)^q = exp(q
 // log1p(d)) as in the reference's form __expf(q * log1pf(d))
-// (src/kernels.cuh:43), with log1p_nonpos for log1pf (the libdevice log1pf
-// took two thirds of the weights phase) and exact zeros without evaluation
-// where q d < -110: there q log1p(d) <= q d < -110, so the power lies below
-// 2^-158 and its fp32 value is 0 either way.
+// (src/kernels.cuh:43), with log1p_nonpos for log1pf, and 0 where
+// q d < -110: there q log1p(d) <= q d < -110, the power lies below 2^-158
+// and its fp32 value is 0 either way.
 __device__ __forceinline__ float pow_from_d_fast(float d, float q) {
-  if (q * d < -110.f) return 0.f;
-  return __expf(q * log1p_nonpos(d));
+  const float w = __expf(q * log1p_nonpos(d));
+  return q * d < -110.f ? 0.f : w;
 }
 __device__ __forceinline__ float dev_exp(float x) { return expf(x); }
 __device__ __forceinline__ double dev_exp(double x) { return exp(x); }

@@ -177,7 +177,8 @@ __device__ __forceinline__ int lp_adam_step(Shared& S, const Lane& ln, int n, in
         mg[i] = mm;
         vg[i] = vv;
       }
-      const float step = lrn * (mm * bc1) / (sqrtf(vv * bc2) + 1e-30f);
+      // (fast division: 2 ulp; the denominator lies in [1e-30, 2^126])
+      const float step = lrn * __fdividef(mm * bc1, sqrtf(vv * bc2) + 1e-30f);
       x = x0 - step;
       if (x < 0.f) x = 0.f;
     } else {

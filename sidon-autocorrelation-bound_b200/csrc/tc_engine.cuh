@@ -526,11 +526,18 @@ __device__ __forceinline__ void issue_tile(uint32_t issuer, uint32_t d, uint32_t
   }
 }
 
+// Tiles in the first stage of a tile sequence at most: the MMAs start after
+// a short build, and the next, full stage is built while they run
+// (measured at n = 8400 with 13-tile stages: the first full stage kept the
+// tensor pipe waiting about 2k cycles per tile phase).
+constexpr int kLeadTiles = 4;
+
 // Run the tiles w = 0, 2, ..., dmax through the warp-specialised pipeline:
 // the builders write the phase's B copy once (one copy slot), then the
-// windows of wps consecutive tiles into each stage of the ring (one run of
-// core matrices, build_stage); the MMA lane
-// issues a stage's tiles in order and releases the stage with one commit.
+// windows of wps consecutive tiles (the first stage: at most kLeadTiles)
+// into each stage of the ring (one run of core matrices, build_stage); the
+// MMA lane issues a stage's tiles in order and releases the stage with one
+// commit.
 // Every accumulator receives its MMAs in the same order whatever the ring
 // shape, so the results do not depend on it.  Ends with every MMA of the sequence
 // complete (bar_done) and the accumulator readable by all warps.
@@ -570,13 +577,14 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
       const uint64_t aplane = (uint64_t)(stage_plane_bytes(wps) >> 4);
       const uint32_t id0 = idesc_bf16(0);
       const bool three = C.three;
-      for (int w = 0; ok && w <= C.dmax; w += 2 * wps) {
+      int per = wps < kLeadTiles ? wps : kLeadTiles;
+      for (int w = 0; ok && w <= C.dmax; w += 2 * per, per = wps) {
         if (!wait_phase(C, &C.full[st], (C.ph >> st) & 1u, status)) { ok = false; break; }
         C.ph ^= 1u << st;
         fence_after();
         uint64_t ah = a0 + sstep * (uint64_t)st;
         const int hn = (C.dmax - w) / 2 + 1;
-        for (int h = 0; h < wps && h < hn; ++h, ah += 128) {
+        for (int h = 0; h < per && h < hn; ++h, ah += 128) {
           // tile v = w + 2h: accumulator columns from dcol, B rows from x0
           const int v = w + 2 * h;
           int dcol, x0, N;
@@ -617,7 +625,8 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
       __syncwarp();
       if (lane == 0) mbar_arrive(&C.bc_full[0]);
     }
-    for (int w = 0; ok && w <= C.dmax; w += 2 * wps) {
+    int per = wps < kLeadTiles ? wps : kLeadTiles;
+    for (int w = 0; ok && w <= C.dmax; w += 2 * per, per = wps) {
       if ((C.started >> st) & 1u) {
         if (!wait_phase(C, &C.empty[st], (C.ph >> st) & 1u, status)) {
           ok = false;
@@ -627,7 +636,7 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
       }
       C.started |= 1u << st;
       const int nt = (C.dmax - w) / 2 + 1;
-      build_stage(C, st, wps, wsrc, w, nt < wps ? nt : wps, lsc, bt);
+      build_stage(C, st, wps, wsrc, w, nt < per ? nt : per, lsc, bt);
       fence_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&C.full[st]);
