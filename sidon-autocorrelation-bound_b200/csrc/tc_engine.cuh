@@ -231,10 +231,21 @@ __device__ __forceinline__ void split_bf16(float x, uint16_t& hi, uint16_t& lo) 
 __device__ __forceinline__ int pidx(int i) { return i + 4 * (i >> 6); }
 
 // Warp roles during the tile phases: warp MMA_WARP (lane 0) issues every
-// MMA; the other warps build windows and B-matrix copies.
+// MMA; the warps of the other three SM sub-partitions (warp w runs on
+// sub-partition w mod 4) build windows and B-matrix copies, and the other
+// warps of the MMA warp's sub-partition stay idle, so that the issuing
+// thread has that sub-partition's issue slots to itself (measured at
+// n = 8400: tile phases 45.8k / 64.5k -> 43.2k / 62.3k cycles against
+// builders in every warp).  builder_index numbers the builders 0 ..
+// NBUILD - 1, or returns -1.
 constexpr int MMA_WARP = NTHREADS / 32 - 1;
-constexpr int NBUILD_WARPS = NTHREADS / 32 - 1;
+static_assert(MMA_WARP % 4 == 3, "the idle warps are those with w mod 4 == 3");
+constexpr int NBUILD_WARPS = NTHREADS / 32 - NTHREADS / 128;
 constexpr int NBUILD = NBUILD_WARPS * 32;
+__device__ __forceinline__ int builder_index() {
+  const int warp = threadIdx.x >> 5;
+  return (warp & 3) == 3 ? -1 : (warp - (warp >> 2)) * 32 + (int)(threadIdx.x & 31);
+}
 
 // Shared state of one CTA.  Every thread holds a copy; the pipeline counters
 // of a role are kept identical by every thread of that role.
@@ -608,8 +619,8 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
       mma_commit(C.bar_done);
     }
     __syncwarp();
-  } else {
-    const int bt = threadIdx.x - (warp > MMA_WARP ? 32 : 0);   // 0 .. NBUILD-1
+  } else if (builder_index() >= 0) {
+    const int bt = builder_index();   // 0 .. NBUILD-1
     bool ok = true;
     if ((C.bc_started & 1u) && !wait_phase(C, &C.bc_empty[0], C.bc_ph & 1u, status)) ok = false;
     if (C.bc_started & 1u) C.bc_ph ^= 1u;

@@ -264,8 +264,8 @@ __device__ __forceinline__ bool run_tiles(Ctx& C, const float* wsrc, const float
       mma_commit(C.bar_done);
     }
     __syncwarp();
-  } else {
-    const int bt = threadIdx.x - (warp > MMA_WARP ? 32 : 0);
+  } else if (builder_index() >= 0) {
+    const int bt = builder_index();
     bool ok = true;
     if ((C.bc_started & 1u) && !wait_phase(C, &C.bc_empty[0], C.bc_ph & 1u, status)) ok = false;
     if (C.bc_started & 1u) C.bc_ph ^= 1u;
