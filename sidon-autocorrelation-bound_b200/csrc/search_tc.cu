@@ -339,7 +339,7 @@ __device__ __forceinline__ void run_piece(Shared& S, const Lane& ln, float* pop,
   float* vg = vel + (size_t)pid * n;
   SIDON_PHASE(10);
   begin(S, n, n);
-  load_heights(S, a, n, status);
+  load_heights(S, a, n);
   if (s0 == 0) {
     bool bad = false;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -368,8 +368,15 @@ __device__ __forceinline__ void run_piece(Shared& S, const Lane& ln, float* pop,
     if (rs) break;          // M <= 0 stops the anneal; the heights are as they were
   }
   __syncthreads();
-  if (rs != 2)
-    for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = S.sa[pidx(i)];
+  if (rs != 2) {
+    // back to the row, 16-byte groups where the row allows (see load_heights)
+    if (((reinterpret_cast<uintptr_t>(a) & 15) == 0) && (n % 4 == 0)) {
+      for (int q = threadIdx.x; q < n / 4; q += blockDim.x)
+        reinterpret_cast<float4*>(a)[q] = *reinterpret_cast<const float4*>(S.sa + pidx(4 * q));
+    } else {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = S.sa[pidx(i)];
+    }
+  }
   SIDON_PHASE(12);
 }
 

@@ -163,7 +163,7 @@ __device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* ra
   S.C.empty = bars + MAX_STAGES;
   S.C.bc_full = bars + 2 * MAX_STAGES;
   S.C.bc_empty = bars + 2 * MAX_STAGES + 2;
-  S.C.bar_done = bars + 2 * MAX_STAGES + 4;      // bar_done + 1: bulk copies
+  S.C.bar_done = bars + 2 * MAX_STAGES + 4;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * MAX_STAGES + 6);
   S.C.abort = reinterpret_cast<int*>(tslot + 1);
   S.C.m = Lo.m;
@@ -186,10 +186,8 @@ __device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* ra
       mbar_init(&S.C.bc_empty[s], 1);
     }
     mbar_init(S.C.bar_done, 1);
-    mbar_init(S.C.bar_done + 1, 1);
     mbar_fence_init();
     S.C.abort[0] = 0;
-    S.C.abort[1] = 0;                      // parity of the bulk-copy barrier
   }
   if ((threadIdx.x >> 5) == 0) tmem_alloc(tslot, 512);
   fence_before();
@@ -204,10 +202,14 @@ __device__ __forceinline__ Shared setup(int n_max, bool three, unsigned char* ra
 // geometry.  Ends synchronised.
 __device__ __forceinline__ void begin(Shared& S, int n, int n_max) {
   const Layout Lo(n_max), Ln(n);
-  float* z0 = S.sa - 136;
+  // 16-byte stores: both arrays start 16-byte aligned and hold multiples
+  // of 4 floats (3.3k -> 1.1k cycles at n = 8400 against 4-byte stores)
+  float4* z0 = reinterpret_cast<float4*>(S.sa - 136);
+  float4* z1 = reinterpret_cast<float4*>(S.cb);
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
-  for (int i = threadIdx.x; i < Lo.sa_len; i += blockDim.x) z0[i] = 0.f;
-  for (int i = threadIdx.x; i < Lo.cb_len; i += blockDim.x) S.cb[i] = 0.f;
+  for (int i = threadIdx.x; i < Lo.sa_len / 4; i += blockDim.x) z0[i] = z;
+  for (int i = threadIdx.x; i < Lo.cb_len / 4; i += blockDim.x) z1[i] = z;
   S.C.n = n;
   S.C.m = Ln.m;
   S.C.rc = Ln.rc;
@@ -217,39 +219,22 @@ __device__ __forceinline__ void begin(Shared& S, int n, int n_max) {
 }
 
 // Heights of a candidate (global row a, n cells) into the padded shared
-// layout S.sa.  When the row and its length allow (16-byte aligned start, n
-// a multiple of 4), the lanes of warp 0 issue a 1-D bulk copy per 64-cell block
-// (cp.async.bulk, the TMA engine; this GPU's memory, no multicast) and the
-// CTA waits for the bytes on bar_load -- a wait that ignores the abort flag,
-// as copies in flight must land before the buffer is reused; otherwise
-// every thread loads through L2.  begin() must have run (it zeroes the
-// margins; its barrier orders those stores before the copies).  Ends
-// synchronised.  Returns whether the bulk path was taken.
-__device__ __forceinline__ bool load_heights(Shared& S, const float* a, int n,
-                                             unsigned int* status) {
-  uint64_t* bar = S.C.bar_done + 1;
-  volatile int* parity = S.C.abort + 1;
-  const bool bulk = ((reinterpret_cast<uintptr_t>(a) & 15) == 0) && (n % 4 == 0);
-  if (bulk) {
-    fence_async_smem();            // begin()'s stores before the copies' writes
-    __syncthreads();
-    if (threadIdx.x < 32) {        // warp 0: lane 0 announces the bytes, every lane copies blocks
-      fence_proxy_async_all();     // rows published to this warp before its copies
-      if (threadIdx.x == 0) mbar_arrive_tx(bar, (uint32_t)n * 4u);
-      __syncwarp();
-      for (int J = threadIdx.x; 64 * J < n; J += 32) {
-        const int len = n - 64 * J < 64 ? n - 64 * J : 64;
-        bulk_load(S.sa + pidx(64 * J), a + 64 * J, (uint32_t)len * 4u, bar);
-      }
-    }
-    drain_phase(bar, (uint32_t)*parity, status);
-    __syncthreads();
-    if (threadIdx.x == 0) *parity ^= 1;
+// layout S.sa, through L2.  When the row allows (16-byte aligned start, n a
+// multiple of 4) every thread moves 16-byte groups of 4 cells (a group
+// never straddles a 64-cell block, so it lands contiguous in the padded
+// layout).  Measured at n = 8400, per candidate: 3.3k cycles, against 9.2k
+// for 1-D bulk copies (cp.async.bulk, one per 64-cell block from the lanes
+// of one warp, completing on an mbarrier) and about as long for 4-byte
+// loads.  begin() must have run (it zeroes the margins).  Ends synchronised.
+__device__ __forceinline__ void load_heights(Shared& S, const float* a, int n) {
+  if (((reinterpret_cast<uintptr_t>(a) & 15) == 0) && (n % 4 == 0)) {
+#pragma unroll 4
+    for (int q = threadIdx.x; q < n / 4; q += blockDim.x)
+      *reinterpret_cast<float4*>(S.sa + pidx(4 * q)) = __ldcg(reinterpret_cast<const float4*>(a) + q);
   } else {
     for (int i = threadIdx.x; i < n; i += blockDim.x) S.sa[pidx(i)] = __ldcg(a + i);
   }
   __syncthreads();
-  return bulk;
 }
 
 __device__ __forceinline__ void teardown(Shared& S) {

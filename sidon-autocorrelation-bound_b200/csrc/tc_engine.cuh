@@ -256,8 +256,7 @@ struct Ctx {
   uint64_t* empty;         // nst "windows consumed" barriers (tcgen05.commit)
   uint64_t* bc_full;       // "copy ready" barrier (NBUILD_WARPS arrivals; [0] used)
   uint64_t* bc_empty;      // "copy consumed" barrier (tcgen05.commit; [0] used)
-  uint64_t* bar_done;      // "all MMAs of a phase done" (the next barrier,
-                           // bar_done + 1, counts the bytes of bulk copies)
+  uint64_t* bar_done;      // "all MMAs of a phase done"
   uint32_t tmem;           // TMEM base address (512 columns)
   // pipeline phases as bit masks (registers, no dynamic indexing): bit s of
   // ph = parity of this thread's next wait on stage s (full for the MMA
@@ -267,8 +266,7 @@ struct Ctx {
   uint32_t ph, started, bc_ph, bc_started, done_ph;
   int st_next;             // next stage in the ring
   int nst, wps;            // ring shape: stages, tiles per stage
-  int* abort;              // shared abort flag (the next word: the parity of
-                           // the bulk-copy barrier's next phase)
+  int* abort;              // shared abort flag
   int m, rc, rcc, n, dmax; // blocks, conv / corr copy rows, cells, last tile
   bool three;              // BF16x3 (else BF16x1)
 };
@@ -318,29 +316,6 @@ __device__ __forceinline__ bool drain_phase(uint64_t* bar, uint32_t parity, unsi
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// ---- 1-D bulk copies (TMA engine, no tensor map, no multicast) ----
-// Global -> this CTA's shared memory, completing on `bar` by byte count.
-// dst, src and bytes must be multiples of 16.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
-                                          uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-      :
-      : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-// the issuing thread's arrival on `bar`, announcing `bytes` of bulk copies
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-// order this thread's earlier generic-proxy accesses before later
-// async-proxy (bulk copy) accesses
-__device__ __forceinline__ void fence_proxy_async_all() {
-  asm volatile("fence.proxy.async;" ::: "memory");
 }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float first, float second) {

@@ -133,10 +133,8 @@ __device__ __forceinline__ Shared setup(int n, unsigned char* raw) {
       mbar_init(&S.C.bc_empty[s], 1);
     }
     mbar_init(S.C.bar_done, 1);
-    mbar_init(S.C.bar_done + 1, 1);
     mbar_fence_init();
     S.C.abort[0] = 0;
-    S.C.abort[1] = 0;
   }
   if ((threadIdx.x >> 5) == 0) tmem_alloc(tslot, 512);
   fence_before();
