@@ -282,19 +282,23 @@ __host__ __device__ __forceinline__ int corr_width(int m) { return round_up(corr
 // another thread has aborted, or after the device state's wait limit
 // (sidon_set_wait_limit), in which case it records SIDON_ERR_TIMEOUT and sets
 // the abort flag.
-__device__ __forceinline__ bool wait_phase(Ctx& C, uint64_t* bar, uint32_t parity,
-                                           unsigned int* status) {
+__device__ __forceinline__ bool wait_bar(int* abort, uint64_t* bar, uint32_t parity,
+                                         unsigned int* status) {
   if (mbar_try(bar, parity)) return true;
   const long long t0 = clock64(), lim = wait_limit(status);
   while (!mbar_try(bar, parity)) {
-    if (*((volatile int*)C.abort)) return false;
+    if (*((volatile int*)abort)) return false;
     if (clock64() - t0 > lim) {
-      atomicExch(C.abort, 1);
+      atomicExch(abort, 1);
       atomicCAS(status, 0u, (unsigned int)SIDON_ERR_TIMEOUT);
       return false;
     }
   }
   return true;
+}
+__device__ __forceinline__ bool wait_phase(Ctx& C, uint64_t* bar, uint32_t parity,
+                                           unsigned int* status) {
+  return wait_bar(C.abort, bar, parity, status);
 }
 
 // The end-of-phase wait for the MMA lane's final commit.  It must see every
@@ -518,6 +522,79 @@ __device__ __forceinline__ void issue_tile(uint32_t issuer, uint32_t d, uint32_t
 // tensor pipe waiting about 2k cycles per tile phase).
 constexpr int kLeadTiles = 4;
 
+
+// The MMA lane's part of a tile phase (run_tiles_ring): wait for the copy,
+// then per stage wait for its windows, issue its tiles' MMAs and release it
+// with one commit; finally commit the copy slot and bar_done.  A function of
+// its own, not inlined, so that the issue loop is compiled apart from the
+// kernel around it: inlined, its rate moved with unrelated changes
+// elsewhere in the step (the convolution tile phase at n = 8400 measured
+// 43.2k and 46.4k cycles in two builds that differed only in how begin()
+// zeroes shared memory; 43.4k as a function).  Descriptors advance by
+// additions (addresses below 256 KB: the 14-bit address field never
+// carries).  Returns the ring position and the stage parities after the
+// phase.
+struct IssueArgs {
+  uint64_t *full, *empty, *bc_full, *bc_empty, *bar_done;
+  int* abort;
+  unsigned int* status;
+  uint32_t tmem, stages, bc;
+  int rows, m, dmax, wps, nst, st;
+  uint32_t ph, bc_ph;
+  int three;
+};
+struct IssueRes {
+  int st;
+  uint32_t ph;
+};
+template <bool CORR, bool THREE_PROD>
+__device__ __noinline__ IssueRes issue_phase(const IssueArgs A) {
+  const uint32_t issuer = 1u;
+  const uint32_t lbo = b_lbo(A.rows);
+  int st = A.st;
+  uint32_t ph = A.ph;
+  fence_after();
+  bool ok = wait_bar(A.abort, &A.bc_full[0], A.bc_ph & 1u, A.status);
+  const uint64_t bh0 = sdesc(A.bc, lbo, 128);
+  const uint64_t bl0 = sdesc(A.bc + (uint32_t)A.rows * 128u, lbo, 128);
+  const uint64_t bstep = (uint64_t)((2u * lbo) >> 4);
+  const uint64_t a0 = sdesc(A.stages, 128, 128);
+  const uint64_t sstep = (uint64_t)(stage_bytes(A.wps) >> 4);
+  const uint64_t aplane = (uint64_t)(stage_plane_bytes(A.wps) >> 4);
+  const uint32_t id0 = idesc_bf16(0);
+  const bool three = A.three != 0;
+  const int m = A.m;
+  int per = A.wps < kLeadTiles ? A.wps : kLeadTiles;
+  for (int w = 0; ok && w <= A.dmax; w += 2 * per, per = A.wps) {
+    if (!wait_bar(A.abort, &A.full[st], (ph >> st) & 1u, A.status)) { ok = false; break; }
+    ph ^= 1u << st;
+    fence_after();
+    uint64_t ah = a0 + sstep * (uint64_t)st;
+    const int hn = (A.dmax - w) / 2 + 1;
+    for (int h = 0; h < per && h < hn; ++h, ah += 128) {
+      const int v = w + 2 * h;
+      int dcol, x0, N;
+      if (CORR) {
+        dcol = col_corr(m);
+        x0 = v;
+        N = corr_n(m);
+      } else {
+        const int off = v & ~(DG - 1), t = off - v;
+        dcol = COL_CONV + off;
+        x0 = t + ZP;
+        N = round_up(m - t, 16);
+      }
+      issue_tile(issuer, A.tmem + (uint32_t)dcol, id0 | ((uint32_t)(N >> 3) << 17), ah,
+                 ah + aplane, bh0 + (uint64_t)x0, bl0 + (uint64_t)x0, bstep, three, THREE_PROD);
+    }
+    mma_commit(&A.empty[st]);
+    st = (st + 1 == A.nst) ? 0 : st + 1;
+  }
+  mma_commit(&A.bc_empty[0]);
+  mma_commit(A.bar_done);
+  return IssueRes{st, ph};
+}
+
 // Run the tiles w = 0, 2, ..., dmax through the warp-specialised pipeline:
 // the builders write the phase's B copy once (one copy slot), then the
 // windows of wps consecutive tiles (the first stage: at most kLeadTiles)
@@ -548,50 +625,16 @@ __device__ __forceinline__ bool run_tiles_ring(Ctx& C, const float* wsrc, const 
   int st = C.st_next;
   if (warp == MMA_WARP) {
     if (lane == 0) {
-      // Descriptors advance by additions (addresses below 256 KB: the
-      // 14-bit address field never carries).
-      const uint32_t issuer = 1u;
-      fence_after();
-      bool ok = wait_phase(C, &C.bc_full[0], C.bc_ph & 1u, status);
+      IssueArgs A;
+      A.full = C.full; A.empty = C.empty; A.bc_full = C.bc_full; A.bc_empty = C.bc_empty;
+      A.bar_done = C.bar_done; A.abort = C.abort; A.status = status;
+      A.tmem = C.tmem; A.stages = smem_u32(C.stages); A.bc = smem_u32(C.bc);
+      A.rows = rows; A.m = m; A.dmax = C.dmax; A.wps = wps; A.nst = nst; A.st = st;
+      A.ph = C.ph; A.bc_ph = C.bc_ph; A.three = C.three ? 1 : 0;
+      const IssueRes R = issue_phase<corr, three_prod>(A);
+      st = R.st;
+      C.ph = R.ph;
       C.bc_ph ^= 1u;
-      const uint32_t bbase = smem_u32(C.bc);
-      const uint64_t bh0 = sdesc(bbase, lbo, 128);
-      const uint64_t bl0 = sdesc(bbase + (uint32_t)rows * 128u, lbo, 128);
-      const uint64_t bstep = (uint64_t)((2u * lbo) >> 4);
-      const uint64_t a0 = sdesc(smem_u32(C.stages), 128, 128);
-      const uint64_t sstep = (uint64_t)(stage_bytes(wps) >> 4);
-      const uint64_t aplane = (uint64_t)(stage_plane_bytes(wps) >> 4);
-      const uint32_t id0 = idesc_bf16(0);
-      const bool three = C.three;
-      int per = wps < kLeadTiles ? wps : kLeadTiles;
-      for (int w = 0; ok && w <= C.dmax; w += 2 * per, per = wps) {
-        if (!wait_phase(C, &C.full[st], (C.ph >> st) & 1u, status)) { ok = false; break; }
-        C.ph ^= 1u << st;
-        fence_after();
-        uint64_t ah = a0 + sstep * (uint64_t)st;
-        const int hn = (C.dmax - w) / 2 + 1;
-        for (int h = 0; h < per && h < hn; ++h, ah += 128) {
-          // tile v = w + 2h: accumulator columns from dcol, B rows from x0
-          const int v = w + 2 * h;
-          int dcol, x0, N;
-          if (corr) {
-            dcol = col_corr(m);
-            x0 = v;
-            N = corr_n(m);
-          } else {
-            const int off = v & ~(DG - 1), t = off - v;
-            dcol = COL_CONV + off;
-            x0 = t + ZP;
-            N = round_up(m - t, 16);
-          }
-          issue_tile(issuer, C.tmem + (uint32_t)dcol, id0 | ((uint32_t)(N >> 3) << 17), ah,
-                     ah + aplane, bh0 + (uint64_t)x0, bl0 + (uint64_t)x0, bstep, three, three_prod);
-        }
-        mma_commit(&C.empty[st]);
-        st = (st + 1 == nst) ? 0 : st + 1;
-      }
-      mma_commit(&C.bc_empty[0]);
-      mma_commit(C.bar_done);
     }
     __syncwarp();
   } else if (builder_index() >= 0) {
