@@ -27,10 +27,11 @@ REF_PROBE = REF_DIR / "libref_probe.so"
 REF_MAIN = REF_DIR / "libref_main.so"
 REF_PROBE_EXE = REF_DIR / "probe"
 # Where the reference project's sources lie, for building oracle/_ref: the
-# SIDON_REFERENCE_ROOT environment variable, else the reference checkout of the
-# development container this checker was written in.  Machines without it
-# (the GPU boxes) use the oracle/_ref built beforehand.
-REFERENCE_TREE = pathlib.Path(os.environ.get("SIDON_REFERENCE_ROOT") or "/root/reference")
+# SIDON_REFERENCE_ROOT environment variable, or the root given to build().
+# Machines without the reference (the GPU boxes) use the oracle/_ref built
+# beforehand.
+_env_root = os.environ.get("SIDON_REFERENCE_ROOT")
+REFERENCE_TREE = pathlib.Path(_env_root) if _env_root else None
 
 _vp, _i, _d, _f = C.c_void_p, C.c_int, C.c_double, C.c_float
 _LD = C.c_longdouble
@@ -75,11 +76,13 @@ _probe = None
 _main = None
 
 
-def build() -> None:
-    """Build the C restatement (and oracle/_ref when the reference tree exists)."""
+def build(reference_root=None) -> None:
+    """Build the C restatement, and oracle/_ref when a reference tree is given
+    (reference_root, else SIDON_REFERENCE_ROOT) and present."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
-    if (REFERENCE_TREE / "src").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REFERENCE_TREE}"],
+    root = pathlib.Path(reference_root) if reference_root else REFERENCE_TREE
+    if root is not None and (root / "src").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={root}"],
                        check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
 
 

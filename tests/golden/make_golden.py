@@ -1,8 +1,8 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container that has the reference tree (the argument, else
-oracle.REFERENCE_TREE: SIDON_REFERENCE_ROOT or the development checkout) and
-oracle/_ref built (``make -C oracle ref REF=<root>``):
+Run in a container that has the reference tree (the argument, else the
+SIDON_REFERENCE_ROOT environment variable) and oracle/_ref built
+(``make -C oracle ref REF=<root>``):
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
 
@@ -114,8 +114,10 @@ def _probe_verify(a: np.ndarray) -> dict:
 
 def main(ref_root: str | None = None) -> None:
     ref = pathlib.Path(ref_root) if ref_root else oracle.REFERENCE_TREE
+    if ref is None:
+        raise SystemExit("give the reference root as the argument or in SIDON_REFERENCE_ROOT")
     if not oracle.have_ref():
-        oracle.build()
+        oracle.build(ref)
     spec = importlib.util.spec_from_file_location("ref_verify", ref / "verify.py")
     ref_verify = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(ref_verify)
