@@ -46,13 +46,15 @@
 //  BF16x1 keeps A_hi B_hi.  fp32 accumulation in TMEM.
 //
 //  Pipeline: one MMA warp (one elected lane issues every MMA) and builder
-//  warps; a ring of stages holding the windows of one to five tiles each,
-//  and one copy slot per phase, each guarded by a full barrier (builder
-//  arrivals) and an empty barrier (tcgen05.commit).  A stage release costs the tensor pipe
-//  far more than an MMA (fitted from phase timers at n = 8400: ~870 cycles
-//  per commit against ~70 per M128 N144 K16 instruction), so long tile
-//  sequences run two stages of two to five tiles -- one commit per stage --
-//  and short ones three single-tile stages (see ring_for).
+//  warps; a ring of stages holding the windows of one to sixteen tiles
+//  each, and one copy slot per phase, each guarded by a full barrier
+//  (builder arrivals) and an empty barrier (tcgen05.commit).  A stage's
+//  release -- the commit, the builders' wait for it and the rebuild before
+//  the MMA lane may use the stage again -- cost ~750-870 cycles per release
+//  with one tile per stage (phase timers at n = 8400, against ~72 of math
+//  per M128 N144 K16 instruction), so long tile sequences run two stages of
+//  many tiles -- one commit per stage -- and short ones three single-tile
+//  stages (see ring_for and Layout).
 //  Every pipeline wait gives up after the device state's wait limit (2^31
 //  clock cycles unless sidon_set_wait_limit changed it), records
 //  SIDON_ERR_TIMEOUT in the library's device status word and unwinds; the
