@@ -7,7 +7,8 @@
 //    stages  the window ring (ring_for): 3 stages of one tile's window
 //            (6 KB: hi | lo planes of 24 core matrices) or 2 stages of the
 //            windows of T = 2 .. 5 consecutive tiles (2 x (16 T + 8) core
-//            matrices, 10-22 KB)
+//            matrices, 10-22 KB); in the wide plan of the fused local
+//            search, 2 stages of up to 16 tiles sharing one region with cb
 //    bc      the tile phase's B-matrix copy (hi, or hi | lo); after a
 //            tile phase, gather scratch for up to 2n-1 outputs
 //    sa      fp32 heights, padded block layout (cell i at i + 4 floor(i/64)),
