@@ -126,28 +126,6 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "r"(smem_u32(bar))
                : "memory");
 }
-// the same, issued by the calling thread when `issuer` is non-zero (the
-// calling warp stays converged)
-__device__ __forceinline__ void mma_bf16_by(uint32_t issuer, uint32_t dtmem, uint64_t adesc,
-                                            uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "setp.ne.b32 q, %5, 0;\n\t"
-      "@q tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
-      :
-      : "r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(issuer)
-      : "memory");
-}
-__device__ __forceinline__ void mma_commit_by(uint32_t issuer, uint64_t* bar) {
-  asm volatile(
-      "{\n\t.reg .pred q;\n\t"
-      "setp.ne.b32 q, %1, 0;\n\t"
-      "@q tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n"
-      :
-      : "r"(smem_u32(bar)), "r"(issuer)
-      : "memory");
-}
 __device__ __forceinline__ void fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -497,23 +475,22 @@ __device__ __forceinline__ int col_corr(int m) { return conv_width(m); }
 //             (hi | lo, one slot), 3 products.
 enum TileMode { CONV_SYM = 0, CONV_X = 1, CORR = 2 };
 
-// Issue the MMAs of one tile: A descriptors ah / al (window hi / lo planes
-// at K step 0), B descriptors bh / bl (copy hi / lo planes at the tile's
-// first row), bstep = the B advance of one K16 step (16-byte units).  Called
-// by the whole MMA warp with warp-uniform operands; `issuer` (lane 0) issues.
-// three_prod selects the 3-product arithmetic, otherwise the 2-product
-// symmetric convolution.
-__device__ __forceinline__ void issue_tile(uint32_t issuer, uint32_t d, uint32_t id, uint64_t ah,
+// Issue the MMAs of one tile (the issuing thread, issue_phase): A
+// descriptors ah / al (window hi / lo planes at K step 0), B descriptors
+// bh / bl (copy hi / lo planes at the tile's first row), bstep = the B
+// advance of one K16 step (16-byte units).  three_prod selects the
+// 3-product arithmetic, otherwise the 2-product symmetric convolution.
+__device__ __forceinline__ void issue_tile(uint32_t d, uint32_t id, uint64_t ah,
                                            uint64_t al, uint64_t bh, uint64_t bl, uint64_t bstep,
                                            bool three, bool three_prod) {
 #pragma unroll
   for (int kc = 0; kc < KSTEPS; ++kc) {
     // K16 step kc = K groups 2kc, 2kc+1: A moves by 256 B, B by two K groups
     const uint64_t a = ah + (uint64_t)(16 * kc), b = bh + bstep * (uint64_t)kc;
-    mma_bf16_by(issuer, d, a, b, id, 1u);
+    mma_bf16(d, a, b, id, 1u);
     if (three) {
-      mma_bf16_by(issuer, d, al + (uint64_t)(16 * kc), b, id, 1u);
-      if (three_prod) mma_bf16_by(issuer, d, a, bl + bstep * (uint64_t)kc, id, 1u);
+      mma_bf16(d, al + (uint64_t)(16 * kc), b, id, 1u);
+      if (three_prod) mma_bf16(d, a, bl + bstep * (uint64_t)kc, id, 1u);
     }
   }
 }
@@ -552,7 +529,6 @@ struct IssueRes {
 };
 template <bool CORR, bool THREE_PROD, bool THREE>
 __device__ __noinline__ IssueRes issue_phase(const IssueArgs A) {
-  const uint32_t issuer = 1u;
   const uint32_t lbo = b_lbo(A.rows);
   int st = A.st;
   uint32_t ph = A.ph;
@@ -588,7 +564,7 @@ __device__ __noinline__ IssueRes issue_phase(const IssueArgs A) {
     }
     for (int h = 0; h < per && h < hn; ++h, ah += 128) {
       const int N = CORR ? corr_n(m) : round_up(m + ZP - x0, 16);
-      issue_tile(issuer, A.tmem + (uint32_t)dcol, id0 | ((uint32_t)(N >> 3) << 17), ah,
+      issue_tile(A.tmem + (uint32_t)dcol, id0 | ((uint32_t)(N >> 3) << 17), ah,
                  ah + aplane, bh0 + (uint64_t)x0, bl0 + (uint64_t)x0, bstep, three, THREE_PROD);
       if (CORR) {
         x0 += 2;
